@@ -1,0 +1,542 @@
+"""Python host layer over libaphi_b200.so (the C ABI in include/aphi_b200.h).
+
+Mirrors the reference's hot-path interface (namespace aphi_solver,
+include/aphi_solver/assembly.hpp and factorization.hpp): the same operations
+under the same names, the same argument meaning and the same error behaviour
+-- std::invalid_argument becomes InvalidArgument (a ValueError),
+std::logic_error becomes LogicError, and a factorization that meets its pivot
+floor returns False with stats.ok == False.
+
+Device memory, streams and tensors come from PyTorch; all arithmetic runs in
+the library's CUDA kernels. There is no CPU fallback: if the library or a GPU
+is missing, every compute call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libaphi_b200.so"
+
+OK = 0
+ERR_BAD_SHAPE = 1
+ERR_PATTERN_MISMATCH = 2
+ERR_PIVOT_FLOOR = 3
+ERR_NAN = 4
+ERR_IR_STALL = 5
+ERR_TIMEOUT = 6
+ERR_OOM = 7
+ERR_ADMISSION = 8
+ERR_CUDA = 9
+ERR_ZERO_PIVOT = 10
+ERR_DEGENERATE_TET = 11
+ERR_INVALID = 12
+
+COND_NATURAL, COND_ROW_SCALED, COND_SCALED_PHI = 0, 1, 2
+PREC_FP64, PREC_FP32 = 64, 32
+
+
+class AphiError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+class InvalidArgument(AphiError, ValueError):
+    """std::invalid_argument in the reference."""
+
+
+class LogicError(AphiError):
+    """std::logic_error in the reference."""
+
+
+class PivotFloor(AphiError):
+    """The factorization stopped at a pivot at or below the floor."""
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded library; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: run hybrid-aphi-solver_b200/build.py")
+        _lib = C.CDLL(str(LIB_PATH))
+        _declare(_lib)
+    return _lib
+
+
+P = C.c_void_p
+I = C.c_int
+D = C.c_double
+I64 = C.c_int64
+PI = C.POINTER(C.c_int)
+PD = C.POINTER(C.c_double)
+PI64 = C.POINTER(C.c_int64)
+
+
+class AssemblyDesc(C.Structure):
+    _fields_ = [("num_nodes", I), ("num_tets", I), ("num_unknowns", I),
+                ("xyz", PD), ("tets", PI), ("tet_idx", PI), ("tet_coeff", PD), ("tet_fixed", PD),
+                ("num_bodies", I), ("material", PD), ("body_ptr", PI), ("body_tets", PI),
+                ("num_ports", I), ("port_current", PI), ("port_row", PI),
+                ("port_amplitude", PD), ("port_value", PD),
+                ("upper_only", I), ("row_ptr", PI), ("col_idx", PI)]
+
+
+class AnalysisOptions(C.Structure):
+    _fields_ = [("relax_small", I), ("relax_fill", D), ("relax_max_width", I), ("small_front", I)]
+
+
+class FactorStats(C.Structure):
+    _fields_ = [("ok", I), ("columns_done", I), ("smallest_pivot", D), ("largest_pivot", D),
+                ("largest_multiplier", D), ("nnz", I64), ("milliseconds", D),
+                ("equilibration_min", D), ("equilibration_max", D)]
+
+
+class IROptions(C.Structure):
+    _fields_ = [("max_iters", I), ("tol", D), ("stall_ratio", D)]
+
+
+_SIGS = {
+    "aphi_status_string": (C.c_char_p, [I]),
+    "aphi_last_error": (C.c_char_p, []),
+    "aphi_workload_cylinder": (I, [I, D, I, C.POINTER(P)]),
+    "aphi_workload_free": (None, [P]),
+    "aphi_workload_sizes": (I, [P, PI64]),
+    "aphi_workload_array": (I, [P, C.c_char_p, C.POINTER(P), PI64]),
+    "aphi_assembly_create": (I, [C.POINTER(AssemblyDesc), C.POINTER(P)]),
+    "aphi_assembly_destroy": (I, [P]),
+    "aphi_assembly_info": (I, [P, PI64]),
+    "aphi_formulation_scales": (I, [I, D, PD, PI]),
+    "aphi_refill": (I, [P, D, I, P, P, P]),
+    "aphi_refill_batch": (I, [P, I, PD, I, P, P, P]),
+    "aphi_refill_host": (I, [P, D, I, PD, PD]),
+    "aphi_element_blocks": (I, [I, PD, D, PD, PD, PD, PD, PD]),
+    "aphi_element_coefficients": (None, [D, D, D, D, PD]),
+    "aphi_analysis_default_options": (None, [C.POINTER(AnalysisOptions)]),
+    "aphi_analysis_create": (I, [I, PI, PI, PI, PI, PI, C.POINTER(AnalysisOptions), C.POINTER(P)]),
+    "aphi_analysis_destroy": (I, [P]),
+    "aphi_analysis_info": (I, [P, PD]),
+    "aphi_analysis_etree": (I, [P, PI, PI]),
+    "aphi_factor_create": (I, [P, I, I, C.POINTER(P)]),
+    "aphi_factor_destroy": (I, [P]),
+    "aphi_factorize": (I, [P, P, I, D, C.POINTER(FactorStats), P]),
+    "aphi_solve": (I, [P, I, P, P, P]),
+    "aphi_factor_export": (I, [P, I, PI, PI, PD, PD, PD]),
+    "aphi_residuals": (I, [P, I, I, P, P, P, PD, P]),
+    "aphi_solve_refined": (I, [P, I, P, P, P, C.POINTER(IROptions), PI, PD, P]),
+    "aphi_solve_symmetric_host": (I, [P, PD, PD, I, D, PD, PD]),
+}
+
+
+def _declare(L: C.CDLL) -> None:
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(L, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGS)
+
+
+def check(status: int) -> int:
+    if status == OK:
+        return status
+    msg = lib().aphi_last_error().decode(errors="replace")
+    if status == ERR_BAD_SHAPE:
+        raise InvalidArgument(status, msg)
+    if status in (ERR_PATTERN_MISMATCH, ERR_ZERO_PIVOT):
+        raise LogicError(status, msg)
+    if status == ERR_PIVOT_FLOOR:
+        raise PivotFloor(status, msg)
+    raise AphiError(status, f"{lib().aphi_status_string(status).decode()}: {msg}")
+
+
+def _ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def dptr(t) -> C.c_void_p:
+    """Device pointer of a torch tensor (or None)."""
+    return C.c_void_p(0 if t is None else t.data_ptr())
+
+
+def stream_ptr(stream) -> C.c_void_p:
+    if stream is None:
+        return C.c_void_p(0)
+    return C.c_void_p(stream.cuda_stream)
+
+
+# ---------------------------------------------------------------- workloads
+class Workload:
+    """The cylinder-in-box problem's host-side inputs (numpy views)."""
+
+    ARRAYS = {"xyz": np.float64, "tets": np.int32, "tet_idx": np.int32, "tet_coeff": np.float64,
+              "tet_fixed": np.float64, "material": np.float64, "body_ptr": np.int32,
+              "body_tets": np.int32, "port_current": np.int32, "port_row": np.int32,
+              "port_amplitude": np.float64, "port_value": np.float64, "row_ptr": np.int32,
+              "col_idx": np.int32, "edges": np.int32, "edge_index": np.int32,
+              "phi_index": np.int32, "tet_edges": np.int32, "body_of_tet": np.int32}
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+        s = (C.c_int64 * 10)()
+        check(lib().aphi_workload_sizes(self._h, s))
+        (self.num_nodes, self.num_tets, self.num_edges, self.num_unknowns, self.nnz,
+         self.num_a, self.num_phi, self.num_ports, self.num_bodies, _) = list(s)
+        self._arrays = {}
+
+    @classmethod
+    def cylinder(cls, cells: int, v_top: float = 1.0, full_wave: bool = False) -> "Workload":
+        h = P()
+        check(lib().aphi_workload_cylinder(cells, v_top, 1 if full_wave else 0, C.byref(h)))
+        return cls(h)
+
+    def array(self, name: str) -> np.ndarray:
+        if name not in self._arrays:
+            data = P()
+            count = C.c_int64()
+            check(lib().aphi_workload_array(self._h, name.encode(), C.byref(data), C.byref(count)))
+            dt = np.dtype(self.ARRAYS[name])
+            if count.value == 0:
+                self._arrays[name] = np.zeros(0, dt)
+            else:
+                buf = (C.c_char * (count.value * dt.itemsize)).from_address(data.value)
+                self._arrays[name] = np.frombuffer(buf, dtype=dt).copy()
+        return self._arrays[name]
+
+    def __getattr__(self, name):
+        if name in Workload.ARRAYS:
+            return self.array(name)
+        raise AttributeError(name)
+
+    def close(self):
+        if self._h:
+            lib().aphi_workload_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def assembly_desc_from(arrays: dict, upper_only: bool = True):
+    """An AssemblyDesc over numpy arrays (kept alive by the returned tuple)."""
+    keep = {}
+
+    def arr(name, dt):
+        a = np.ascontiguousarray(arrays[name], dtype=dt)
+        keep[name] = a
+        return a
+
+    xyz = arr("xyz", np.float64)
+    tets = arr("tets", np.int32)
+    tet_idx = arr("tet_idx", np.int32)
+    tet_coeff = arr("tet_coeff", np.float64)
+    tet_fixed = arr("tet_fixed", np.float64)
+    material = arr("material", np.float64)
+    body_ptr = arr("body_ptr", np.int32)
+    body_tets = arr("body_tets", np.int32)
+    port_current = arr("port_current", np.int32)
+    port_row = arr("port_row", np.int32)
+    port_amplitude = arr("port_amplitude", np.float64)
+    port_value = arr("port_value", np.float64)
+    row_ptr = arr("row_ptr", np.int32)
+    col_idx = arr("col_idx", np.int32)
+    d = AssemblyDesc()
+    d.num_nodes = xyz.size // 3
+    d.num_tets = tets.size // 4
+    d.num_unknowns = row_ptr.size - 1
+    d.xyz, d.tets, d.tet_idx = _ptr(xyz, C.c_double), _ptr(tets, C.c_int), _ptr(tet_idx, C.c_int)
+    d.tet_coeff, d.tet_fixed = _ptr(tet_coeff, C.c_double), _ptr(tet_fixed, C.c_double)
+    d.num_bodies = material.size // 3
+    d.material, d.body_ptr, d.body_tets = (_ptr(material, C.c_double), _ptr(body_ptr, C.c_int),
+                                           _ptr(body_tets, C.c_int))
+    d.num_ports = port_row.size
+    d.port_current, d.port_row = _ptr(port_current, C.c_int), _ptr(port_row, C.c_int)
+    d.port_amplitude, d.port_value = _ptr(port_amplitude, C.c_double), _ptr(port_value, C.c_double)
+    d.upper_only = 1 if upper_only else 0
+    d.row_ptr, d.col_idx = _ptr(row_ptr, C.c_int), _ptr(col_idx, C.c_int)
+    return d, keep
+
+
+def workload_arrays(w: Workload) -> dict:
+    return {k: w.array(k) for k in Workload.ARRAYS}
+
+
+# ---------------------------------------------------------------- assembly
+def formulation_scales(conditioning: int, omega: float):
+    """formulation_scales (src/assembly.cpp:12-45): (row, column, symmetric)."""
+    rc = (C.c_double * 4)()
+    sym = C.c_int()
+    check(lib().aphi_formulation_scales(conditioning, omega, rc, C.byref(sym)))
+    return complex(rc[0], rc[1]), complex(rc[2], rc[3]), bool(sym.value)
+
+
+def element_coefficients(sigma: float, eps_r: float, mu_r: float, omega: float):
+    out = (C.c_double * 5)()
+    lib().aphi_element_coefficients(sigma, eps_r, mu_r, omega, out)
+    return out[0], complex(out[1], out[2]), complex(out[3], out[4])
+
+
+def element_blocks(xyz: np.ndarray, nu: float, alpha: complex, beta: complex):
+    """kernel_AA / kernel_APhi / kernel_PhiPhi on the device for tets xyz[T,4,3]."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 12)
+    t = xyz.shape[0]
+    aa = np.zeros((t, 36), np.complex128)
+    ap = np.zeros((t, 60), np.complex128)
+    pp = np.zeros((t, 100), np.complex128)
+    a = (C.c_double * 2)(alpha.real, alpha.imag)
+    b = (C.c_double * 2)(beta.real, beta.imag)
+    check(lib().aphi_element_blocks(t, _ptr(xyz, C.c_double), nu, a, b,
+                                    aa.view(np.float64).ctypes.data_as(PD),
+                                    ap.view(np.float64).ctypes.data_as(PD),
+                                    pp.view(np.float64).ctypes.data_as(PD)))
+    return aa.reshape(t, 6, 6), ap.reshape(t, 6, 10), pp.reshape(t, 10, 10)
+
+
+class Assembly:
+    """Device assembly for one mesh: refill at any frequency (refill,
+    src/assembly.cpp:453-494). Values and rhs are complex128 device tensors."""
+
+    def __init__(self, arrays: dict, upper_only: bool = True):
+        desc, keep = assembly_desc_from(arrays, upper_only)
+        self._h = P()
+        check(lib().aphi_assembly_create(C.byref(desc), C.byref(self._h)))
+        info = (C.c_int64 * 4)()
+        check(lib().aphi_assembly_info(self._h, info))
+        self.nnz, self.num_unknowns, self.num_terms, self.device_bytes = list(info)
+
+    def refill(self, omega, conditioning=COND_ROW_SCALED, values=None, rhs=None, stream=None):
+        import torch
+        omegas = np.atleast_1d(np.asarray(omega, dtype=np.float64))
+        nf = omegas.size
+        if values is None:
+            values = torch.empty((nf, self.nnz), dtype=torch.complex128, device="cuda")
+        if rhs is None:
+            rhs = torch.empty((nf, self.num_unknowns), dtype=torch.complex128, device="cuda")
+        check(lib().aphi_refill_batch(self._h, nf, _ptr(omegas, C.c_double), conditioning,
+                                      dptr(values), dptr(rhs), stream_ptr(stream)))
+        return values, rhs
+
+    def refill_host(self, omega: float, conditioning=COND_ROW_SCALED):
+        v = np.zeros(self.nnz, np.complex128)
+        r = np.zeros(self.num_unknowns, np.complex128)
+        check(lib().aphi_refill_host(self._h, omega, conditioning, v.view(np.float64).ctypes.data_as(PD),
+                                     r.view(np.float64).ctypes.data_as(PD)))
+        return v, r
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().aphi_assembly_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- analysis
+def default_analysis_options() -> AnalysisOptions:
+    o = AnalysisOptions()
+    lib().aphi_analysis_default_options(C.byref(o))
+    return o
+
+
+class Analysis:
+    """Supernodal schedule for one pattern + permutation (the reference's
+    SolverAnalysis, include/aphi_solver/symbolic.hpp:69-92, consumed as input).
+
+    perm is the reference's Permutation::perm (new -> old); parent and
+    col_count, when given, must equal this pattern's elimination tree and
+    column counts under perm (LogicError otherwise)."""
+
+    INFO = ["n", "nnz_upper", "nnz_l", "stored", "supernodes", "levels", "max_rows", "max_width",
+            "flops", "cb_pool", "factor_bytes_fp64", "num_roots"]
+
+    def __init__(self, row_ptr, col_idx, perm=None, parent=None, col_count=None, options=None):
+        rp = np.ascontiguousarray(row_ptr, np.int32)
+        ci = np.ascontiguousarray(col_idx, np.int32)
+        n = rp.size - 1
+        pm = None if perm is None else np.ascontiguousarray(perm, np.int32)
+        pa = None if parent is None else np.ascontiguousarray(parent, np.int32)
+        cc = None if col_count is None else np.ascontiguousarray(col_count, np.int32)
+        opt = options if options is not None else default_analysis_options()
+        self._keep = (rp, ci)
+        self._h = P()
+        nul = C.POINTER(C.c_int)()
+        check(lib().aphi_analysis_create(
+            n, _ptr(rp, C.c_int), _ptr(ci, C.c_int),
+            nul if pm is None else _ptr(pm, C.c_int), nul if pa is None else _ptr(pa, C.c_int),
+            nul if cc is None else _ptr(cc, C.c_int), C.byref(opt), C.byref(self._h)))
+        info = (C.c_double * 12)()
+        check(lib().aphi_analysis_info(self._h, info))
+        self.info = dict(zip(self.INFO, list(info)))
+        self.n = n
+        self.nnz = int(self.info["nnz_upper"])
+        self.row_ptr, self.col_idx = rp, ci
+
+    def etree(self):
+        parent = np.zeros(self.n, np.int32)
+        cc = np.zeros(self.n, np.int32)
+        check(lib().aphi_analysis_etree(self._h, _ptr(parent, C.c_int), _ptr(cc, C.c_int)))
+        return parent, cc
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().aphi_analysis_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # Python-side mirror of factorize_ldlt / solve / solve_symmetric lives in
+    # the Factor class and the module functions below.
+
+
+STATS_KEYS = ["ok", "columns_done", "smallest_pivot", "largest_pivot", "largest_multiplier", "nnz",
+              "milliseconds", "equilibration_min", "equilibration_max"]
+
+
+def _stats_dict(s: FactorStats) -> dict:
+    return {k: getattr(s, k) for k in STATS_KEYS}
+
+
+class Factor:
+    """`batch` numeric factorizations sharing one Analysis, resident on the
+    device (factorize_ldlt, src/factorization.cpp:109-218, run as a
+    supernodal multifrontal LDL^T with no pivoting and no conjugation)."""
+
+    def __init__(self, analysis: Analysis, precision: int = PREC_FP64, batch: int = 1):
+        self.analysis = analysis
+        self.precision = precision
+        self.batch = batch
+        self.n = analysis.n
+        self._h = P()
+        check(lib().aphi_factor_create(analysis._h, precision, batch, C.byref(self._h)))
+        self.stats = []
+
+    def factorize(self, values, equilibration_iterations: int = 10, pivot_floor: float = 0.0,
+                  stream=None) -> bool:
+        """values: complex128 device tensor [batch, nnz]. Returns False (with
+        self.stats[k]['ok'] == 0) if any entry met the pivot floor."""
+        st = (FactorStats * self.batch)()
+        rc = lib().aphi_factorize(self._h, dptr(values), equilibration_iterations, pivot_floor, st,
+                                  stream_ptr(stream))
+        self.stats = [_stats_dict(s) for s in st]
+        if rc == ERR_PIVOT_FLOOR:
+            return False
+        check(rc)
+        return True
+
+    def solve(self, b, x=None, stream=None):
+        """b: complex128 device tensor [batch, nrhs, n] (or [batch, n])."""
+        import torch
+        squeeze = b.dim() == 2
+        bb = b.unsqueeze(1) if squeeze else b
+        nrhs = bb.shape[1]
+        bb = bb.contiguous()
+        if x is None:
+            x = torch.empty_like(bb)
+        check(lib().aphi_solve(self._h, nrhs, dptr(bb), dptr(x), stream_ptr(stream)))
+        return x.squeeze(1) if squeeze else x
+
+    def solve_refined(self, values, b, tol=1e-14, max_iters=10, stall_ratio=0.5, stream=None):
+        import torch
+        squeeze = b.dim() == 2
+        bb = (b.unsqueeze(1) if squeeze else b).contiguous()
+        nrhs = bb.shape[1]
+        x = torch.empty_like(bb)
+        it = (C.c_int * (self.batch * nrhs))()
+        be = (C.c_double * (self.batch * nrhs))()
+        opt = IROptions(max_iters, tol, stall_ratio)
+        rc = lib().aphi_solve_refined(self._h, nrhs, dptr(values), dptr(bb), dptr(x), C.byref(opt), it, be,
+                                      stream_ptr(stream))
+        if rc not in (OK, ERR_IR_STALL):
+            check(rc)
+        x = x.squeeze(1) if squeeze else x
+        return x, np.array(list(it)).reshape(self.batch, nrhs), np.array(list(be)).reshape(self.batch, nrhs), rc == OK
+
+    def export(self, k: int = 0) -> dict:
+        """Entry k in the reference's SymmetricFactor layout (strictly lower
+        CSC, rows ascending, caller's permuted numbering) plus D and the
+        equilibration vector."""
+        n = self.n
+        nl = int(self.analysis.info["nnz_l"]) - n
+        cp = np.zeros(n + 1, np.int32)
+        ri = np.zeros(max(nl, 1), np.int32)
+        val = np.zeros(max(nl, 1), np.complex128)
+        dg = np.zeros(n, np.complex128)
+        ds = np.zeros(n)
+        check(lib().aphi_factor_export(self._h, k, _ptr(cp, C.c_int), _ptr(ri, C.c_int),
+                                       val.view(np.float64).ctypes.data_as(PD),
+                                       dg.view(np.float64).ctypes.data_as(PD), _ptr(ds, C.c_double)))
+        return dict(col_ptr=cp, row_index=ri[:nl], value=val[:nl], diagonal=dg, d=ds)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().aphi_factor_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def residuals(analysis: Analysis, values, x, b, stream=None) -> np.ndarray:
+    """[batch, nrhs, 2]: relative_residual and backward_error per solution
+    (src/factorization.cpp:315-329, :401-416), on the original system."""
+    bb = b.unsqueeze(1) if b.dim() == 2 else b
+    xx = x.unsqueeze(1) if x.dim() == 2 else x
+    batch, nrhs = bb.shape[0], bb.shape[1]
+    out = np.zeros((batch, nrhs, 2))
+    check(lib().aphi_residuals(analysis._h, batch, nrhs, dptr(values), dptr(xx.contiguous()),
+                               dptr(bb.contiguous()), out.ctypes.data_as(PD), None))
+    return out
+
+
+REPORT_KEYS = ["ok", "backward_error", "residual", "equilibration_min", "equilibration_max", "smallest_pivot",
+               "largest_pivot", "largest_multiplier", "factor_nnz", "columns_done", "analyze_ms", "factorize_ms",
+               "solve_ms"]
+
+
+def solve_symmetric(analysis: Analysis, values: np.ndarray, b: np.ndarray, equilibration_iterations: int = 10,
+                    pivot_floor: float = 0.0):
+    """solve_symmetric (src/factorization.cpp:332-398) on host arrays:
+    returns (ok, x, report). ok is False, with the report filled as far as it
+    got, when the factorization met its pivot floor."""
+    v = np.ascontiguousarray(values, np.complex128)
+    bb = np.ascontiguousarray(b, np.complex128)
+    if bb.size != analysis.n:
+        raise InvalidArgument(ERR_BAD_SHAPE, f"solve_symmetric: the right-hand side has {bb.size} entries "
+                                             f"for a matrix of {analysis.n} rows")
+    x = np.zeros(analysis.n, np.complex128)
+    rep = np.zeros(13)
+    rc = lib().aphi_solve_symmetric_host(analysis._h, v.view(np.float64).ctypes.data_as(PD),
+                                         bb.view(np.float64).ctypes.data_as(PD), equilibration_iterations,
+                                         pivot_floor, x.view(np.float64).ctypes.data_as(PD),
+                                         rep.ctypes.data_as(PD))
+    report = dict(zip(REPORT_KEYS, rep.tolist()))
+    if rc == ERR_PIVOT_FLOOR:
+        return False, x, report
+    check(rc)
+    return True, x, report

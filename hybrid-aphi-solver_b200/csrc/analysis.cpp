@@ -1,0 +1,202 @@
+#include "analysis.hpp"
+
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace aphi_b200 {
+
+namespace {
+
+template <class T>
+T* upload(const std::vector<T>& h, long long& bytes) {
+    T* d = nullptr;
+    const size_t n = std::max<size_t>(h.size(), 1);
+    APHI_CUDA(cudaMalloc(&d, n * sizeof(T)));
+    if (!h.empty()) APHI_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    bytes += static_cast<long long>(n * sizeof(T));
+    return d;
+}
+
+// The factorization plan: per level, extend-add items, then one-CTA fronts,
+// then the blocked steps of the large fronts (diagonal block, panel rows,
+// trailing update), step by step.
+void build_plans(aphi_analysis& A, std::vector<Item>& items) {
+    const Symbolic& S = A.S;
+    auto push = [&](std::vector<Launch>& plan, int kind, long long first) {
+        const int count = static_cast<int>(items.size() - first);
+        if (count > 0) plan.push_back({kind, first, count});
+    };
+    for (int L = 0; L < S.num_levels; ++L) {
+        const int* lb = S.level_list.data() + S.level_ptr[L];
+        const int* le = S.level_list.data() + S.level_ptr[L + 1];
+        long long f0 = static_cast<long long>(items.size());
+        for (const int* p = lb; p < le; ++p) {
+            const int s = *p;
+            const int w = S.sn_first[s + 1] - S.sn_first[s];
+            const int m = S.sn_rows[s];
+            const bool kids = S.child_ptr[s + 1] > S.child_ptr[s];
+            const int c0 = kids ? 0 : w;  // without children only the CB needs zeroing
+            for (int c = c0 - (c0 % kEaCols); c < m; c += kEaCols)
+                if (kids || m > w) items.push_back({s, c, 0, 0});
+        }
+        push(A.plan_factor, K_EXTEND_ADD, f0);
+        f0 = static_cast<long long>(items.size());
+        std::vector<int> large;
+        for (const int* p = lb; p < le; ++p) {
+            if (S.sn_rows[*p] <= A.opt.small_front)
+                items.push_back({*p, 0, 0, 0});
+            else
+                large.push_back(*p);
+        }
+        push(A.plan_factor, K_SMALL, f0);
+        int maxw = 0;
+        for (int s : large) maxw = std::max(maxw, S.sn_first[s + 1] - S.sn_first[s]);
+        for (int k0 = 0; k0 < maxw; k0 += kStep) {
+            f0 = static_cast<long long>(items.size());
+            for (int s : large)
+                if (k0 < S.sn_first[s + 1] - S.sn_first[s]) items.push_back({s, k0, 0, 0});
+            push(A.plan_factor, K_DIAG, f0);
+            f0 = static_cast<long long>(items.size());
+            for (int s : large) {
+                const int w = S.sn_first[s + 1] - S.sn_first[s];
+                if (k0 >= w) continue;
+                const int k1 = std::min(w, k0 + kStep);
+                for (int r = k1; r < S.sn_rows[s]; r += kTrsmRows) items.push_back({s, k0, r, 0});
+            }
+            push(A.plan_factor, K_TRSM, f0);
+            f0 = static_cast<long long>(items.size());
+            for (int s : large) {
+                const int w = S.sn_first[s + 1] - S.sn_first[s];
+                if (k0 >= w) continue;
+                const int k1 = std::min(w, k0 + kStep);
+                const int m = S.sn_rows[s];
+                for (int j = k1; j < m; j += kTile)
+                    for (int i = j; i < m; i += kTile) items.push_back({s, k0, i, j});
+            }
+            push(A.plan_factor, K_UPDATE, f0);
+        }
+    }
+    // Solves: forward bottom-up, backward top-down, one item per supernode.
+    for (int L = 0; L < S.num_levels; ++L) {
+        const long long f0 = static_cast<long long>(items.size());
+        for (int k = S.level_ptr[L]; k < S.level_ptr[L + 1]; ++k) items.push_back({S.level_list[k], 0, 0, 0});
+        push(A.plan_fwd, K_FWD, f0);
+    }
+    for (int L = S.num_levels - 1; L >= 0; --L) {
+        const long long f0 = static_cast<long long>(items.size());
+        for (int k = S.level_ptr[L]; k < S.level_ptr[L + 1]; ++k) items.push_back({S.level_list[k], 0, 0, 0});
+        push(A.plan_bwd, K_BWD, f0);
+    }
+}
+
+}  // namespace
+
+aphi_analysis* analysis_create(int n, const int* row_ptr, const int* col_idx, const int* perm,
+                               const int* parent, const int* col_count, const aphi_analysis_options& o) {
+    auto* A = new aphi_analysis;
+    try {
+        A->opt = o;
+        if (A->opt.small_front < 1) A->opt.small_front = 1;
+        if (A->opt.small_front > 96) A->opt.small_front = 96;
+        A->S = analyze_supernodal(n, row_ptr, col_idx, perm, parent, col_count, A->opt);
+        const Symbolic& S = A->S;
+        build_plans(*A, A->h_items);
+        A->num_items = static_cast<long long>(A->h_items.size());
+        A->h_uoff.assign(S.ns + 1, 0);
+        for (int s = 0; s < S.ns; ++s)
+            A->h_uoff[s + 1] = A->h_uoff[s] + (S.sn_rows[s] - (S.sn_first[s + 1] - S.sn_first[s]));
+        A->upool = A->h_uoff[S.ns];
+        A->h_row_ptr.assign(row_ptr, row_ptr + n + 1);
+        A->h_col_idx.assign(col_idx, col_idx + row_ptr[n]);
+        // Both triangles, for the residual's SpMV: row r lists its upper entries
+        // then the mirrors of the entries above it, in a fixed order.
+        A->h_fptr.assign(n + 1, 0);
+        for (int r = 0; r < n; ++r)
+            for (int k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
+                ++A->h_fptr[r + 1];
+                if (col_idx[k] != r) ++A->h_fptr[col_idx[k] + 1];
+            }
+        for (int r = 0; r < n; ++r) A->h_fptr[r + 1] += A->h_fptr[r];
+        A->h_fcol.resize(A->h_fptr[n]);
+        A->h_fmap.resize(A->h_fptr[n]);
+        {
+            std::vector<int> cur(A->h_fptr.begin(), A->h_fptr.end() - 1);
+            for (int r = 0; r < n; ++r)
+                for (int k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
+                    const int c = col_idx[k];
+                    A->h_fcol[cur[r]] = c;
+                    A->h_fmap[cur[r]++] = k;
+                    if (c != r) {
+                        A->h_fcol[cur[c]] = r;
+                        A->h_fmap[cur[c]++] = k;
+                    }
+                }
+        }
+    } catch (...) {
+        delete A;
+        throw;
+    }
+    return A;
+}
+
+void analysis_destroy(aphi_analysis* a) { delete a; }
+
+// Device copies are made when the first factor is created, so an analysis can
+// be built and inspected on a host without a GPU.
+void analysis_ensure_device(aphi_analysis* A) {
+    if (A->on_device) return;
+    const Symbolic& S = A->S;
+    long long& b = A->device_bytes;
+    DeviceSchedule& d = A->d;
+    d.first = upload(S.sn_first, b);
+    d.rows = upload(S.sn_rows, b);
+    d.loff = upload(S.sn_loff, b);
+    d.cboff = upload(S.sn_cboff, b);
+    d.soff = upload(S.sn_struct_off, b);
+    d.structs = upload(S.structs, b);
+    d.reloff = upload(S.rel_off, b);
+    d.rel = upload(S.rel, b);
+    d.child_ptr = upload(S.child_ptr, b);
+    d.child_list = upload(S.child_list, b);
+    d.uoff = upload(A->h_uoff, b);
+    d.a_dest = upload(S.a_dest, b);
+    d.row_ptr = upload(A->h_row_ptr, b);
+    d.col_idx = upload(A->h_col_idx, b);
+    d.new_of_orig = upload(S.new_of_orig, b);
+    d.orig_of_new = upload(S.orig_of_new, b);
+    d.ref_of_post = upload(S.ref_of_post, b);
+    d.fptr = upload(A->h_fptr, b);
+    d.fcol = upload(A->h_fcol, b);
+    d.fmap = upload(A->h_fmap, b);
+    d.items = upload(A->h_items, b);
+    A->on_device = true;
+}
+
+const Symbolic& analysis_symbolic(const aphi_analysis* a) { return a->S; }
+
+void analysis_info(const aphi_analysis* a, double* info) {
+    const Symbolic& S = a->S;
+    info[0] = S.n;
+    info[1] = static_cast<double>(S.nnz_a);
+    info[2] = static_cast<double>(S.nnz_l);
+    info[3] = static_cast<double>(S.stored);
+    info[4] = S.ns;
+    info[5] = S.num_levels;
+    info[6] = S.max_rows;
+    info[7] = S.max_width;
+    info[8] = S.flops;
+    info[9] = static_cast<double>(S.cb_pool);
+    info[10] = static_cast<double>((S.stored + S.cb_pool) * 16);
+    info[11] = S.num_roots;
+}
+
+}  // namespace aphi_b200
+
+aphi_analysis::~aphi_analysis() {
+    void* ptrs[] = {d.first, d.rows, d.loff, d.cboff, d.soff, d.structs, d.reloff, d.rel, d.child_ptr,
+                    d.child_list, d.uoff, d.a_dest, d.row_ptr, d.col_idx, d.new_of_orig, d.orig_of_new,
+                    d.ref_of_post, d.fptr, d.fcol, d.fmap, d.items};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+}

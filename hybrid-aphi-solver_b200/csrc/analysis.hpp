@@ -1,0 +1,91 @@
+// Device-side analysis: the supernodal schedule uploaded once per pattern,
+// plus the launch plans (work lists per elimination-tree level) that the
+// numeric factorization and the solves replay.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "aphi_b200.h"
+#include "symbolic.hpp"
+
+namespace aphi_b200 {
+
+// Work item kinds.
+enum Kind : int {
+    K_EXTEND_ADD = 0,  // (s, col0): zero CB columns, add children's CBs, for 32 front columns
+    K_SMALL = 1,       // (s): whole front in shared memory
+    K_DIAG = 2,        // (s, k0): factor the diagonal block of step k0
+    K_TRSM = 3,        // (s, k0, row0): rows row0.. of L21 for step k0
+    K_UPDATE = 4,      // (s, k0, i0, j0): trailing update tile
+    K_FWD = 5,         // (s): forward solve of one supernode
+    K_BWD = 6,         // (s): backward solve of one supernode
+};
+
+struct Launch {
+    int kind;
+    long long first;  // offset into the item array
+    int count;
+};
+
+struct Item {
+    int s, a, b, c;
+};
+
+constexpr int kStep = 32;        // pivot block width of the blocked factorization
+constexpr int kTile = 64;        // update tile
+constexpr int kTrsmRows = 128;   // rows per TRSM block
+constexpr int kEaCols = 32;      // front columns per extend-add item
+
+struct DeviceSchedule {
+    int* first = nullptr;
+    int* rows = nullptr;
+    long long* loff = nullptr;
+    long long* cboff = nullptr;
+    long long* soff = nullptr;
+    int* structs = nullptr;
+    long long* reloff = nullptr;
+    int* rel = nullptr;
+    int* child_ptr = nullptr;
+    int* child_list = nullptr;
+    long long* uoff = nullptr;  // update-vector offsets (solve), per supernode
+    long long* a_dest = nullptr;
+    int* row_ptr = nullptr;     // upper CSR, original numbering
+    int* col_idx = nullptr;
+    int* new_of_orig = nullptr;
+    int* orig_of_new = nullptr;
+    int* ref_of_post = nullptr;
+    int* fptr = nullptr;        // both triangles of A: row pointers,
+    int* fcol = nullptr;        // columns,
+    long long* fmap = nullptr;  // and the index of each entry in the upper values
+    Item* items = nullptr;
+};
+
+}  // namespace aphi_b200
+
+struct aphi_analysis {
+    aphi_b200::Symbolic S;
+    aphi_analysis_options opt{};
+    aphi_b200::DeviceSchedule d;
+    std::vector<aphi_b200::Launch> plan_factor, plan_fwd, plan_bwd;
+    std::vector<aphi_b200::Item> h_items;
+    std::vector<long long> h_uoff;
+    std::vector<int> h_row_ptr, h_col_idx;
+    std::vector<int> h_fptr, h_fcol;
+    std::vector<long long> h_fmap;
+    bool on_device = false;
+    long long num_items = 0;
+    long long upool = 0;   // update-vector pool entries (per rhs)
+    long long device_bytes = 0;
+    ~aphi_analysis();
+};
+
+namespace aphi_b200 {
+aphi_analysis* analysis_create(int n, const int* row_ptr, const int* col_idx, const int* perm,
+                               const int* parent, const int* col_count, const aphi_analysis_options& o);
+void analysis_destroy(aphi_analysis* a);
+void analysis_ensure_device(aphi_analysis* a);
+void analysis_info(const aphi_analysis* a, double* info);
+const Symbolic& analysis_symbolic(const aphi_analysis* a);
+}  // namespace aphi_b200

@@ -1,0 +1,719 @@
+// Numeric assembly on the device: element fill (K1) and deterministic scatter
+// (K2) into the upper-triangle CSR of the symmetric system.
+//
+// Reference: refill -> scatter_into, src/assembly.cpp:255-422;
+// element_coefficients and kernel_AA/APhi/PhiPhi, src/element_matrix.cpp:10-115;
+// compute_tet_geometry, src/basis_functions.cpp:15-85; the degree-2 rule,
+// src/quadrature.cpp:16-35.
+//
+// Design. The reference accumulates `values[slot] += term` while it walks
+// bodies -> tets -> (AA, A-Phi/Phi-A, Phi-Phi) blocks. Here
+//   K1 (k_tet_terms): one thread per tet computes the tet's geometry and its
+//       element blocks and writes every term it contributes -- already scaled
+//       exactly as the reference forms the addend -- into a term array, in the
+//       reference's loop order. Terms bound for the right-hand side are stored
+//       negated (the reference subtracts them).
+//   K2 (k_slot_sum): one thread per destination (CSR slot or rhs row) sums its
+//       terms in increasing term order through a slot -> term list built once
+//       per mesh. Increasing term order IS the reference's accumulation order,
+//       so the sums are bitwise those of the reference: no float atomics, no
+//       order that depends on scheduling.
+// This file is compiled with -fmad=false and uses explicitly rounded
+// intrinsics for complex products, so every element entry and every addend is
+// rounded exactly as the host's std::complex<double> arithmetic rounds it.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <vector>
+
+#include "assembly.hpp"
+#include "common.cuh"
+
+namespace aphi_b200 {
+
+namespace {
+
+__constant__ int c_edge_verts[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {2, 3}, {1, 3}};
+
+// mu_0 and eps_0 as include/aphi_solver/constants.hpp:12-13 defines them.
+constexpr double kMu0 = 4.0e-7 * 3.14159265358979323846;
+constexpr double kEps0 = 8.8541878128e-12;
+
+struct Geometry {
+    double grad[4][3];
+    double volume;
+};
+
+// Gauss-Jordan inverse of M = [1 x y z] per vertex row with partial
+// pivoting; column i of M^-1 holds L_i's affine coefficients. Returns false
+// for a pivot below 1e-14 (a degenerate tet).
+__device__ bool tet_geometry(const double p[4][3], Geometry& g) {
+    double m[4][4], inv[4][4];
+    for (int r = 0; r < 4; ++r) {
+        m[r][0] = 1.0;
+        m[r][1] = p[r][0];
+        m[r][2] = p[r][1];
+        m[r][3] = p[r][2];
+        for (int c = 0; c < 4; ++c) inv[r][c] = (r == c) ? 1.0 : 0.0;
+    }
+    for (int col = 0; col < 4; ++col) {
+        int prow = col;
+        double pval = fabs(m[col][col]);
+        for (int r = col + 1; r < 4; ++r)
+            if (fabs(m[r][col]) > pval) {
+                prow = r;
+                pval = fabs(m[r][col]);
+            }
+        if (pval < 1e-14) return false;
+        if (prow != col)
+            for (int c = 0; c < 4; ++c) {
+                double t = m[prow][c];
+                m[prow][c] = m[col][c];
+                m[col][c] = t;
+                t = inv[prow][c];
+                inv[prow][c] = inv[col][c];
+                inv[col][c] = t;
+            }
+        const double piv = m[col][col];
+        for (int c = 0; c < 4; ++c) {
+            m[col][c] = __ddiv_rn(m[col][c], piv);
+            inv[col][c] = __ddiv_rn(inv[col][c], piv);
+        }
+        for (int r = 0; r < 4; ++r) {
+            if (r == col) continue;
+            const double f = m[r][col];
+            if (f == 0.0) continue;
+            for (int c = 0; c < 4; ++c) {
+                m[r][c] = __dsub_rn(m[r][c], __dmul_rn(f, m[col][c]));
+                inv[r][c] = __dsub_rn(inv[r][c], __dmul_rn(f, inv[col][c]));
+            }
+        }
+    }
+    for (int i = 0; i < 4; ++i) {
+        g.grad[i][0] = inv[1][i];
+        g.grad[i][1] = inv[2][i];
+        g.grad[i][2] = inv[3][i];
+    }
+    // |((p1 - p0) x (p2 - p0)) . (p3 - p0)| / 6
+    double a[3], b[3], c[3];
+    for (int k = 0; k < 3; ++k) {
+        a[k] = __dsub_rn(p[1][k], p[0][k]);
+        b[k] = __dsub_rn(p[2][k], p[0][k]);
+        c[k] = __dsub_rn(p[3][k], p[0][k]);
+    }
+    const double x = __dsub_rn(__dmul_rn(a[1], b[2]), __dmul_rn(a[2], b[1]));
+    const double y = __dsub_rn(__dmul_rn(a[2], b[0]), __dmul_rn(a[0], b[2]));
+    const double z = __dsub_rn(__dmul_rn(a[0], b[1]), __dmul_rn(a[1], b[0]));
+    const double dot = __dadd_rn(__dadd_rn(__dmul_rn(x, c[0]), __dmul_rn(y, c[1])), __dmul_rn(z, c[2]));
+    g.volume = fabs(__ddiv_rn(dot, 6.0));
+    return true;
+}
+
+__device__ __forceinline__ double dot3(const double* u, const double* v) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(u[0], v[0]), __dmul_rn(u[1], v[1])), __dmul_rn(u[2], v[2]));
+}
+
+// Whitney edge function at barycentric point L: grad(L_j) L_i - grad(L_i) L_j.
+__device__ __forceinline__ void whitney(const Geometry& g, int e, const double* L, double* out) {
+    const int vi = c_edge_verts[e][0], vj = c_edge_verts[e][1];
+    for (int k = 0; k < 3; ++k)
+        out[k] = __dsub_rn(__dmul_rn(g.grad[vj][k], L[vi]), __dmul_rn(g.grad[vi][k], L[vj]));
+}
+
+// Gradient of P2 nodal function b at L.
+__device__ __forceinline__ void p2_grad(const Geometry& g, int b, const double* L, double* out) {
+    if (b < 4) {
+        const double s = __dsub_rn(__dmul_rn(4.0, L[b]), 1.0);
+        for (int k = 0; k < 3; ++k) out[k] = __dmul_rn(g.grad[b][k], s);
+    } else {
+        const int v0 = c_edge_verts[b - 4][0], v1 = c_edge_verts[b - 4][1];
+        const double s0 = __dmul_rn(4.0, L[v1]), s1 = __dmul_rn(4.0, L[v0]);
+        for (int k = 0; k < 3; ++k)
+            out[k] = __dadd_rn(__dmul_rn(g.grad[v0][k], s0), __dmul_rn(g.grad[v1][k], s1));
+    }
+}
+
+struct Coeff {
+    double nu;
+    cplx alpha, beta;
+};
+
+// element_coefficients, src/element_matrix.cpp:10-25.
+__host__ __device__ inline Coeff body_coefficients(double sigma, double eps_r, double mu_r, double omega) {
+    Coeff c;
+#ifdef __CUDA_ARCH__
+    const double mu = __dmul_rn(mu_r, kMu0);
+    const double eps = __dmul_rn(eps_r, kEps0);
+    c.nu = __ddiv_rn(1.0, mu);
+    c.alpha = cplx{__dmul_rn(__dmul_rn(-omega, omega), eps), __dmul_rn(omega, sigma)};
+    c.beta = cplx{sigma, __dmul_rn(omega, eps)};
+#else
+    const double mu = mu_r * kMu0;
+    const double eps = eps_r * kEps0;
+    c.nu = 1.0 / mu;
+    c.alpha = cplx{-omega * omega * eps, omega * sigma};
+    c.beta = cplx{sigma, omega * eps};
+#endif
+    return c;
+}
+
+// The degree-2 rule: points (a,b,b,b) and permutations, weights 1/4.
+struct Quad {
+    double a, b;
+};
+
+// kernel_AA, kernel_APhi, kernel_PhiPhi (src/element_matrix.cpp:27-115), with
+// the same accumulation order over quadrature points.
+__device__ void element_blocks(const Geometry& g, const Coeff& c, const Quad& q, bool need_phi,
+                               cplx* aa, cplx* ap, cplx* pp) {
+    double curl[6][3];
+    for (int e = 0; e < 6; ++e) {
+        const int vi = c_edge_verts[e][0], vj = c_edge_verts[e][1];
+        const double* u = g.grad[vi];
+        const double* v = g.grad[vj];
+        curl[e][0] = __dmul_rn(__dsub_rn(__dmul_rn(u[1], v[2]), __dmul_rn(u[2], v[1])), 2.0);
+        curl[e][1] = __dmul_rn(__dsub_rn(__dmul_rn(u[2], v[0]), __dmul_rn(u[0], v[2])), 2.0);
+        curl[e][2] = __dmul_rn(__dsub_rn(__dmul_rn(u[0], v[1]), __dmul_rn(u[1], v[0])), 2.0);
+    }
+    const double nv = __dmul_rn(c.nu, g.volume);
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) aa[i * 6 + j] = cplx{__dmul_rn(nv, dot3(curl[i], curl[j])), 0.0};
+
+    const bool mass = !(c.alpha.re == 0.0 && c.alpha.im == 0.0);
+    const bool coupling = need_phi && !(c.beta.re == 0.0 && c.beta.im == 0.0);
+    if (need_phi) {
+        for (int i = 0; i < 60; ++i) ap[i] = cplx{0.0, 0.0};
+        for (int i = 0; i < 100; ++i) pp[i] = cplx{0.0, 0.0};
+    }
+    if (!mass && !coupling) return;
+    for (int k = 0; k < 4; ++k) {
+        double L[4];
+        for (int i = 0; i < 4; ++i) L[i] = (i == k) ? q.a : q.b;
+        const double w = __dmul_rn(0.25, g.volume);
+        double wv[6][3];
+        for (int e = 0; e < 6; ++e) whitney(g, e, L, wv[e]);
+        if (mass) {
+            for (int i = 0; i < 6; ++i)
+                for (int j = 0; j < 6; ++j) {
+                    const double s = __dmul_rn(w, dot3(wv[i], wv[j]));
+                    aa[i * 6 + j] = cadd_exact(aa[i * 6 + j], cscale_exact(c.alpha, s));
+                }
+        }
+        if (coupling) {
+            double gr[10][3];
+            for (int b = 0; b < 10; ++b) p2_grad(g, b, L, gr[b]);
+            for (int i = 0; i < 6; ++i)
+                for (int b = 0; b < 10; ++b) {
+                    const double s = __dmul_rn(w, dot3(wv[i], gr[b]));
+                    ap[i * 10 + b] = cadd_exact(ap[i * 10 + b], cscale_exact(c.beta, s));
+                }
+            for (int a = 0; a < 10; ++a)
+                for (int b = 0; b < 10; ++b) {
+                    const double s = __dmul_rn(w, dot3(gr[a], gr[b]));
+                    pp[a * 10 + b] = cadd_exact(pp[a * 10 + b], cscale_exact(c.beta, s));
+                }
+        }
+    }
+}
+
+// Complex division in the order the host runtime uses for finite operands of
+// ordinary magnitude (Smith's method), for the prescribed-value and port
+// scalars: v / c.
+__device__ cplx cdiv_smith(cplx a, cplx b) {
+    if (fabs(b.re) < fabs(b.im)) {
+        const double ratio = __ddiv_rn(b.re, b.im);
+        const double denom = __dadd_rn(__dmul_rn(b.re, ratio), b.im);
+        return cplx{__ddiv_rn(__dadd_rn(__dmul_rn(a.re, ratio), a.im), denom),
+                    __ddiv_rn(__dsub_rn(__dmul_rn(a.im, ratio), a.re), denom)};
+    }
+    const double ratio = __ddiv_rn(b.im, b.re);
+    const double denom = __dadd_rn(b.re, __dmul_rn(b.im, ratio));
+    return cplx{__ddiv_rn(__dadd_rn(a.re, __dmul_rn(a.im, ratio)), denom),
+                __ddiv_rn(__dsub_rn(a.im, __dmul_rn(a.re, ratio)), denom)};
+}
+
+struct Scales {
+    cplx row, col, jw;
+};
+
+// formulation_scales, src/assembly.cpp:12-45 (omega == 0 is refused on the host).
+__device__ Scales scales_of(int cond, double omega) {
+    Scales s;
+    s.jw = cplx{0.0, omega};
+    s.row = cplx{1.0, 0.0};
+    s.col = cplx{1.0, 0.0};
+    if (cond == APHI_COND_ROW_SCALED) s.row = cdiv_smith(cplx{1.0, 0.0}, s.jw);
+    if (cond == APHI_COND_SCALED_PHI) s.col = s.jw;
+    return s;
+}
+
+struct TetArgs {
+    int num_tets;
+    int upper_only;
+    const double* xyz;
+    const int* tets;
+    const int* visit_tet;
+    const int* visit_body;
+    const double* material;
+    const int* tet_idx;
+    const double* tet_coeff;
+    const double* tet_fixed;
+    const long long* term_off;
+    long long stride;  // terms per frequency
+    int* err;          // [0] degenerate tet, [1] term count mismatch
+};
+
+struct Omegas {
+    int n;
+    double w[kMaxBatchOmegas];
+};
+
+__global__ void __launch_bounds__(128) k_tet_terms(TetArgs A, Omegas om, int cond, Quad quad,
+                                                    cplx* terms) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f = blockIdx.y;
+    if (v >= A.num_tets) return;
+    const double omega = om.w[f];
+    const int t = A.visit_tet[v];
+    const int b = A.visit_body[v];
+    const Coeff c = body_coefficients(A.material[3 * b], A.material[3 * b + 1], A.material[3 * b + 2], omega);
+    const Scales sc = scales_of(cond, omega);
+
+    int idx[16];
+    double co[16];
+    bool fixed_nz[10];
+    cplx fixed[10];
+    bool need_phi = false;
+    for (int q = 0; q < 16; ++q) {
+        idx[q] = A.tet_idx[16LL * t + q];
+        co[q] = A.tet_coeff[16LL * t + q];
+    }
+    for (int q = 0; q < 10; ++q) {
+        fixed[q] = cplx{A.tet_fixed[20LL * t + 2 * q], A.tet_fixed[20LL * t + 2 * q + 1]};
+        fixed_nz[q] = !(fixed[q].re == 0.0 && fixed[q].im == 0.0);
+        if (idx[6 + q] >= 0 || fixed_nz[q]) need_phi = true;
+    }
+
+    double p[4][3];
+    for (int q = 0; q < 4; ++q) {
+        const int node = A.tets[4LL * t + q];
+        p[q][0] = A.xyz[3LL * node];
+        p[q][1] = A.xyz[3LL * node + 1];
+        p[q][2] = A.xyz[3LL * node + 2];
+    }
+    Geometry g;
+    if (!tet_geometry(p, g)) {
+        atomicExch(&A.err[0], 1);
+        return;
+    }
+    cplx aa[36], ap[60], pp[100];
+    element_blocks(g, c, quad, need_phi, aa, ap, pp);
+
+    cplx* out = terms + f * A.stride + A.term_off[v];
+    long long k = 0;
+    const bool up = A.upper_only != 0;
+    // (A, A)
+    for (int pi = 0; pi < 6; ++pi) {
+        if (idx[pi] < 0) continue;
+        for (int qi = 0; qi < 6; ++qi) {
+            if (idx[qi] < 0) continue;
+            if (up && idx[qi] < idx[pi]) continue;
+            out[k++] = cscale_exact(aa[pi * 6 + qi], __dmul_rn(co[pi], co[qi]));
+        }
+    }
+    if (need_phi) {
+        const cplx rjw = cmul_exact(sc.row, sc.jw);
+        // (A, Phi) and (Phi, A)
+        for (int pi = 0; pi < 6; ++pi) {
+            if (idx[pi] < 0) continue;
+            for (int qi = 0; qi < 10; ++qi) {
+                const int col = idx[6 + qi];
+                const cplx blk = ap[pi * 10 + qi];
+                if (col >= 0) {
+                    if (!(up && col < idx[pi]))
+                        out[k++] = cmul_exact(cscale_exact(sc.col, __dmul_rn(co[pi], co[6 + qi])), blk);
+                } else if (fixed_nz[qi]) {
+                    const cplx fx = cdiv_smith(fixed[qi], sc.col);
+                    out[k++] = cneg(cmul_exact(cmul_exact(cscale_exact(sc.col, co[pi]), blk), fx));
+                }
+                if (col >= 0) {
+                    if (!(up && idx[pi] < col))
+                        out[k++] = cmul_exact(cscale_exact(rjw, __dmul_rn(co[6 + qi], co[pi])), blk);
+                }
+            }
+        }
+        // (Phi, Phi)
+        const cplx rc = cmul_exact(sc.row, sc.col);
+        for (int pi = 0; pi < 10; ++pi) {
+            const int row = idx[6 + pi];
+            if (row < 0) continue;
+            for (int qi = 0; qi < 10; ++qi) {
+                const int col = idx[6 + qi];
+                const cplx blk = pp[pi * 10 + qi];
+                if (col >= 0) {
+                    if (!(up && col < row))
+                        out[k++] = cmul_exact(cscale_exact(rc, __dmul_rn(co[6 + pi], co[6 + qi])), blk);
+                } else if (fixed_nz[qi]) {
+                    const cplx fx = cdiv_smith(fixed[qi], sc.col);
+                    out[k++] = cneg(cmul_exact(cmul_exact(cscale_exact(rc, co[6 + pi]), blk), fx));
+                }
+            }
+        }
+    }
+    if (k != A.term_off[v + 1] - A.term_off[v]) atomicExch(&A.err[1], 1);
+}
+
+struct PortArgs {
+    int num_ports;
+    const int* current;
+    const double* amplitude;
+    const double* value;
+    long long first_term;  // index of the first port term within a frequency
+    long long stride;
+};
+
+// Port rows, src/assembly.cpp:396-421: a voltage port's unit diagonal and
+// rhs V / c; a current port's rhs r * I. One thread per frequency.
+__global__ void k_port_terms(PortArgs P, Omegas om, int cond, cplx* terms) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= om.n) return;
+    const Scales sc = scales_of(cond, om.w[f]);
+    cplx* out = terms + f * P.stride + P.first_term;
+    int k = 0;
+    for (int p = 0; p < P.num_ports; ++p) {
+        if (P.current[p]) {
+            out[k++] = cmul_exact(sc.row, cplx{P.amplitude[2 * p], P.amplitude[2 * p + 1]});
+        } else {
+            out[k++] = cplx{1.0, 0.0};
+            out[k++] = cdiv_smith(cplx{P.value[2 * p], P.value[2 * p + 1]}, sc.col);
+        }
+    }
+}
+
+// K2: one thread per destination; fixed-order sum of its terms.
+__global__ void __launch_bounds__(256) k_slot_sum(int ndest, int nnz, int n, const int* dest_ptr,
+                                                  const int* dest_terms, const cplx* terms,
+                                                  long long stride, cplx* values, cplx* rhs) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f = blockIdx.y;
+    if (d >= ndest) return;
+    const cplx* tf = terms + f * stride;
+    cplx s{0.0, 0.0};
+    const int e = dest_ptr[d + 1];
+    for (int k = dest_ptr[d]; k < e; ++k) s = cadd_exact(s, tf[dest_terms[k]]);
+    if (d < nnz)
+        values[static_cast<long long>(f) * nnz + d] = s;
+    else
+        rhs[static_cast<long long>(f) * n + (d - nnz)] = s;
+}
+
+// Element blocks for a list of tets (parity hook).
+__global__ void k_element_blocks(int ntets, const double* xyz, Coeff c, Quad q, cplx* aa, cplx* ap,
+                                 cplx* pp, int* err) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntets) return;
+    double p[4][3];
+    for (int i = 0; i < 4; ++i)
+        for (int k = 0; k < 3; ++k) p[i][k] = xyz[12LL * t + 3 * i + k];
+    Geometry g;
+    if (!tet_geometry(p, g)) {
+        atomicExch(err, 1);
+        return;
+    }
+    element_blocks(g, c, q, true, aa + 36LL * t, ap + 60LL * t, pp + 100LL * t);
+}
+
+template <class T>
+T* upload(const T* h, size_t n) {
+    T* d = nullptr;
+    APHI_CUDA(cudaMalloc(&d, std::max<size_t>(n, 1) * sizeof(T)));
+    if (n) APHI_CUDA(cudaMemcpy(d, h, n * sizeof(T), cudaMemcpyHostToDevice));
+    return d;
+}
+
+Quad quad_points() {
+    const double s5 = std::sqrt(5.0);
+    return Quad{(5.0 + 3.0 * s5) / 20.0, (5.0 - s5) / 20.0};
+}
+
+}  // namespace
+
+void assembly_coefficients(double sigma, double eps_r, double mu_r, double omega, double* out5) {
+    const Coeff c = body_coefficients(sigma, eps_r, mu_r, omega);
+    out5[0] = c.nu;
+    out5[1] = c.alpha.re;
+    out5[2] = c.alpha.im;
+    out5[3] = c.beta.re;
+    out5[4] = c.beta.im;
+}
+
+void formulation_scales_host(int cond, double omega, std::complex<double>& row, std::complex<double>& col,
+                             bool& symmetric) {
+    const std::complex<double> jw(0.0, omega);
+    switch (cond) {
+        case APHI_COND_NATURAL:
+            row = col = std::complex<double>(1.0, 0.0);
+            symmetric = false;
+            return;
+        case APHI_COND_ROW_SCALED:
+            if (omega == 0.0)
+                throw Error(APHI_ERR_BAD_SHAPE,
+                            "formulation_scales: the row-scaled formulation divides the Phi rows by "
+                            "j*omega, which is undefined at DC. Use the natural form.");
+            row = std::complex<double>(1.0, 0.0) / jw;
+            col = std::complex<double>(1.0, 0.0);
+            symmetric = true;
+            return;
+        case APHI_COND_SCALED_PHI:
+            if (omega == 0.0)
+                throw Error(APHI_ERR_BAD_SHAPE,
+                            "formulation_scales: the scaled-potential formulation would divide a "
+                            "prescribed potential by j*omega, which is undefined at DC. Use the "
+                            "natural form.");
+            row = std::complex<double>(1.0, 0.0);
+            col = jw;
+            symmetric = true;
+            return;
+    }
+    throw Error(APHI_ERR_BAD_SHAPE, "formulation_scales: unknown formulation");
+}
+
+Assembly::~Assembly() {
+    for (void* p : {(void*)d_xyz, (void*)d_tets, (void*)d_visit_tet, (void*)d_visit_body,
+                    (void*)d_material, (void*)d_tet_idx, (void*)d_tet_coeff, (void*)d_tet_fixed,
+                    (void*)d_term_off, (void*)d_dest_ptr, (void*)d_dest_terms, (void*)d_terms,
+                    (void*)d_port_current, (void*)d_port_amp, (void*)d_port_value, (void*)d_err})
+        if (p) cudaFree(p);
+}
+
+namespace {
+
+int find_slot(const int* row_ptr, const int* col_idx, int r, int c) {
+    const int* b = col_idx + row_ptr[r];
+    const int* e = col_idx + row_ptr[r + 1];
+    const int* it = std::lower_bound(b, e, c);
+    return (it == e || *it != c) ? -1 : static_cast<int>(it - col_idx);
+}
+
+}  // namespace
+
+std::unique_ptr<Assembly> assembly_create(const aphi_assembly_desc& d) {
+    if (d.num_tets < 0 || d.num_unknowns < 0 || d.num_bodies < 1 || !d.row_ptr || !d.col_idx ||
+        !d.tet_idx || !d.tet_coeff || !d.tets || !d.xyz || !d.body_ptr || !d.body_tets || !d.material)
+        throw Error(APHI_ERR_INVALID, "aphi_assembly_create: missing arrays in the description");
+    const int N = d.num_unknowns;
+    const int nnz = d.row_ptr[N];
+    const int T = d.num_tets;
+    if (d.body_ptr[0] != 0 || d.body_ptr[d.num_bodies] != T)
+        throw Error(APHI_ERR_BAD_SHAPE,
+                    "refill: the bodies must partition the tets (body_ptr runs 0 .. num_tets)");
+    for (int p = 0; p < d.num_ports; ++p)
+        if (d.port_row[p] < 0 || d.port_row[p] >= N)
+            throw Error(APHI_ERR_BAD_SHAPE, "refill: a port row lies outside the unknowns");
+
+    auto A = std::make_unique<Assembly>();
+    A->N = N;
+    A->nnz = nnz;
+    A->T = T;
+    A->num_bodies = d.num_bodies;
+    A->num_ports = d.num_ports;
+    A->upper_only = d.upper_only != 0;
+
+    // Visit order and, per tet, the destination of every term in the order
+    // the scatter produces it.
+    std::vector<int> visit_tet(d.body_tets, d.body_tets + T), visit_body(T);
+    for (int b = 0; b < d.num_bodies; ++b)
+        for (int v = d.body_ptr[b]; v < d.body_ptr[b + 1]; ++v) visit_body[v] = b;
+    std::vector<long long> term_off(static_cast<size_t>(T) + 1, 0);
+    std::vector<int> dest;
+    dest.reserve(static_cast<size_t>(T) * 24);
+    const bool up = A->upper_only;
+    auto slot_of = [&](int r, int c) {
+        const int s = find_slot(d.row_ptr, d.col_idx, r, c);
+        if (s < 0)
+            throw Error(APHI_ERR_PATTERN_MISMATCH,
+                        "assemble: no slot for entry (" + std::to_string(r) + ", " + std::to_string(c) +
+                            "). The sparsity pattern and the scatter disagree about the matrix's "
+                            "shape; dropping the term would give a quietly wrong matrix.");
+        return s;
+    };
+    for (int v = 0; v < T; ++v) {
+        const int t = visit_tet[v];
+        if (t < 0 || t >= T) throw Error(APHI_ERR_BAD_SHAPE, "refill: body tet index out of range");
+        const int* idx = d.tet_idx + 16LL * t;
+        const double* fx = d.tet_fixed ? d.tet_fixed + 20LL * t : nullptr;
+        for (int q = 0; q < 16; ++q)
+            if (idx[q] >= N) throw Error(APHI_ERR_BAD_SHAPE, "refill: a DOF index exceeds the unknowns");
+        auto nz = [&](int q) { return fx && (fx[2 * q] != 0.0 || fx[2 * q + 1] != 0.0); };
+        bool need_phi = false;
+        for (int q = 0; q < 10; ++q)
+            if (idx[6 + q] >= 0 || nz(q)) need_phi = true;
+        for (int p = 0; p < 6; ++p) {
+            if (idx[p] < 0) continue;
+            for (int q = 0; q < 6; ++q) {
+                if (idx[q] < 0 || (up && idx[q] < idx[p])) continue;
+                dest.push_back(slot_of(idx[p], idx[q]));
+            }
+        }
+        if (need_phi) {
+            for (int p = 0; p < 6; ++p) {
+                if (idx[p] < 0) continue;
+                for (int q = 0; q < 10; ++q) {
+                    const int col = idx[6 + q];
+                    if (col >= 0) {
+                        if (!(up && col < idx[p])) dest.push_back(slot_of(idx[p], col));
+                    } else if (nz(q)) {
+                        dest.push_back(nnz + idx[p]);
+                    }
+                    if (col >= 0 && !(up && idx[p] < col)) dest.push_back(slot_of(col, idx[p]));
+                }
+            }
+            for (int p = 0; p < 10; ++p) {
+                const int row = idx[6 + p];
+                if (row < 0) continue;
+                for (int q = 0; q < 10; ++q) {
+                    const int col = idx[6 + q];
+                    if (col >= 0) {
+                        if (!(up && col < row)) dest.push_back(slot_of(row, col));
+                    } else if (nz(q)) {
+                        dest.push_back(nnz + row);
+                    }
+                }
+            }
+        }
+        term_off[v + 1] = static_cast<long long>(dest.size());
+    }
+    A->tet_terms = static_cast<long long>(dest.size());
+    std::vector<int> port_current(d.num_ports), h_port(0);
+    for (int p = 0; p < d.num_ports; ++p) {
+        port_current[p] = d.port_current[p] ? 1 : 0;
+        if (port_current[p]) {
+            dest.push_back(nnz + d.port_row[p]);
+        } else {
+            dest.push_back(slot_of(d.port_row[p], d.port_row[p]));
+            dest.push_back(nnz + d.port_row[p]);
+        }
+    }
+    A->num_terms = static_cast<long long>(dest.size());
+    if (A->num_terms >= (1LL << 31))
+        throw Error(APHI_ERR_BAD_SHAPE, "refill: more than 2^31 element terms");
+
+    // Slot -> term lists, stable in term order.
+    const int ndest = nnz + N;
+    std::vector<int> dptr(static_cast<size_t>(ndest) + 1, 0), dterm(dest.size());
+    for (int x : dest) ++dptr[x + 1];
+    for (int i = 0; i < ndest; ++i) dptr[i + 1] += dptr[i];
+    {
+        std::vector<int> cur(dptr.begin(), dptr.end() - 1);
+        for (size_t k = 0; k < dest.size(); ++k) dterm[cur[dest[k]]++] = static_cast<int>(k);
+    }
+
+    A->d_xyz = upload(d.xyz, 3LL * d.num_nodes);
+    A->d_tets = upload(d.tets, 4LL * T);
+    A->d_visit_tet = upload(visit_tet.data(), visit_tet.size());
+    A->d_visit_body = upload(visit_body.data(), visit_body.size());
+    A->d_material = upload(d.material, 3LL * d.num_bodies);
+    A->d_tet_idx = upload(d.tet_idx, 16LL * T);
+    A->d_tet_coeff = upload(d.tet_coeff, 16LL * T);
+    std::vector<double> zeros;
+    if (!d.tet_fixed) zeros.assign(20LL * T, 0.0);
+    A->d_tet_fixed = upload(d.tet_fixed ? d.tet_fixed : zeros.data(), 20LL * T);
+    A->d_term_off = upload(term_off.data(), term_off.size());
+    A->d_dest_ptr = upload(dptr.data(), dptr.size());
+    A->d_dest_terms = upload(dterm.data(), dterm.size());
+    A->d_port_current = upload(port_current.data(), port_current.size());
+    A->d_port_amp = upload(d.port_amplitude, 2LL * d.num_ports);
+    A->d_port_value = upload(d.port_value, 2LL * d.num_ports);
+    A->d_err = upload(std::vector<int>(4, 0).data(), 4);
+    A->bytes = (3LL * d.num_nodes + 16LL * T + 20LL * T) * 8 + (4LL * T + 2LL * T + 16LL * T) * 4 +
+               (T + 1LL) * 8 + (ndest + 1LL + dest.size()) * 4;
+    return A;
+}
+
+void assembly_refill(Assembly& A, int nfreq, const double* omegas, int cond, double* values_dev,
+                     double* rhs_dev, cudaStream_t stream) {
+    if (nfreq < 1) throw Error(APHI_ERR_BAD_SHAPE, "refill: no frequency given");
+    for (int f = 0; f < nfreq; ++f) {
+        std::complex<double> r, c;
+        bool sym = false;
+        formulation_scales_host(cond, omegas[f], r, c, sym);
+        if (A.upper_only && !sym)
+            throw Error(APHI_ERR_BAD_SHAPE,
+                        "refill: this conditioning does not give a symmetric matrix, so only half of "
+                        "it cannot be stored. Its (Phi,A) block is j*omega times its (A,Phi) block. "
+                        "Use row_scaled or scaled_phi for symmetric storage.");
+    }
+    const int chunk = std::min(nfreq, kMaxBatchOmegas);
+    if (A.terms_capacity < chunk) {
+        if (A.d_terms) APHI_CUDA(cudaFree(A.d_terms));
+        A.d_terms = nullptr;
+        APHI_CUDA(cudaMalloc(&A.d_terms, static_cast<size_t>(chunk) * A.num_terms * sizeof(cplx)));
+        A.terms_capacity = chunk;
+    }
+    TetArgs ta{A.T, A.upper_only ? 1 : 0, A.d_xyz, A.d_tets, A.d_visit_tet, A.d_visit_body,
+               A.d_material, A.d_tet_idx, A.d_tet_coeff, A.d_tet_fixed, A.d_term_off, A.num_terms, A.d_err};
+    PortArgs pa{A.num_ports, A.d_port_current, A.d_port_amp, A.d_port_value, A.tet_terms, A.num_terms};
+    const Quad q = quad_points();
+    for (int f0 = 0; f0 < nfreq; f0 += chunk) {
+        Omegas om{};
+        om.n = std::min(chunk, nfreq - f0);
+        for (int i = 0; i < om.n; ++i) om.w[i] = omegas[f0 + i];
+        cplx* terms = reinterpret_cast<cplx*>(A.d_terms);
+        if (A.T > 0) {
+            dim3 grid(ceil_div(A.T, 128), om.n);
+            k_tet_terms<<<grid, 128, 0, stream>>>(ta, om, cond, q, terms);
+            APHI_CHECK_LAUNCH();
+        }
+        if (A.num_ports > 0) {
+            k_port_terms<<<1, 64, 0, stream>>>(pa, om, cond, terms);
+            APHI_CHECK_LAUNCH();
+        }
+        const int ndest = A.nnz + A.N;
+        dim3 g2(ceil_div(ndest, 256), om.n);
+        k_slot_sum<<<g2, 256, 0, stream>>>(ndest, A.nnz, A.N, A.d_dest_ptr, A.d_dest_terms, terms,
+                                           A.num_terms,
+                                           reinterpret_cast<cplx*>(values_dev) + static_cast<long long>(f0) * A.nnz,
+                                           reinterpret_cast<cplx*>(rhs_dev) + static_cast<long long>(f0) * A.N);
+        APHI_CHECK_LAUNCH();
+    }
+}
+
+void assembly_check_errors(Assembly& A, cudaStream_t stream) {
+    int h[4] = {0, 0, 0, 0};
+    APHI_CUDA(cudaMemcpyAsync(h, A.d_err, sizeof(h), cudaMemcpyDeviceToHost, stream));
+    APHI_CUDA(cudaStreamSynchronize(stream));
+    if (h[0] || h[1]) {
+        APHI_CUDA(cudaMemsetAsync(A.d_err, 0, sizeof(h), stream));
+        if (h[0]) throw Error(APHI_ERR_DEGENERATE_TET, "compute_tet_geometry: degenerate (zero-volume) tet");
+        throw Error(APHI_ERR_PATTERN_MISMATCH, "refill: a tet produced a different number of terms than planned");
+    }
+}
+
+void element_blocks_host(int ntets, const double* xyz, double nu, const double* alpha,
+                         const double* beta, double* aa, double* ap, double* pp) {
+    double* d_xyz = upload(xyz, 12LL * ntets);
+    cplx *d_aa = nullptr, *d_ap = nullptr, *d_pp = nullptr;
+    int* d_err = nullptr;
+    APHI_CUDA(cudaMalloc(&d_aa, 36LL * ntets * sizeof(cplx)));
+    APHI_CUDA(cudaMalloc(&d_ap, 60LL * ntets * sizeof(cplx)));
+    APHI_CUDA(cudaMalloc(&d_pp, 100LL * ntets * sizeof(cplx)));
+    APHI_CUDA(cudaMalloc(&d_err, sizeof(int)));
+    APHI_CUDA(cudaMemset(d_err, 0, sizeof(int)));
+    Coeff c{nu, cplx{alpha[0], alpha[1]}, cplx{beta[0], beta[1]}};
+    k_element_blocks<<<ceil_div(ntets, 64), 64>>>(ntets, d_xyz, c, quad_points(), d_aa, d_ap, d_pp, d_err);
+    APHI_CHECK_LAUNCH();
+    int err = 0;
+    APHI_CUDA(cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    APHI_CUDA(cudaMemcpy(aa, d_aa, 36LL * ntets * sizeof(cplx), cudaMemcpyDeviceToHost));
+    APHI_CUDA(cudaMemcpy(ap, d_ap, 60LL * ntets * sizeof(cplx), cudaMemcpyDeviceToHost));
+    APHI_CUDA(cudaMemcpy(pp, d_pp, 100LL * ntets * sizeof(cplx), cudaMemcpyDeviceToHost));
+    cudaFree(d_xyz);
+    cudaFree(d_aa);
+    cudaFree(d_ap);
+    cudaFree(d_pp);
+    cudaFree(d_err);
+    if (err) throw Error(APHI_ERR_DEGENERATE_TET, "compute_tet_geometry: degenerate (zero-volume) tet");
+}
+
+}  // namespace aphi_b200

@@ -1,0 +1,140 @@
+// C ABI: factors, factorization, solves, residuals, refinement and the
+// whole solve_symmetric pipeline on host buffers.
+#include <chrono>
+#include <cstring>
+#include <vector>
+
+#include "capi_util.hpp"
+#include "factor.hpp"
+
+using namespace aphi_b200;
+
+namespace {
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+}  // namespace
+
+extern "C" {
+
+int aphi_factor_create(const aphi_analysis* an, int precision, int batch, aphi_factor** out) {
+    return guard([&] {
+        if (!out) throw Error(APHI_ERR_INVALID, "aphi_factor_create: null output");
+        *out = factor_create(const_cast<aphi_analysis*>(an), precision, batch);
+    });
+}
+
+int aphi_factor_destroy(aphi_factor* f) {
+    return guard([&] { factor_destroy(f); });
+}
+
+int aphi_factorize(aphi_factor* f, const double* values_dev, int equil_iters, double pivot_floor,
+                   aphi_factor_stats* stats, void* stream) {
+    int rc = APHI_OK;
+    const int g = guard([&] {
+        if (!f) throw Error(APHI_ERR_INVALID, "aphi_factorize: null factor");
+        rc = factorize(f, values_dev, equil_iters, pivot_floor, stats, as_stream(stream));
+        if (rc == APHI_ERR_PIVOT_FLOOR)
+            g_last_error = "factorize_ldlt: a pivot at or below the floor stopped the factorization";
+    });
+    if (g != APHI_OK) return g;
+    return rc;
+}
+
+int aphi_solve(aphi_factor* f, int nrhs, const double* b_dev, double* x_dev, void* stream) {
+    return guard([&] {
+        if (!f || !b_dev || !x_dev) throw Error(APHI_ERR_INVALID, "aphi_solve: null argument");
+        solve(f, nrhs, b_dev, x_dev, as_stream(stream));
+    });
+}
+
+int aphi_factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, double* value,
+                       double* diagonal, double* d_scale) {
+    return guard([&] {
+        if (!f) throw Error(APHI_ERR_INVALID, "aphi_factor_export: null factor");
+        factor_export(f, k, col_ptr, row_index, value, diagonal, d_scale);
+    });
+}
+
+int aphi_residuals(const aphi_analysis* an, int batch, int nrhs, const double* values_dev, const double* x_dev,
+                   const double* b_dev, double* out, void* stream) {
+    return guard([&] {
+        if (!an || !values_dev || !x_dev || !b_dev || !out) throw Error(APHI_ERR_INVALID, "aphi_residuals: null argument");
+        if (batch < 1 || nrhs < 1) throw Error(APHI_ERR_BAD_SHAPE, "aphi_residuals: batch and nrhs must be >= 1");
+        analysis_ensure_device(const_cast<aphi_analysis*>(an));
+        residuals(an, batch, nrhs, values_dev, x_dev, b_dev, out, as_stream(stream));
+    });
+}
+
+int aphi_solve_refined(aphi_factor* f, int nrhs, const double* values_dev, const double* b_dev, double* x_dev,
+                       const aphi_ir_options* opt, int* iters, double* berr, void* stream) {
+    int rc = APHI_OK;
+    const int g = guard([&] {
+        if (!f || !values_dev || !b_dev || !x_dev || !iters || !berr)
+            throw Error(APHI_ERR_INVALID, "aphi_solve_refined: null argument");
+        aphi_ir_options o{10, 1e-14, 0.5};
+        if (opt) o = *opt;
+        rc = solve_refined(f, nrhs, values_dev, b_dev, x_dev, o, iters, berr, as_stream(stream));
+        if (rc == APHI_ERR_IR_STALL) g_last_error = "iterative refinement stalled before reaching the tolerance";
+    });
+    if (g != APHI_OK) return g;
+    return rc;
+}
+
+int aphi_solve_symmetric_host(const aphi_analysis* an_c, const double* values, const double* b, int equil_iters,
+                              double pivot_floor, double* x, double* report) {
+    int rc = APHI_OK;
+    const int g = guard([&] {
+        if (!an_c || !values || !b || !x || !report) throw Error(APHI_ERR_INVALID, "aphi_solve_symmetric_host: null argument");
+        auto* an = const_cast<aphi_analysis*>(an_c);
+        const int n = an->S.n;
+        const long long nnz = an->S.nnz_a;
+        std::memset(report, 0, sizeof(double) * 13);
+        report[3] = report[4] = 1.0;
+        aphi_factor* f = factor_create(an, 64, 1);
+        double *dv = nullptr, *db = nullptr, *dx = nullptr;
+        try {
+            APHI_CUDA(cudaMalloc(&dv, sizeof(double) * 2 * std::max<long long>(nnz, 1)));
+            APHI_CUDA(cudaMalloc(&db, sizeof(double) * 2 * std::max(n, 1)));
+            APHI_CUDA(cudaMalloc(&dx, sizeof(double) * 2 * std::max(n, 1)));
+            APHI_CUDA(cudaMemcpy(dv, values, sizeof(double) * 2 * nnz, cudaMemcpyHostToDevice));
+            APHI_CUDA(cudaMemcpy(db, b, sizeof(double) * 2 * n, cudaMemcpyHostToDevice));
+            aphi_factor_stats st{};
+            rc = factorize(f, dv, equil_iters, pivot_floor, &st, nullptr);
+            report[3] = st.equilibration_min;
+            report[4] = st.equilibration_max;
+            report[5] = st.smallest_pivot;
+            report[6] = st.largest_pivot;
+            report[7] = st.largest_multiplier;
+            report[8] = static_cast<double>(st.nnz);
+            report[9] = st.columns_done;
+            report[11] = st.milliseconds;
+            if (rc == APHI_OK) {
+                const auto s0 = std::chrono::steady_clock::now();
+                solve(f, 1, db, dx, nullptr);
+                APHI_CUDA(cudaDeviceSynchronize());
+                report[12] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - s0).count();
+                double res[2];
+                residuals(an, 1, 1, dv, dx, db, res, nullptr);
+                report[1] = res[1];
+                report[2] = res[0];
+                report[0] = 1.0;
+                APHI_CUDA(cudaMemcpy(x, dx, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost));
+            } else {
+                g_last_error = "factorize_ldlt: a pivot at or below the floor stopped the factorization";
+            }
+        } catch (...) {
+            cudaFree(dv);
+            cudaFree(db);
+            cudaFree(dx);
+            factor_destroy(f);
+            throw;
+        }
+        cudaFree(dv);
+        cudaFree(db);
+        cudaFree(dx);
+        factor_destroy(f);
+    });
+    if (g != APHI_OK) return g;
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,644 @@
+// Host orchestration of the numeric factorization, the solves, the residuals
+// and iterative refinement, plus the memory-bound helper kernels
+// (equilibration, scatter of A into the fronts, permutations, SpMV, norms).
+//
+// Reference: solve_symmetric, src/factorization.cpp:332-398; factorize_ldlt
+// :109-218; solve/solve_in_place :254-313; relative_residual :315-329;
+// backward_error :401-416; compute_symmetric_equilibration,
+// src/equilibration.cpp:94-139.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "factor.hpp"
+#include "factor_kernels.cuh"
+
+namespace aphi_b200 {
+
+namespace {
+
+constexpr int kEqThreads = 256;
+
+// ---------------------------------------------------------------- equilibration
+// |a_ij| d_i d_j contributes to the maxima of BOTH row i and row j
+// (src/equilibration.cpp:101-118): the matrix is stored as its upper
+// triangle. Maxima of non-negative doubles are taken as unsigned integers,
+// which orders them exactly, so the result does not depend on the order in
+// which threads arrive.
+__global__ void k_eq_rowmax(int n, const int* row_ptr, const int* col_idx, const double* values,
+                            long long nnz, const double* d, unsigned long long* rowmax) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y;
+    if (r >= n) return;
+    const double* v = values + 2LL * nnz * b;
+    const double* db = d + static_cast<long long>(n) * b;
+    unsigned long long* mx = rowmax + static_cast<long long>(n) * b;
+    const double dr = db[r];
+    double best = 0.0;
+    for (int k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
+        const int c = col_idx[k];
+        const double mag = hypot(v[2 * k], v[2 * k + 1]) * (dr * db[c]);
+        best = fmax(best, mag);
+        if (c != r) atomicMax(&mx[c], __double_as_longlong(mag));
+    }
+    atomicMax(&mx[r], __double_as_longlong(best));
+}
+
+__global__ void k_eq_update(int n, double* d, unsigned long long* rowmax) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y;
+    if (r >= n) return;
+    const long long at = static_cast<long long>(n) * b + r;
+    const double mx = __longlong_as_double(rowmax[at]);
+    if (mx > 0.0) d[at] *= 1.0 / sqrt(mx);
+    rowmax[at] = 0ULL;
+}
+
+__global__ void k_fill(double* p, long long n, double v) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+// Scaled A entries into their panel slots: L[dest[k]] = a_k d_r d_c.
+template <class R>
+__global__ void k_scatter_a(int n, const int* row_ptr, const int* col_idx, const double* values, long long nnz,
+                            const double* d, const long long* dest, cx<R>* Lb, long long lstride) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y;
+    if (r >= n) return;
+    const double* v = values + 2LL * nnz * b;
+    const double* db = d + static_cast<long long>(n) * b;
+    cx<R>* L = Lb + lstride * b;
+    const double dr = db[r];
+    for (int k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
+        const double s = dr * db[col_idx[k]];
+        L[dest[k]] = cx<R>{static_cast<R>(v[2 * k] * s), static_cast<R>(v[2 * k + 1] * s)};
+    }
+}
+
+// D in the caller's permuted order (complex128), for the host-side stats.
+template <class R>
+__global__ void k_extract_d(Sched S, int ns, const int* ref_of_post, const cx<R>* Lb, long long lstride,
+                            double* dref, int n) {
+    const int s = blockIdx.x;
+    const int b = blockIdx.y;
+    const cx<R>* L = Lb + lstride * b + S.loff[s];
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    for (int j = threadIdx.x; j < w; j += blockDim.x) {
+        const cx<R> v = L[j + static_cast<long long>(j) * m];
+        const int k = ref_of_post[S.first[s] + j];
+        dref[2 * (static_cast<long long>(n) * b + k)] = v.re;
+        dref[2 * (static_cast<long long>(n) * b + k) + 1] = v.im;
+    }
+}
+
+// max |L(i, j)| over the multipliers whose row (in the caller's order) is at
+// most kmax[b] -- the rows the reference had computed when it stopped.
+template <class R>
+__global__ void k_max_multiplier(Sched S, const int* ref_of_post, const cx<R>* Lb, long long lstride,
+                                 const int* kmax, unsigned long long* out) {
+    const int s = blockIdx.x;
+    const int b = blockIdx.y;
+    const cx<R>* L = Lb + lstride * b + S.loff[s];
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int* st = S.structs + S.soff[s];
+    const int lim = kmax[b];
+    double best = 0.0;
+    for (long long e = threadIdx.x; e < static_cast<long long>(m) * w; e += blockDim.x) {
+        const int i = static_cast<int>(e % m), j = static_cast<int>(e / m);
+        if (i <= j) continue;
+        if (ref_of_post[st[i]] > lim) continue;
+        best = fmax(best, cabs_d(L[e]));
+    }
+    atomicMax(&out[b], __double_as_longlong(best));
+}
+
+// y[new] = b[orig] * d[orig]  (permute in, with the equilibration scaling).
+template <class R>
+__global__ void k_permute_in(int n, int nrhs, const int* orig_of_new, const double* dsc, const double* b,
+                             cx<R>* y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int bk = blockIdx.y;  // batch * nrhs + k
+    if (i >= n) return;
+    const int bb = bk / nrhs;
+    const int o = orig_of_new[i];
+    const double s = dsc[static_cast<long long>(n) * bb + o];
+    const double* src = b + 2LL * n * bk;
+    y[static_cast<long long>(n) * bk + i] = cx<R>{static_cast<R>(src[2 * o] * s), static_cast<R>(src[2 * o + 1] * s)};
+}
+
+// x[orig] = y[new] * d[orig]  (permute out, undoing the substitution x = D y).
+template <class R>
+__global__ void k_permute_out(int n, int nrhs, const int* new_of_orig, const double* dsc, const cx<R>* y,
+                              double* x) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    const int bk = blockIdx.y;
+    if (o >= n) return;
+    const int bb = bk / nrhs;
+    const double s = dsc[static_cast<long long>(n) * bb + o];
+    const cx<R> v = y[static_cast<long long>(n) * bk + new_of_orig[o]];
+    x[2LL * n * bk + 2 * o] = static_cast<double>(v.re) * s;
+    x[2LL * n * bk + 2 * o + 1] = static_cast<double>(v.im) * s;
+}
+
+// ---------------------------------------------------------------- residuals
+// r = b - A x on the original upper-stored A (both triangles through the
+// mirrored CSR); per-row partial sums of |r|^2, |b|^2, |x|^2 reduced in a
+// fixed order by k_norms_final.
+__global__ void k_residual(int n, int nrhs, const int* fptr, const int* fcol, const long long* fmap,
+                           const double* values, long long nnz, const double* x, const double* b, double* r_out,
+                           double* partial) {
+    __shared__ double sh[3][256];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int bk = blockIdx.y;
+    const int bb = bk / nrhs;
+    const double* v = values + 2LL * nnz * bb;
+    const double* xb = x + 2LL * n * bk;
+    const double* bb_ = b + 2LL * n * bk;
+    double rr = 0, b2 = 0, x2 = 0;
+    if (i < n) {
+        double ar = 0, ai = 0;
+        for (int k = fptr[i]; k < fptr[i + 1]; ++k) {
+            const long long q = fmap[k];
+            const double vr = v[2 * q], vi = v[2 * q + 1];
+            const double xr = xb[2 * fcol[k]], xi = xb[2 * fcol[k] + 1];
+            ar += vr * xr - vi * xi;
+            ai += vr * xi + vi * xr;
+        }
+        const double er = bb_[2 * i] - ar, ei = bb_[2 * i + 1] - ai;
+        if (r_out) {
+            r_out[2LL * n * bk + 2 * i] = er;
+            r_out[2LL * n * bk + 2 * i + 1] = ei;
+        }
+        rr = er * er + ei * ei;
+        b2 = bb_[2 * i] * bb_[2 * i] + bb_[2 * i + 1] * bb_[2 * i + 1];
+        x2 = xb[2 * i] * xb[2 * i] + xb[2 * i + 1] * xb[2 * i + 1];
+    }
+    sh[0][threadIdx.x] = rr;
+    sh[1][threadIdx.x] = b2;
+    sh[2][threadIdx.x] = x2;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            for (int q = 0; q < 3; ++q) sh[q][threadIdx.x] += sh[q][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 3; ++q) partial[(static_cast<long long>(bk) * gridDim.x + blockIdx.x) * 3 + q] = sh[q][0];
+}
+
+__global__ void k_amax(const double* values, long long nnz, unsigned long long* out) {
+    const long long k = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    const int b = blockIdx.y;
+    if (k >= nnz) return;
+    const double* v = values + 2LL * nnz * b;
+    atomicMax(&out[b], __double_as_longlong(hypot(v[2 * k], v[2 * k + 1])));
+}
+
+// norms[bk] = {||r||, ||b||, ||x||, max|A|}: fixed-order sums of the partials.
+__global__ void k_norms_final(int nblocks, int nrhs, const double* partial, const unsigned long long* amax,
+                              double* norms) {
+    const int bk = blockIdx.x;
+    __shared__ double sh[3][256];
+    double acc[3] = {0, 0, 0};
+    for (int t = threadIdx.x; t < nblocks; t += blockDim.x)
+        for (int q = 0; q < 3; ++q) acc[q] += partial[(static_cast<long long>(bk) * nblocks + t) * 3 + q];
+    for (int q = 0; q < 3; ++q) sh[q][threadIdx.x] = acc[q];
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            for (int q = 0; q < 3; ++q) sh[q][threadIdx.x] += sh[q][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        norms[4 * bk] = sqrt(sh[0][0]);
+        norms[4 * bk + 1] = sqrt(sh[1][0]);
+        norms[4 * bk + 2] = sqrt(sh[2][0]);
+        norms[4 * bk + 3] = __longlong_as_double(amax[bk / nrhs]);
+    }
+}
+
+// x += dx (FP64).
+__global__ void k_axpy(long long len, double* x, const double* dx) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i < len) x[i] += dx[i];
+}
+
+template <class T>
+T* dalloc(size_t n) {
+    T* p = nullptr;
+    APHI_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+    return p;
+}
+
+template <class R>
+void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_t st, int nrhs,
+              cx<R>* y, cx<R>* U) {
+    const aphi_analysis* A = f->an;
+    const Sched S = sched_of(A->d);
+    cx<R>* L = reinterpret_cast<cx<R>*>(f->L);
+    cx<R>* CB = reinterpret_cast<cx<R>*>(f->CB);
+    const long long ls = A->S.stored, cs = A->S.cb_pool;
+    const int smallsm = A->opt.small_front * A->opt.small_front * static_cast<int>(sizeof(cx<R>));
+    for (const Launch& l : plan) {
+        dim3 grid(l.count, f->batch);
+        switch (l.kind) {
+            case K_EXTEND_ADD: k_extend_add<R><<<grid, 256, 0, st>>>(S, l.first, L, CB, ls, cs); break;
+            case K_SMALL: k_small_front<R><<<grid, 256, smallsm, st>>>(S, l.first, L, CB, ls, cs); break;
+            case K_DIAG: k_diag_block<R><<<grid, 128, 0, st>>>(S, l.first, L, ls); break;
+            case K_TRSM: k_panel_trsm<R><<<grid, kTrsmRows, 0, st>>>(S, l.first, L, ls); break;
+            case K_UPDATE:
+                k_update_tile<R><<<grid, 256, 2 * kStep * kTile * sizeof(cx<R>), st>>>(S, l.first, L, CB, ls, cs);
+                break;
+            case K_FWD: k_forward<R><<<grid, 256, 0, st>>>(S, l.first, L, ls, y, U, A->S.n, A->upool, nrhs); break;
+            case K_BWD: k_backward<R><<<grid, 256, 0, st>>>(S, l.first, L, ls, y, A->S.n, nrhs); break;
+        }
+        APHI_CHECK_LAUNCH();
+    }
+}
+
+template <class R>
+void set_smem_limits(int small_front) {
+    static bool done = false;
+    if (done) return;
+    APHI_CUDA(cudaFuncSetAttribute(k_small_front<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   96 * 96 * static_cast<int>(sizeof(cx<R>))));
+    APHI_CUDA(cudaFuncSetAttribute(k_update_tile<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   2 * kStep * kTile * static_cast<int>(sizeof(cx<R>))));
+    (void)small_front;
+    done = true;
+}
+
+template <class R>
+void factorize_numeric(aphi_factor* f, const double* values, cudaStream_t st) {
+    const aphi_analysis* A = f->an;
+    const int n = A->S.n;
+    const dim3 g(ceil_div(std::max(n, 1), 256), f->batch);
+    set_smem_limits<R>(A->opt.small_front);
+    APHI_CUDA(cudaMemsetAsync(f->L, 0, static_cast<size_t>(A->S.stored) * f->batch * f->elem, st));
+    k_scatter_a<R><<<g, 256, 0, st>>>(n, A->d.row_ptr, A->d.col_idx, values, A->S.nnz_a, f->dscale, A->d.a_dest,
+                                      reinterpret_cast<cx<R>*>(f->L), A->S.stored);
+    APHI_CHECK_LAUNCH();
+    run_plan<R>(f, A->plan_factor, st, 0, nullptr, nullptr);
+    k_extract_d<R><<<dim3(A->S.ns, f->batch), 128, 0, st>>>(sched_of(A->d), A->S.ns, A->d.ref_of_post,
+                                                          reinterpret_cast<const cx<R>*>(f->L), A->S.stored,
+                                                          f->dref, n);
+    APHI_CHECK_LAUNCH();
+}
+
+template <class R>
+void solve_numeric(aphi_factor* f, int nrhs, const double* b, double* x, cudaStream_t st) {
+    const aphi_analysis* A = f->an;
+    const int n = A->S.n;
+    if (f->nrhs_cap < nrhs) {
+        if (f->y) cudaFree(f->y);
+        if (f->U) cudaFree(f->U);
+        f->y = f->U = nullptr;
+        APHI_CUDA(cudaMalloc(&f->y, static_cast<size_t>(n) * nrhs * f->batch * sizeof(cx<R>) + 16));
+        APHI_CUDA(cudaMalloc(&f->U, static_cast<size_t>(std::max<long long>(A->upool, 1)) * nrhs * f->batch *
+                                        sizeof(cx<R>)));
+        f->nrhs_cap = nrhs;
+    }
+    cx<R>* y = reinterpret_cast<cx<R>*>(f->y);
+    cx<R>* U = reinterpret_cast<cx<R>*>(f->U);
+    const dim3 g(ceil_div(std::max(n, 1), 256), f->batch * nrhs);
+    k_permute_in<R><<<g, 256, 0, st>>>(n, nrhs, A->d.orig_of_new, f->dscale, b, y);
+    APHI_CHECK_LAUNCH();
+    run_plan<R>(f, A->plan_fwd, st, nrhs, y, U);
+    run_plan<R>(f, A->plan_bwd, st, nrhs, y, U);
+    k_permute_out<R><<<g, 256, 0, st>>>(n, nrhs, A->d.new_of_orig, f->dscale, y, x);
+    APHI_CHECK_LAUNCH();
+}
+
+}  // namespace
+
+aphi_factor* factor_create(aphi_analysis* an, int precision, int batch) {
+    if (!an) throw Error(APHI_ERR_INVALID, "factor: null analysis");
+    if (precision != 64 && precision != 32) throw Error(APHI_ERR_BAD_SHAPE, "factor: precision must be 64 or 32");
+    if (batch < 1) throw Error(APHI_ERR_BAD_SHAPE, "factor: batch must be at least 1");
+    analysis_ensure_device(an);
+    auto* f = new aphi_factor;
+    try {
+        f->an = an;
+        f->precision = precision;
+        f->batch = batch;
+        f->elem = precision == 64 ? 16 : 8;
+        const Symbolic& S = an->S;
+        APHI_CUDA(cudaMalloc(&f->L, static_cast<size_t>(std::max<long long>(S.stored, 1)) * batch * f->elem));
+        APHI_CUDA(cudaMalloc(&f->CB, static_cast<size_t>(std::max<long long>(S.cb_pool, 1)) * batch * f->elem));
+        f->dscale = dalloc<double>(static_cast<size_t>(S.n) * batch);
+        f->rowmax = dalloc<unsigned long long>(static_cast<size_t>(S.n) * batch);
+        f->stats = dalloc<unsigned long long>(4 * static_cast<size_t>(batch));
+        f->dref = dalloc<double>(2 * static_cast<size_t>(S.n) * batch);
+        f->host_stats.assign(batch, aphi_factor_stats{});
+    } catch (...) {
+        delete f;
+        throw;
+    }
+    return f;
+}
+
+void factor_destroy(aphi_factor* f) { delete f; }
+
+int factorize(aphi_factor* f, const double* values, int equil_iters, double pivot_floor,
+              aphi_factor_stats* stats_out, cudaStream_t st) {
+    const aphi_analysis* A = f->an;
+    const Symbolic& S = A->S;
+    const int n = S.n;
+    const int B = f->batch;
+    if (!values) throw Error(APHI_ERR_INVALID, "factorize: null values");
+    if (equil_iters < 0) throw Error(APHI_ERR_BAD_SHAPE, "factorize: negative equilibration iterations");
+    const auto t0 = std::chrono::steady_clock::now();
+    cudaEvent_t e0, e1;
+    APHI_CUDA(cudaEventCreate(&e0));
+    APHI_CUDA(cudaEventCreate(&e1));
+    APHI_CUDA(cudaEventRecord(e0, st));
+
+    // Equilibration (FP64 on the original values).
+    const long long nd = static_cast<long long>(n) * B;
+    k_fill<<<ceil_div(std::max<long long>(nd, 1), 256), 256, 0, st>>>(f->dscale, nd, 1.0);
+    APHI_CHECK_LAUNCH();
+    APHI_CUDA(cudaMemsetAsync(f->rowmax, 0, sizeof(unsigned long long) * std::max<long long>(nd, 1), st));
+    const dim3 g(ceil_div(std::max(n, 1), kEqThreads), B);
+    for (int it = 0; it < equil_iters; ++it) {
+        k_eq_rowmax<<<g, kEqThreads, 0, st>>>(n, A->d.row_ptr, A->d.col_idx, values, S.nnz_a, f->dscale, f->rowmax);
+        k_eq_update<<<g, kEqThreads, 0, st>>>(n, f->dscale, f->rowmax);
+        APHI_CHECK_LAUNCH();
+    }
+    if (f->precision == 64)
+        factorize_numeric<double>(f, values, st);
+    else
+        factorize_numeric<float>(f, values, st);
+    APHI_CUDA(cudaEventRecord(e1, st));
+
+    // Stats, computed as the reference computes them: walk the pivots in its
+    // column order, stop at the first at or below the floor.
+    std::vector<double> dref(2 * static_cast<size_t>(n) * B), dsc(static_cast<size_t>(n) * B);
+    APHI_CUDA(cudaMemcpyAsync(dref.data(), f->dref, dref.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    APHI_CUDA(cudaMemcpyAsync(dsc.data(), f->dscale, dsc.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    APHI_CUDA(cudaStreamSynchronize(st));
+    float ms = 0;
+    APHI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::vector<int> kmax(B, n);
+    bool any_fail = false;
+    for (int b = 0; b < B; ++b) {
+        aphi_factor_stats& s = f->host_stats[b];
+        s = aphi_factor_stats{};
+        s.ok = 1;
+        bool first = true;
+        for (int k = 0; k < n; ++k) {
+            const double* d = &dref[2 * (static_cast<size_t>(n) * b + k)];
+            const double mag = std::hypot(d[0], d[1]);
+            s.largest_pivot = std::max(s.largest_pivot, mag);
+            if (first || mag < s.smallest_pivot) {
+                s.smallest_pivot = mag;
+                first = false;
+            }
+            s.columns_done = k + 1;
+            if (!(mag > pivot_floor)) {
+                s.ok = 0;
+                kmax[b] = k;
+                any_fail = true;
+                break;
+            }
+        }
+        s.nnz = S.nnz_l;
+        s.milliseconds = ms;
+        if (n > 0) {
+            s.equilibration_min = *std::min_element(dsc.begin() + static_cast<long long>(n) * b,
+                                                    dsc.begin() + static_cast<long long>(n) * (b + 1));
+            s.equilibration_max = *std::max_element(dsc.begin() + static_cast<long long>(n) * b,
+                                                    dsc.begin() + static_cast<long long>(n) * (b + 1));
+        } else {
+            s.equilibration_min = s.equilibration_max = 1.0;
+        }
+    }
+    // Largest multiplier, over the rows the reference would have reached.
+    int* d_kmax = dalloc<int>(B);
+    APHI_CUDA(cudaMemcpyAsync(d_kmax, kmax.data(), sizeof(int) * B, cudaMemcpyHostToDevice, st));
+    APHI_CUDA(cudaMemsetAsync(f->stats, 0, sizeof(unsigned long long) * 4 * B, st));
+    if (S.ns > 0) {
+        if (f->precision == 64)
+            k_max_multiplier<double><<<dim3(S.ns, B), 256, 0, st>>>(sched_of(A->d), A->d.ref_of_post,
+                                                                    reinterpret_cast<const cx<double>*>(f->L),
+                                                                    S.stored, d_kmax, f->stats);
+        else
+            k_max_multiplier<float><<<dim3(S.ns, B), 256, 0, st>>>(sched_of(A->d), A->d.ref_of_post,
+                                                                   reinterpret_cast<const cx<float>*>(f->L),
+                                                                   S.stored, d_kmax, f->stats);
+        APHI_CHECK_LAUNCH();
+    }
+    std::vector<unsigned long long> mx(4 * B);
+    APHI_CUDA(cudaMemcpyAsync(mx.data(), f->stats, sizeof(unsigned long long) * 4 * B, cudaMemcpyDeviceToHost, st));
+    APHI_CUDA(cudaStreamSynchronize(st));
+    cudaFree(d_kmax);
+    for (int b = 0; b < B; ++b) {
+        double v;
+        std::memcpy(&v, &mx[b], sizeof(double));
+        f->host_stats[b].largest_multiplier = v;
+        if (stats_out) stats_out[b] = f->host_stats[b];
+    }
+    (void)t0;
+    f->factored = true;
+    return any_fail ? APHI_ERR_PIVOT_FLOOR : APHI_OK;
+}
+
+void solve(aphi_factor* f, int nrhs, const double* b, double* x, cudaStream_t st) {
+    if (!f->factored) throw Error(APHI_ERR_INVALID, "solve: the factor holds no factorization");
+    if (nrhs < 1) throw Error(APHI_ERR_BAD_SHAPE, "solve: nrhs must be at least 1");
+    for (const aphi_factor_stats& s : f->host_stats)
+        if (!s.ok)
+            throw Error(APHI_ERR_ZERO_PIVOT,
+                        "solve_in_place: the factorization stopped at a pivot at or below the floor, so "
+                        "this factor cannot be used.");
+    if (f->precision == 64)
+        solve_numeric<double>(f, nrhs, b, x, st);
+    else
+        solve_numeric<float>(f, nrhs, b, x, st);
+}
+
+void residuals(const aphi_analysis* an, int batch, int nrhs, const double* values, const double* x,
+               const double* b, double* out, cudaStream_t st) {
+    // Uses per-call scratch: residuals are off the hot loop.
+    const int n = an->S.n;
+    const int nb = ceil_div(std::max(n, 1), 256);
+    double* partial = dalloc<double>(static_cast<size_t>(nb) * 3 * batch * nrhs);
+    unsigned long long* amax = dalloc<unsigned long long>(batch);
+    double* norms = dalloc<double>(4 * static_cast<size_t>(batch) * nrhs);
+    APHI_CUDA(cudaMemsetAsync(amax, 0, sizeof(unsigned long long) * batch, st));
+    k_residual<<<dim3(nb, batch * nrhs), 256, 0, st>>>(n, nrhs, an->d.fptr, an->d.fcol, an->d.fmap, values,
+                                                       an->S.nnz_a, x, b, nullptr, partial);
+    k_amax<<<dim3(ceil_div(std::max<long long>(an->S.nnz_a, 1), 256), batch), 256, 0, st>>>(values, an->S.nnz_a, amax);
+    k_norms_final<<<batch * nrhs, 256, 0, st>>>(nb, nrhs, partial, amax, norms);
+    APHI_CHECK_LAUNCH();
+    std::vector<double> h(4 * static_cast<size_t>(batch) * nrhs);
+    APHI_CUDA(cudaMemcpyAsync(h.data(), norms, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    APHI_CUDA(cudaStreamSynchronize(st));
+    cudaFree(partial);
+    cudaFree(amax);
+    cudaFree(norms);
+    for (int q = 0; q < batch * nrhs; ++q) {
+        const double rn = h[4 * q], bn = h[4 * q + 1], xn = h[4 * q + 2], am = h[4 * q + 3];
+        out[2 * q] = bn > 0.0 ? rn / bn : rn;
+        const double den = am * xn + bn;
+        out[2 * q + 1] = den > 0.0 ? rn / den : rn;
+    }
+}
+
+int solve_refined(aphi_factor* f, int nrhs, const double* values, const double* b, double* x,
+                  const aphi_ir_options& opt, int* iters, double* berr, cudaStream_t st) {
+    const aphi_analysis* A = f->an;
+    const int n = A->S.n;
+    const int B = f->batch;
+    const long long len = 2LL * n * nrhs * B;
+    if (f->ir_cap < nrhs) {
+        if (f->ir) cudaFree(f->ir);
+        f->ir = dalloc<double>(static_cast<size_t>(len) * 2);
+        f->ir_cap = nrhs;
+    }
+    double* r = f->ir;
+    double* dx = f->ir + len;
+    const int nb = ceil_div(std::max(n, 1), 256);
+    if (f->red_cap < nrhs) {
+        if (f->red) cudaFree(f->red);
+        if (f->norms) cudaFree(f->norms);
+        f->red = dalloc<double>(static_cast<size_t>(nb) * 3 * B * nrhs + B + 1);
+        f->norms = dalloc<double>(4 * static_cast<size_t>(B) * nrhs);
+        f->red_cap = nrhs;
+    }
+    unsigned long long* amax = reinterpret_cast<unsigned long long*>(f->red + static_cast<size_t>(nb) * 3 * B * nrhs);
+    solve(f, nrhs, b, x, st);
+    APHI_CUDA(cudaMemsetAsync(amax, 0, sizeof(unsigned long long) * B, st));
+    k_amax<<<dim3(ceil_div(std::max<long long>(A->S.nnz_a, 1), 256), B), 256, 0, st>>>(values, A->S.nnz_a, amax);
+    APHI_CHECK_LAUNCH();
+    const int q = B * nrhs;
+    std::vector<double> prev(q, INFINITY), h(4 * static_cast<size_t>(q));
+    std::vector<int> it(q, 0);
+    std::vector<char> done(q, 0);
+    int status = APHI_OK;
+    for (int step = 0;; ++step) {
+        k_residual<<<dim3(nb, q), 256, 0, st>>>(n, nrhs, A->d.fptr, A->d.fcol, A->d.fmap, values, A->S.nnz_a, x, b,
+                                                r, f->red);
+        k_norms_final<<<q, 256, 0, st>>>(nb, nrhs, f->red, amax, f->norms);
+        APHI_CHECK_LAUNCH();
+        APHI_CUDA(cudaMemcpyAsync(h.data(), f->norms, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        APHI_CUDA(cudaStreamSynchronize(st));
+        bool all = true;
+        for (int k = 0; k < q; ++k) {
+            if (done[k]) continue;
+            const double den = h[4 * k + 3] * h[4 * k + 2] + h[4 * k + 1];
+            const double e = den > 0.0 ? h[4 * k] / den : h[4 * k];
+            berr[k] = e;
+            iters[k] = it[k];
+            if (e <= opt.tol) {
+                done[k] = 1;
+                continue;
+            }
+            if (!(e < opt.stall_ratio * prev[k]) || it[k] >= opt.max_iters) {
+                done[k] = 1;
+                status = APHI_ERR_IR_STALL;
+                continue;
+            }
+            prev[k] = e;
+            all = false;
+        }
+        if (all) break;
+        // One correction for every entry (converged ones get a tiny harmless step
+        // from their own residual; their reported error is already frozen).
+        solve(f, nrhs, r, dx, st);
+        k_axpy<<<ceil_div(len, 256), 256, 0, st>>>(len, x, dx);
+        APHI_CHECK_LAUNCH();
+        for (int k = 0; k < q; ++k)
+            if (!done[k]) ++it[k];
+    }
+    return status;
+}
+
+void factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, double* value, double* diagonal,
+                   double* d_scale) {
+    const aphi_analysis* A = f->an;
+    const Symbolic& S = A->S;
+    const int n = S.n;
+    if (k < 0 || k >= f->batch) throw Error(APHI_ERR_BAD_SHAPE, "factor_export: batch index out of range");
+    if (!f->factored) throw Error(APHI_ERR_INVALID, "factor_export: nothing factorized yet");
+    // Panels of entry k, widened to complex128.
+    std::vector<double> Lh(2 * static_cast<size_t>(S.stored));
+    if (f->precision == 64) {
+        APHI_CUDA(cudaMemcpy(Lh.data(), static_cast<const char*>(f->L) + static_cast<size_t>(S.stored) * k * 16,
+                             static_cast<size_t>(S.stored) * 16, cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> tmp(2 * static_cast<size_t>(S.stored));
+        APHI_CUDA(cudaMemcpy(tmp.data(), static_cast<const char*>(f->L) + static_cast<size_t>(S.stored) * k * 8,
+                             static_cast<size_t>(S.stored) * 8, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < tmp.size(); ++i) Lh[i] = tmp[i];
+    }
+    if (d_scale) APHI_CUDA(cudaMemcpy(d_scale, f->dscale + static_cast<size_t>(n) * k, sizeof(double) * n,
+                                      cudaMemcpyDeviceToHost));
+    // L's true column structures in the caller's numbering: row k of L is
+    // what the row-subtree walk from A(k, 0:k-1) visits; rows come out in
+    // increasing k, so each column is ascending.
+    const std::vector<int>& parent = S.ref_parent;
+    std::vector<int> iperm(n);
+    for (int i = 0; i < n; ++i) iperm[S.perm[i]] = i;
+    std::vector<std::vector<int>> earlier(n);
+    for (int r = 0; r < n; ++r)
+        for (int q = A->h_row_ptr[r]; q < A->h_row_ptr[r + 1]; ++q) {
+            const int c = A->h_col_idx[q];
+            if (c == r) continue;
+            const int a = iperm[r], b = iperm[c];
+            earlier[std::max(a, b)].push_back(std::min(a, b));
+        }
+    std::vector<int> cp(n + 1, 0);
+    for (int j = 0; j < n; ++j) cp[j + 1] = cp[j] + S.ref_colcount[j] - 1;
+    std::vector<int> fill(n, 0), mark(n, -1);
+    std::vector<int> rows(cp[n]);
+    for (int r = 0; r < n; ++r) {
+        mark[r] = r;
+        for (int j0 : earlier[r])
+            for (int j = j0; j != -1 && mark[j] != r; j = parent[j]) {
+                mark[j] = r;
+                rows[cp[j] + fill[j]++] = r;
+            }
+    }
+    if (col_ptr) std::copy(cp.begin(), cp.end(), col_ptr);
+    for (int j = 0; j < n; ++j) {
+        const int pj = S.post_of_ref[j];
+        const int s = S.col_snode[pj];
+        const int m = S.sn_rows[s];
+        const int lc = pj - S.sn_first[s];
+        const int* sb = S.structs.data() + S.sn_struct_off[s];
+        const size_t base = static_cast<size_t>(S.sn_loff[s]) + static_cast<size_t>(lc) * m;
+        if (diagonal) {
+            diagonal[2 * j] = Lh[2 * (base + lc)];
+            diagonal[2 * j + 1] = Lh[2 * (base + lc) + 1];
+        }
+        std::sort(rows.begin() + cp[j], rows.begin() + cp[j + 1]);
+        for (int t = cp[j]; t < cp[j + 1]; ++t) {
+            const int r = rows[t];
+            if (row_index) row_index[t] = r;
+            if (value) {
+                const int pr = S.post_of_ref[r];
+                const int* it = std::lower_bound(sb, sb + m, pr);
+                if (it == sb + m || *it != pr) throw Error(APHI_ERR_PATTERN_MISMATCH, "factor_export: entry outside the panel");
+                const size_t at = base + static_cast<size_t>(it - sb);
+                value[2 * t] = Lh[2 * at];
+                value[2 * t + 1] = Lh[2 * at + 1];
+            }
+        }
+    }
+}
+
+}  // namespace aphi_b200
+
+aphi_factor::~aphi_factor() {
+    void* ptrs[] = {L, CB, dscale, rowmax, stats, dref, y, U, ir, red, norms};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+}

@@ -1,0 +1,52 @@
+// Numeric factorization state: batch x (panels + contribution-block pool) in
+// FP64 or FP32 complex, the equilibration vectors, and solve scratch.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "aphi_b200.h"
+#include "analysis.hpp"
+
+struct aphi_factor {
+    aphi_analysis* an = nullptr;
+    int precision = 64;
+    int batch = 1;
+    size_t elem = 16;          // bytes per complex entry
+    void* L = nullptr;         // batch x stored
+    void* CB = nullptr;        // batch x cb_pool
+    double* dscale = nullptr;  // batch x n, original numbering
+    unsigned long long* rowmax = nullptr;  // batch x n (equilibration scratch)
+    unsigned long long* stats = nullptr;   // batch x 4 (max|L| bits, ...)
+    double* dref = nullptr;    // batch x n complex128: D in the reference's permuted order
+    // Solve scratch, grown on demand: y (batch x nrhs x n), U (batch x nrhs x upool).
+    void* y = nullptr;
+    void* U = nullptr;
+    int nrhs_cap = 0;
+    // Refinement scratch (FP64): x, r, d, per batch x nrhs x n; norms.
+    double* ir = nullptr;
+    int ir_cap = 0;
+    double* red = nullptr;     // reduction partials
+    double* norms = nullptr;   // batch x nrhs x 4
+    int red_cap = 0;
+    bool factored = false;
+    std::vector<aphi_factor_stats> host_stats;
+    ~aphi_factor();
+};
+
+namespace aphi_b200 {
+
+aphi_factor* factor_create(aphi_analysis* an, int precision, int batch);
+void factor_destroy(aphi_factor* f);
+int factorize(aphi_factor* f, const double* values_dev, int equil_iters, double pivot_floor,
+              aphi_factor_stats* stats, cudaStream_t stream);
+void solve(aphi_factor* f, int nrhs, const double* b_dev, double* x_dev, cudaStream_t stream);
+void factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, double* value,
+                   double* diagonal, double* d_scale);
+void residuals(const aphi_analysis* an, int batch, int nrhs, const double* values_dev, const double* x_dev,
+               const double* b_dev, double* out, cudaStream_t stream);
+int solve_refined(aphi_factor* f, int nrhs, const double* values_dev, const double* b_dev, double* x_dev,
+                  const aphi_ir_options& opt, int* iters, double* berr, cudaStream_t stream);
+
+}  // namespace aphi_b200

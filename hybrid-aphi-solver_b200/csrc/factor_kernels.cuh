@@ -1,0 +1,420 @@
+// Device kernels of the supernodal multifrontal complex-symmetric LDL^T and
+// its solves, templated on the real type R (double: complex128 factor;
+// float: complex64 factor). No conjugation anywhere: the matrices are complex
+// symmetric (A = A^T), so every product below is a plain transpose product.
+//
+// Front layout. Supernode s owns columns [first, first + w) of the
+// post-ordered matrix and the sorted row structure struct_s (m rows, the
+// first w being its own columns). Its front is m x m; the first w columns
+// live in the panel L_s (m x w, column-major, leading dimension m, inside the
+// factor storage), the trailing (m - w) x (m - w) block -- the contribution
+// block CB_s -- in the CB pool. After factorization the panel holds D on its
+// diagonal and the multipliers below it.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "analysis.hpp"
+#include "common.cuh"
+
+namespace aphi_b200 {
+
+template <class R>
+struct cx {
+    R re, im;
+};
+
+template <class R>
+__device__ __forceinline__ cx<R> operator*(cx<R> a, cx<R> b) {
+    return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <class R>
+__device__ __forceinline__ cx<R> operator+(cx<R> a, cx<R> b) {
+    return {a.re + b.re, a.im + b.im};
+}
+template <class R>
+__device__ __forceinline__ cx<R> operator-(cx<R> a, cx<R> b) {
+    return {a.re - b.re, a.im - b.im};
+}
+// a - b * c
+template <class R>
+__device__ __forceinline__ cx<R> fms(cx<R> a, cx<R> b, cx<R> c) {
+    return {a.re - b.re * c.re + b.im * c.im, a.im - b.re * c.im - b.im * c.re};
+}
+// 1 / d, scaled so that neither component over- nor underflows for ordinary d.
+template <class R>
+__device__ __forceinline__ cx<R> crecip(cx<R> d) {
+    if (fabs(d.re) >= fabs(d.im)) {
+        const R r = d.im / d.re;
+        const R den = d.re + d.im * r;
+        return {R(1) / den, -r / den};
+    }
+    const R r = d.re / d.im;
+    const R den = d.re * r + d.im;
+    return {r / den, R(-1) / den};
+}
+template <class R>
+__device__ __forceinline__ double cabs_d(cx<R> a) {
+    return hypot(static_cast<double>(a.re), static_cast<double>(a.im));
+}
+
+struct Sched {
+    const int* first;
+    const int* rows;
+    const long long* loff;
+    const long long* cboff;
+    const long long* soff;
+    const int* structs;
+    const long long* reloff;
+    const int* rel;
+    const int* child_ptr;
+    const int* child_list;
+    const long long* uoff;
+    const Item* items;
+};
+
+inline Sched sched_of(const DeviceSchedule& d) {
+    return Sched{d.first, d.rows, d.loff, d.cboff, d.soff, d.structs, d.reloff, d.rel,
+                 d.child_ptr, d.child_list, d.uoff, d.items};
+}
+
+// ---------------------------------------------------------------- extend-add
+// Item (s, c0): front columns [c0, c0 + 32) of supernode s. Zeroes the CB
+// columns in that range, then adds every child's contribution block entries
+// that land in it, children in ascending order (a fixed summation order).
+template <class R>
+__global__ void __launch_bounds__(256) k_extend_add(Sched S, long long item0, cx<R>* Lb, cx<R>* CBb,
+                                                    long long lstride, long long cbstride) {
+    const Item it = S.items[item0 + blockIdx.x];
+    const int s = it.s, c0 = it.a;
+    cx<R>* L = Lb + lstride * blockIdx.y;
+    cx<R>* CB = CBb + cbstride * blockIdx.y;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int cs = m - w;
+    const int c1 = min(c0 + kEaCols, m);
+    cx<R>* Ls = L + S.loff[s];
+    cx<R>* CBs = CB + (cs > 0 ? S.cboff[s] : 0);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int j = max(c0, w) + warp; j < c1; j += 8)
+        for (int i = j + lane; i < m; i += 32) CBs[(i - w) + static_cast<long long>(j - w) * cs] = cx<R>{0, 0};
+    __syncthreads();
+    for (int t = S.child_ptr[s]; t < S.child_ptr[s + 1]; ++t) {
+        const int c = S.child_list[t];
+        const int cw = S.first[c + 1] - S.first[c];
+        const int cc = S.rows[c] - cw;
+        if (cc <= 0) continue;
+        const int* rel = S.rel + S.reloff[c];
+        const cx<R>* CBc = CB + S.cboff[c];
+        // Child columns whose parent position falls in [c0, c1): binary search.
+        int lo = 0, hi = cc;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (rel[mid] < c0) lo = mid + 1; else hi = mid;
+        }
+        const int j0 = lo;
+        hi = cc;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (rel[mid] < c1) lo = mid + 1; else hi = mid;
+        }
+        const int j1 = lo;
+        for (int j = j0 + warp; j < j1; j += 8) {
+            const int pj = rel[j];
+            const cx<R>* src = CBc + static_cast<long long>(j) * cc;
+            if (pj < w) {
+                cx<R>* dst = Ls + static_cast<long long>(pj) * m;
+                for (int i = j + lane; i < cc; i += 32) dst[rel[i]] = dst[rel[i]] + src[i];
+            } else {
+                cx<R>* dst = CBs + static_cast<long long>(pj - w) * cs - w;
+                for (int i = j + lane; i < cc; i += 32) dst[rel[i]] = dst[rel[i]] + src[i];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- small fronts
+// One CTA factorizes a whole front (m <= 96) in shared memory.
+template <class R>
+__global__ void __launch_bounds__(256) k_small_front(Sched S, long long item0, cx<R>* Lb, cx<R>* CBb,
+                                                     long long lstride, long long cbstride) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<R>* F = reinterpret_cast<cx<R>*>(smem_raw);
+    const int s = S.items[item0 + blockIdx.x].s;
+    cx<R>* L = Lb + lstride * blockIdx.y;
+    cx<R>* CB = CBb + cbstride * blockIdx.y;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int cs = m - w;
+    cx<R>* Ls = L + S.loff[s];
+    cx<R>* CBs = CB + (cs > 0 ? S.cboff[s] : 0);
+    const int nt = blockDim.x;
+    for (int e = threadIdx.x; e < m * m; e += nt) {
+        const int i = e % m, j = e / m;
+        cx<R> v{0, 0};
+        if (i >= j) v = (j < w) ? Ls[e] : CBs[(i - w) + static_cast<long long>(j - w) * cs];
+        F[e] = v;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = nt >> 5;
+    for (int k = 0; k < w; ++k) {
+        const cx<R> inv = crecip(F[k + k * m]);
+        for (int j = k + 1 + warp; j < m; j += nw) {
+            const cx<R> ljk = F[j + k * m] * inv;
+            for (int i = j + lane; i < m; i += 32) F[i + j * m] = fms(F[i + j * m], F[i + k * m], ljk);
+        }
+        __syncthreads();
+        for (int i = k + 1 + threadIdx.x; i < m; i += nt) F[i + k * m] = F[i + k * m] * inv;
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < m * m; e += nt) {
+        const int i = e % m, j = e / m;
+        if (i < j) continue;
+        if (j < w)
+            Ls[e] = F[e];
+        else
+            CBs[(i - w) + static_cast<long long>(j - w) * cs] = F[e];
+    }
+}
+
+// ---------------------------------------------------------------- blocked fronts
+// Step k0 of a large front: factor the kb x kb diagonal block in place.
+template <class R>
+__global__ void __launch_bounds__(128) k_diag_block(Sched S, long long item0, cx<R>* Lb, long long lstride) {
+    __shared__ cx<R> F[kStep * kStep];
+    const Item it = S.items[item0 + blockIdx.x];
+    const int s = it.s, k0 = it.a;
+    cx<R>* L = Lb + lstride * blockIdx.y;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int kb = min(kStep, w - k0);
+    cx<R>* D = L + S.loff[s] + k0 + static_cast<long long>(k0) * m;
+    for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
+        const int i = e % kb, j = e / kb;
+        F[i + j * kStep] = D[i + static_cast<long long>(j) * m];
+    }
+    __syncthreads();
+    for (int k = 0; k < kb; ++k) {
+        const cx<R> inv = crecip(F[k + k * kStep]);
+        const int rem = kb - k - 1;
+        for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
+            const int i = k + 1 + e % rem, j = k + 1 + e / rem;
+            if (i >= j) F[i + j * kStep] = fms(F[i + j * kStep], F[i + k * kStep], F[j + k * kStep] * inv);
+        }
+        __syncthreads();
+        for (int i = k + 1 + threadIdx.x; i < kb; i += blockDim.x) F[i + k * kStep] = F[i + k * kStep] * inv;
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
+        const int i = e % kb, j = e / kb;
+        if (i >= j) D[i + static_cast<long long>(j) * m] = F[i + j * kStep];
+    }
+}
+
+// Rows row0 .. row0+127 of the panel below the diagonal block of step k0:
+// L21 = A21 L11^-T D^-1, one row per thread.
+template <class R>
+__global__ void __launch_bounds__(kTrsmRows) k_panel_trsm(Sched S, long long item0, cx<R>* Lb, long long lstride) {
+    __shared__ cx<R> T[kStep * kStep];
+    __shared__ cx<R> Dinv[kStep];
+    const Item it = S.items[item0 + blockIdx.x];
+    const int s = it.s, k0 = it.a, row0 = it.b;
+    cx<R>* L = Lb + lstride * blockIdx.y;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int kb = min(kStep, w - k0);
+    cx<R>* P = L + S.loff[s] + static_cast<long long>(k0) * m;  // column k0 of the panel
+    for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
+        const int i = e % kb, j = e / kb;
+        T[i + j * kStep] = P[k0 + i + static_cast<long long>(j) * m];
+    }
+    __syncthreads();
+    if (threadIdx.x < kb) Dinv[threadIdx.x] = crecip(T[threadIdx.x * (kStep + 1)]);
+    __syncthreads();
+    const int i = row0 + threadIdx.x;
+    if (i >= m) return;
+    cx<R> x[kStep];
+#pragma unroll
+    for (int j = 0; j < kStep; ++j)
+        if (j < kb) x[j] = P[i + static_cast<long long>(j) * m];
+#pragma unroll
+    for (int j = 0; j < kStep; ++j) {
+        if (j >= kb) break;
+        cx<R> v = x[j];
+#pragma unroll
+        for (int t = 0; t < kStep; ++t) {
+            if (t >= j) break;
+            v = fms(v, T[j + t * kStep], x[t]);
+        }
+        x[j] = v;
+    }
+#pragma unroll
+    for (int j = 0; j < kStep; ++j)
+        if (j < kb) P[i + static_cast<long long>(j) * m] = x[j] * Dinv[j];
+}
+
+// Trailing update tile (i0, j0) of step k0: F[i, j] -= sum_t L[i,t] D[t] L[j,t]
+// for i >= j >= k0 + kb. Columns below w are panel columns, the rest CB.
+template <class R>
+__global__ void __launch_bounds__(256) k_update_tile(Sched S, long long item0, cx<R>* Lb, cx<R>* CBb,
+                                                     long long lstride, long long cbstride) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<R>* As = reinterpret_cast<cx<R>*>(smem_raw);  // [kStep][kTile], scaled by D
+    cx<R>* Bs = As + kStep * kTile;                  // [kStep][kTile]
+    const Item it = S.items[item0 + blockIdx.x];
+    const int s = it.s, k0 = it.a, i0 = it.b, j0 = it.c;
+    cx<R>* L = Lb + lstride * blockIdx.y;
+    cx<R>* CB = CBb + cbstride * blockIdx.y;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int cs = m - w;
+    const int kb = min(kStep, w - k0);
+    const cx<R>* P = L + S.loff[s] + static_cast<long long>(k0) * m;
+    for (int e = threadIdx.x; e < kStep * kTile; e += blockDim.x) {
+        const int r = e % kTile, t = e / kTile;
+        cx<R> a{0, 0}, b{0, 0};
+        if (t < kb) {
+            const cx<R> d = P[k0 + t + static_cast<long long>(t) * m];
+            if (i0 + r < m) a = P[i0 + r + static_cast<long long>(t) * m] * d;
+            if (j0 + r < m) b = P[j0 + r + static_cast<long long>(t) * m];
+        }
+        As[t * kTile + r] = a;
+        Bs[t * kTile + r] = b;
+    }
+    __syncthreads();
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    cx<R> acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = cx<R>{0, 0};
+    for (int t = 0; t < kb; ++t) {
+        cx<R> av[4], bv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) av[a] = As[t * kTile + tx + 16 * a];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) bv[b] = Bs[t * kTile + ty + 16 * b];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                acc[a][b].re += av[a].re * bv[b].re - av[a].im * bv[b].im;
+                acc[a][b].im += av[a].re * bv[b].im + av[a].im * bv[b].re;
+            }
+    }
+    cx<R>* Ls = L + S.loff[s];
+    cx<R>* CBs = CB + (cs > 0 ? S.cboff[s] : 0);
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        const int j = j0 + ty + 16 * b;
+        if (j >= m) continue;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int i = i0 + tx + 16 * a;
+            if (i >= m || i < j) continue;
+            cx<R>* dst = (j < w) ? Ls + i + static_cast<long long>(j) * m
+                                 : CBs + (i - w) + static_cast<long long>(j - w) * cs;
+            *dst = *dst - acc[a][b];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- solves
+// y, U: per batch entry, nrhs vectors of length n (post-ordered) and upool.
+// Forward: the front vector of s is y[cols of s] plus the children's update
+// vectors (extend-add, children in order); solve with the unit L11, then
+// U_s = (accumulated) - L21 y_s.
+template <class R>
+__global__ void __launch_bounds__(256) k_forward(Sched S, long long item0, const cx<R>* Lb, long long lstride,
+                                                 cx<R>* yb, cx<R>* Ub, int n, long long upool, int nrhs) {
+    const int s = S.items[item0 + blockIdx.x].s;
+    const cx<R>* L = Lb + lstride * blockIdx.y;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int cs = m - w;
+    const int f = S.first[s];
+    const cx<R>* Ls = L + S.loff[s];
+    for (int k = 0; k < nrhs; ++k) {
+        cx<R>* y = yb + (static_cast<long long>(blockIdx.y) * nrhs + k) * n;
+        cx<R>* U = Ub + (static_cast<long long>(blockIdx.y) * nrhs + k) * upool;
+        cx<R>* Us = U + S.uoff[s];
+        for (int i = threadIdx.x; i < cs; i += blockDim.x) Us[i] = cx<R>{0, 0};
+        __syncthreads();
+        for (int t = S.child_ptr[s]; t < S.child_ptr[s + 1]; ++t) {
+            const int c = S.child_list[t];
+            const int cc = S.rows[c] - (S.first[c + 1] - S.first[c]);
+            const int* rel = S.rel + S.reloff[c];
+            const cx<R>* Uc = U + S.uoff[c];
+            for (int i = threadIdx.x; i < cc; i += blockDim.x) {
+                const int p = rel[i];
+                if (p < w) y[f + p] = y[f + p] + Uc[i];
+                else Us[p - w] = Us[p - w] + Uc[i];
+            }
+            __syncthreads();
+        }
+        for (int j = 0; j < w; ++j) {
+            const cx<R> yj = y[f + j];
+            const cx<R>* col = Ls + static_cast<long long>(j) * m;
+            for (int i = j + 1 + threadIdx.x; i < w; i += blockDim.x) y[f + i] = fms(y[f + i], col[i], yj);
+            __syncthreads();
+        }
+        for (int i = threadIdx.x; i < cs; i += blockDim.x) {
+            cx<R> acc = Us[i];
+            for (int j = 0; j < w; ++j) acc = fms(acc, Ls[w + i + static_cast<long long>(j) * m], y[f + j]);
+            Us[i] = acc;
+        }
+        __syncthreads();
+    }
+}
+
+// Backward: x_s = L11^-T (D^-1 y_s - L21^T x[struct rows below]).
+template <class R>
+__global__ void __launch_bounds__(256) k_backward(Sched S, long long item0, const cx<R>* Lb, long long lstride,
+                                                  cx<R>* yb, int n, int nrhs) {
+    __shared__ cx<R> red[8];
+    const int s = S.items[item0 + blockIdx.x].s;
+    const cx<R>* L = Lb + lstride * blockIdx.y;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int f = S.first[s];
+    const cx<R>* Ls = L + S.loff[s];
+    const int* st = S.structs + S.soff[s];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int k = 0; k < nrhs; ++k) {
+        cx<R>* y = yb + (static_cast<long long>(blockIdx.y) * nrhs + k) * n;
+        // z_j = y_j / D_j - sum_{i >= w} L[i, j] x[struct_i], one warp per column.
+        for (int j = warp; j < w; j += 8) {
+            const cx<R>* col = Ls + static_cast<long long>(j) * m;
+            cx<R> acc{0, 0};
+            for (int i = w + lane; i < m; i += 32) acc = acc + col[i] * y[st[i]];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                acc.re += __shfl_xor_sync(0xffffffffu, acc.re, o);
+                acc.im += __shfl_xor_sync(0xffffffffu, acc.im, o);
+            }
+            if (lane == 0) y[f + j] = y[f + j] * crecip(col[j]) - acc;
+        }
+        __syncthreads();
+        for (int j = w - 1; j >= 0; --j) {
+            const cx<R>* col = Ls + static_cast<long long>(j) * m;
+            cx<R> acc{0, 0};
+            for (int i = j + 1 + threadIdx.x; i < w; i += blockDim.x) acc = acc + col[i] * y[f + i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                acc.re += __shfl_xor_sync(0xffffffffu, acc.re, o);
+                acc.im += __shfl_xor_sync(0xffffffffu, acc.im, o);
+            }
+            if (lane == 0) red[warp] = acc;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                cx<R> t{0, 0};
+                for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t = t + red[q];
+                y[f + j] = y[f + j] - t;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+}  // namespace aphi_b200

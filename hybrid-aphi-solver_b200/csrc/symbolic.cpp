@@ -1,0 +1,379 @@
+#include "symbolic.hpp"
+
+#include <algorithm>
+#include <numeric>
+#include <string>
+
+#include "common.cuh"
+
+namespace aphi_b200 {
+
+namespace {
+
+[[noreturn]] void mismatch(const std::string& m) { throw Error(APHI_ERR_PATTERN_MISMATCH, m); }
+
+// CB memory: children's contribution blocks stay alive until their parent
+// has been assembled. Blocks are placed by first fit over the level schedule
+// (a block is live from its own level to its parent's level, inclusive), so
+// the pool is far smaller than the sum of all blocks.
+long long place_blocks(const Symbolic& S, std::vector<long long>& off) {
+    struct Live {
+        long long begin, end;
+        int until;  // last level at which the block is read
+    };
+    std::vector<Live> live;
+    long long top = 0;
+    off.assign(S.ns, -1);
+    for (int L = 0; L < S.num_levels; ++L) {
+        // Blocks read for the last time at an earlier level are free now.
+        live.erase(std::remove_if(live.begin(), live.end(), [&](const Live& b) { return b.until < L; }),
+                   live.end());
+        for (int k = S.level_ptr[L]; k < S.level_ptr[L + 1]; ++k) {
+            const int s = S.level_list[k];
+            const long long w = S.sn_first[s + 1] - S.sn_first[s];
+            const long long c = S.sn_rows[s] - w;
+            if (c <= 0) continue;
+            const long long need = c * c;
+            const int until = S.sn_parent[s] >= 0 ? S.sn_level[S.sn_parent[s]] : L;
+            std::sort(live.begin(), live.end(), [](const Live& a, const Live& b) { return a.begin < b.begin; });
+            long long at = 0;
+            for (const Live& b : live) {
+                if (b.begin - at >= need) break;
+                at = std::max(at, b.end);
+            }
+            // Keep every block 32-entry aligned (512 B for complex128).
+            at = (at + 31) / 32 * 32;
+            for (const Live& b : live)
+                if (at < b.end && b.begin < at + need) at = (std::max(at, b.end) + 31) / 32 * 32;
+            off[s] = at;
+            live.push_back({at, at + need, until});
+            top = std::max(top, at + need);
+        }
+    }
+    return top;
+}
+
+}  // namespace
+
+Symbolic analyze_supernodal(int n, const int* row_ptr, const int* col_idx, const int* perm_in,
+                            const int* parent_in, const int* col_count_in, const aphi_analysis_options& opt) {
+    if (n < 0 || !row_ptr || (!col_idx && n > 0))
+        throw Error(APHI_ERR_INVALID, "analysis: missing pattern");
+    Symbolic S;
+    S.n = n;
+    S.nnz_a = row_ptr[n];
+
+    // Permutation and its inverse.
+    S.perm.resize(n);
+    std::vector<int> iperm(n, -1);
+    for (int k = 0; k < n; ++k) {
+        const int old = perm_in ? perm_in[k] : k;
+        if (old < 0 || old >= n || iperm[old] >= 0)
+            throw Error(APHI_ERR_BAD_SHAPE, "analysis: perm is not a permutation of 0..n-1");
+        S.perm[k] = old;
+        iperm[old] = k;
+    }
+
+    // Earlier neighbours of each permuted row (the strictly lower part).
+    std::vector<int> lo_ptr(n + 1, 0);
+    for (int r = 0; r < n; ++r) {
+        if (row_ptr[r + 1] < row_ptr[r]) throw Error(APHI_ERR_BAD_SHAPE, "analysis: row_ptr decreases");
+        for (int k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
+            const int c = col_idx[k];
+            if (c < 0 || c >= n) throw Error(APHI_ERR_BAD_SHAPE, "analysis: column index out of range");
+            if (c < r) throw Error(APHI_ERR_BAD_SHAPE, "analysis: entry below the diagonal in an upper pattern");
+            if (c == r) continue;
+            ++lo_ptr[std::max(iperm[r], iperm[c]) + 1];
+        }
+    }
+    for (int i = 0; i < n; ++i) lo_ptr[i + 1] += lo_ptr[i];
+    std::vector<int> lo_idx(lo_ptr[n]);
+    {
+        std::vector<int> cur(lo_ptr.begin(), lo_ptr.end() - 1);
+        for (int r = 0; r < n; ++r)
+            for (int k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
+                const int c = col_idx[k];
+                if (c == r) continue;
+                const int a = iperm[r], b = iperm[c];
+                lo_idx[cur[std::max(a, b)]++] = std::min(a, b);
+            }
+    }
+
+    // Elimination tree, path compression through `ancestor`.
+    std::vector<int>& parent = S.ref_parent;
+    parent.assign(n, -1);
+    {
+        std::vector<int> ancestor(n, -1);
+        for (int k = 0; k < n; ++k)
+            for (int t = lo_ptr[k]; t < lo_ptr[k + 1]; ++t) {
+                int i = lo_idx[t];
+                while (i != -1 && i < k) {
+                    const int next = ancestor[i];
+                    ancestor[i] = k;
+                    if (next == -1) parent[i] = k;
+                    i = next;
+                }
+            }
+    }
+    // Column counts from the row subtrees: row k of L is every node met
+    // walking up from each earlier neighbour until a node already marked.
+    std::vector<int>& cc = S.ref_colcount;
+    cc.assign(n, 1);
+    {
+        std::vector<int> mark(n, -1);
+        for (int k = 0; k < n; ++k) {
+            mark[k] = k;
+            for (int t = lo_ptr[k]; t < lo_ptr[k + 1]; ++t)
+                for (int i = lo_idx[t]; i != -1 && mark[i] != k; i = parent[i]) {
+                    mark[i] = k;
+                    ++cc[i];
+                }
+        }
+    }
+    if (parent_in)
+        for (int j = 0; j < n; ++j)
+            if (parent_in[j] != parent[j])
+                mismatch("analysis: the elimination tree handed in differs from this pattern's at column " +
+                         std::to_string(j));
+    if (col_count_in)
+        for (int j = 0; j < n; ++j)
+            if (col_count_in[j] != cc[j])
+                mismatch("analysis: the column counts handed in differ from this pattern's at column " +
+                         std::to_string(j));
+
+    // Post order (children in ascending order, roots ascending).
+    std::vector<int> head(n, -1), next(n, -1);
+    for (int j = n - 1; j >= 0; --j)
+        if (parent[j] >= 0) {
+            next[j] = head[parent[j]];
+            head[parent[j]] = j;
+        }
+    S.post_of_ref.assign(n, -1);
+    S.ref_of_post.assign(n, -1);
+    {
+        int k = 0;
+        std::vector<int> stack;
+        for (int r = 0; r < n; ++r) {
+            if (parent[r] != -1) continue;
+            ++S.num_roots;
+            stack.push_back(r);
+            while (!stack.empty()) {
+                const int p = stack.back();
+                const int c = head[p];
+                if (c == -1) {
+                    stack.pop_back();
+                    S.ref_of_post[k] = p;
+                    S.post_of_ref[p] = k++;
+                } else {
+                    head[p] = next[c];
+                    stack.push_back(c);
+                }
+            }
+        }
+        if (k != n) mismatch("analysis: the elimination tree is not a forest");
+    }
+    S.new_of_orig.resize(n);
+    S.orig_of_new.resize(n);
+    for (int r = 0; r < n; ++r) {
+        S.new_of_orig[r] = S.post_of_ref[iperm[r]];
+        S.orig_of_new[S.new_of_orig[r]] = r;
+    }
+    std::vector<int> pp(n), pcc(n), nchild(n, 0);
+    for (int j = 0; j < n; ++j) {
+        const int q = S.post_of_ref[j];
+        pp[q] = parent[j] < 0 ? -1 : S.post_of_ref[parent[j]];
+        pcc[q] = cc[j];
+    }
+    for (int j = 0; j < n; ++j)
+        if (pp[j] >= 0) ++nchild[pp[j]];
+    for (int j = 0; j < n; ++j) {
+        S.nnz_l += pcc[j];
+        const double c = pcc[j] - 1;
+        S.flops += 8.0 * c * (c + 1) / 2;
+    }
+
+    // Fundamental supernodes.
+    std::vector<int> ffirst;
+    for (int j = 0; j < n; ++j)
+        if (!(j > 0 && pp[j - 1] == j && pcc[j - 1] == pcc[j] + 1 && nchild[j] == 1)) ffirst.push_back(j);
+    const int nf = static_cast<int>(ffirst.size());
+    ffirst.push_back(n);
+    std::vector<int> fsn(n);
+    for (int s = 0; s < nf; ++s)
+        for (int j = ffirst[s]; j < ffirst[s + 1]; ++j) fsn[j] = s;
+
+    // Relaxed amalgamation: a supernode absorbs the supernode ending just
+    // before it when that one is its child and the padding stays small.
+    struct Cur {
+        int first, width;
+        long long rows, nz;
+    };
+    std::vector<Cur> cur;
+    for (int s = 0; s < nf; ++s) {
+        Cur c{ffirst[s], ffirst[s + 1] - ffirst[s], pcc[ffirst[s]], 0};
+        for (int j = ffirst[s]; j < ffirst[s + 1]; ++j) c.nz += pcc[j];
+        while (!cur.empty()) {
+            const Cur& q = cur.back();
+            const int ql = q.first + q.width - 1;
+            if (ql + 1 != c.first || pp[ql] < c.first || pp[ql] >= c.first + c.width) break;
+            const long long w = q.width + c.width;
+            const long long m = q.width + c.rows;
+            const long long stored = w * m - w * (w - 1) / 2;
+            const double zeros = static_cast<double>(stored - q.nz - c.nz) / static_cast<double>(stored);
+            const bool ok = w <= opt.relax_max_width &&
+                            (w <= opt.relax_small || (w <= 16 && zeros < 0.8) ||
+                             (w <= 48 && zeros < 0.1) || zeros < opt.relax_fill);
+            if (!ok) break;
+            c = Cur{q.first, static_cast<int>(w), m, q.nz + c.nz};
+            cur.pop_back();
+        }
+        cur.push_back(c);
+    }
+    S.ns = static_cast<int>(cur.size());
+    const int ns = S.ns;
+    S.sn_first.resize(ns + 1);
+    for (int s = 0; s < ns; ++s) S.sn_first[s] = cur[s].first;
+    S.sn_first[ns] = n;
+    S.col_snode.resize(n);
+    for (int s = 0; s < ns; ++s)
+        for (int j = S.sn_first[s]; j < S.sn_first[s + 1]; ++j) S.col_snode[j] = s;
+    S.sn_parent.assign(ns, -1);
+    for (int s = 0; s < ns; ++s) {
+        const int l = S.sn_first[s + 1] - 1;
+        S.sn_parent[s] = pp[l] < 0 ? -1 : S.col_snode[pp[l]];
+    }
+
+    // Lower column lists of A in post-ordered numbering.
+    std::vector<int> acol_ptr(n + 1, 0);
+    for (int r = 0; r < n; ++r)
+        for (int k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
+            const int a = S.new_of_orig[r], b = S.new_of_orig[col_idx[k]];
+            if (a != b) ++acol_ptr[std::min(a, b) + 1];
+        }
+    for (int j = 0; j < n; ++j) acol_ptr[j + 1] += acol_ptr[j];
+    std::vector<int> acol(acol_ptr[n]);
+    {
+        std::vector<int> c2(acol_ptr.begin(), acol_ptr.end() - 1);
+        for (int r = 0; r < n; ++r)
+            for (int k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
+                const int a = S.new_of_orig[r], b = S.new_of_orig[col_idx[k]];
+                if (a != b) acol[c2[std::min(a, b)]++] = std::max(a, b);
+            }
+    }
+
+    // Children lists (ascending), then structures bottom-up.
+    S.child_ptr.assign(ns + 1, 0);
+    for (int s = 0; s < ns; ++s)
+        if (S.sn_parent[s] >= 0) ++S.child_ptr[S.sn_parent[s] + 1];
+    for (int s = 0; s < ns; ++s) S.child_ptr[s + 1] += S.child_ptr[s];
+    S.child_list.resize(S.child_ptr[ns]);
+    {
+        std::vector<int> c2(S.child_ptr.begin(), S.child_ptr.end() - 1);
+        for (int s = 0; s < ns; ++s)
+            if (S.sn_parent[s] >= 0) S.child_list[c2[S.sn_parent[s]]++] = s;
+    }
+    S.sn_rows.assign(ns, 0);
+    S.sn_struct_off.assign(ns + 1, 0);
+    std::vector<int> mark(n, -1), rows;
+    S.structs.clear();
+    for (int s = 0; s < ns; ++s) {
+        const int f = S.sn_first[s], l = S.sn_first[s + 1] - 1;
+        rows.clear();
+        for (int j = f; j <= l; ++j) {
+            rows.push_back(j);
+            mark[j] = s;
+        }
+        for (int j = f; j <= l; ++j)
+            for (int t = acol_ptr[j]; t < acol_ptr[j + 1]; ++t) {
+                const int i = acol[t];
+                if (i > l && mark[i] != s) {
+                    mark[i] = s;
+                    rows.push_back(i);
+                }
+            }
+        for (int t = S.child_ptr[s]; t < S.child_ptr[s + 1]; ++t) {
+            const int c = S.child_list[t];
+            for (long long q = S.sn_struct_off[c]; q < S.sn_struct_off[c + 1]; ++q) {
+                const int i = S.structs[q];
+                if (i > l && mark[i] != s) {
+                    mark[i] = s;
+                    rows.push_back(i);
+                }
+            }
+        }
+        std::sort(rows.begin() + (l - f + 1), rows.end());
+        S.sn_rows[s] = static_cast<int>(rows.size());
+        if (S.sn_rows[s] < pcc[f])
+            mismatch("analysis: a supernode's structure is smaller than its first column's count");
+        S.structs.insert(S.structs.end(), rows.begin(), rows.end());
+        S.sn_struct_off[s + 1] = static_cast<long long>(S.structs.size());
+    }
+    for (int s = 0; s < ns; ++s) {
+        const int w = S.sn_first[s + 1] - S.sn_first[s];
+        S.max_rows = std::max(S.max_rows, S.sn_rows[s]);
+        S.max_width = std::max(S.max_width, w);
+    }
+
+    // Panel offsets; each panel starts on a 32-entry (512 B) boundary.
+    S.sn_loff.assign(ns + 1, 0);
+    for (int s = 0; s < ns; ++s) {
+        const long long w = S.sn_first[s + 1] - S.sn_first[s];
+        S.sn_loff[s + 1] = S.sn_loff[s] + (static_cast<long long>(S.sn_rows[s]) * w + 31) / 32 * 32;
+    }
+    S.stored = S.sn_loff[ns];
+
+    // Extend-add maps: each CB row of child c -> its position in the parent's structure.
+    S.rel_off.assign(ns + 1, 0);
+    for (int s = 0; s < ns; ++s) {
+        const int w = S.sn_first[s + 1] - S.sn_first[s];
+        S.rel_off[s + 1] = S.rel_off[s] + (S.sn_parent[s] >= 0 ? S.sn_rows[s] - w : 0);
+    }
+    S.rel.assign(S.rel_off[ns], 0);
+    for (int s = 0; s < ns; ++s) {
+        const int p = S.sn_parent[s];
+        if (p < 0) continue;
+        const int w = S.sn_first[s + 1] - S.sn_first[s];
+        const int* pb = S.structs.data() + S.sn_struct_off[p];
+        const int* pe = S.structs.data() + S.sn_struct_off[p + 1];
+        for (int i = w; i < S.sn_rows[s]; ++i) {
+            const int row = S.structs[S.sn_struct_off[s] + i];
+            const int* it = std::lower_bound(pb, pe, row);
+            if (it == pe || *it != row) mismatch("analysis: a child's row is missing from its parent's structure");
+            S.rel[S.rel_off[s] + (i - w)] = static_cast<int>(it - pb);
+        }
+    }
+
+    // A entries -> panel positions.
+    S.a_dest.resize(S.nnz_a);
+    for (int r = 0; r < n; ++r)
+        for (int k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
+            const int a = S.new_of_orig[r], b = S.new_of_orig[col_idx[k]];
+            const int col = std::min(a, b), row = std::max(a, b);
+            const int s = S.col_snode[col];
+            const int* sb = S.structs.data() + S.sn_struct_off[s];
+            const int* se = S.structs.data() + S.sn_struct_off[s + 1];
+            const int* it = std::lower_bound(sb, se, row);
+            if (it == se || *it != row) mismatch("analysis: an entry of A has no place in L's structure");
+            S.a_dest[k] = S.sn_loff[s] + static_cast<long long>(col - S.sn_first[s]) * S.sn_rows[s] + (it - sb);
+        }
+
+    // Levels.
+    S.sn_level.assign(ns, 0);
+    for (int s = 0; s < ns; ++s)
+        if (S.sn_parent[s] >= 0)
+            S.sn_level[S.sn_parent[s]] = std::max(S.sn_level[S.sn_parent[s]], S.sn_level[s] + 1);
+    S.num_levels = 0;
+    for (int s = 0; s < ns; ++s) S.num_levels = std::max(S.num_levels, S.sn_level[s] + 1);
+    S.level_ptr.assign(S.num_levels + 1, 0);
+    for (int s = 0; s < ns; ++s) ++S.level_ptr[S.sn_level[s] + 1];
+    for (int L = 0; L < S.num_levels; ++L) S.level_ptr[L + 1] += S.level_ptr[L];
+    S.level_list.resize(ns);
+    {
+        std::vector<int> c2(S.level_ptr.begin(), S.level_ptr.end() - 1);
+        for (int s = 0; s < ns; ++s) S.level_list[c2[S.sn_level[s]]++] = s;
+    }
+    S.cb_pool = place_blocks(S, S.sn_cboff);
+    return S;
+}
+
+}  // namespace aphi_b200

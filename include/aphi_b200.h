@@ -1,0 +1,243 @@
+/*
+ * aphi_b200 -- C ABI of the B200 (sm_100a) implementation of the A-Phi
+ * solver's per-frequency numeric hot path.
+ *
+ * Every entry point takes plain pointers and sizes, never throws, and returns
+ * an int status (APHI_OK or one of the APHI_ERR_* codes below); the message of
+ * the last failure on the calling thread is in aphi_last_error(). Complex
+ * numbers are interleaved (re, im) doubles or floats. "dev" pointers are CUDA
+ * device pointers; "stream" is a cudaStream_t passed as void* (NULL = the
+ * legacy default stream).
+ *
+ * The interfaces replaced, in the reference (namespace aphi_solver):
+ *   include/aphi_solver/assembly.hpp       formulation_scales, ScatterMap,
+ *                                          refill (both overloads),
+ *                                          make_symmetric_system, assemble
+ *   include/aphi_solver/factorization.hpp  permuted_lower, factorize_ldlt,
+ *                                          solve_in_place, solve,
+ *                                          relative_residual, backward_error,
+ *                                          solve_symmetric, reconstruct
+ *   include/aphi_solver/equilibration.hpp  compute_symmetric_equilibration
+ *                                          (upper-triangle overload)
+ * Each declaration cites the reference function it stands in for.
+ */
+#ifndef APHI_B200_H
+#define APHI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------
+ * The drop-in C++ layer maps these back onto the reference's conventions:
+ * BAD_SHAPE -> std::invalid_argument, PATTERN_MISMATCH and ZERO_PIVOT ->
+ * std::logic_error, PIVOT_FLOOR -> `return false` with stats.ok == false. */
+#define APHI_OK 0
+#define APHI_ERR_BAD_SHAPE 1        /* sizes/shapes disagree; also refused conditioning */
+#define APHI_ERR_PATTERN_MISMATCH 2 /* symbolic and numeric passes disagree (no slot, ...) */
+#define APHI_ERR_PIVOT_FLOOR 3      /* |D[j]| <= pivot_floor: factorization stopped */
+#define APHI_ERR_NAN 4              /* non-finite value met */
+#define APHI_ERR_IR_STALL 5         /* refinement stalled (FP64 fallback is taken if enabled) */
+#define APHI_ERR_TIMEOUT 6          /* a bounded device wait gave up */
+#define APHI_ERR_OOM 7              /* device allocation failed */
+#define APHI_ERR_ADMISSION 8        /* serving: request rejected by HBM admission */
+#define APHI_ERR_CUDA 9             /* any other CUDA error */
+#define APHI_ERR_ZERO_PIVOT 10      /* a solve met D[j] == 0 */
+#define APHI_ERR_DEGENERATE_TET 11  /* zero-volume tetrahedron */
+#define APHI_ERR_INVALID 12         /* null handle or argument */
+
+const char* aphi_status_string(int status);
+const char* aphi_last_error(void);
+
+/* Conditioning, as include/aphi_solver/problem.hpp:58-62 numbers it. */
+#define APHI_COND_NATURAL 0
+#define APHI_COND_ROW_SCALED 1
+#define APHI_COND_SCALED_PHI 2
+
+/* ---- synthetic workloads --------------------------------------------------
+ * The cylinder-in-box problem generated on the host in the layouts the
+ * device path consumes: n^3 cells x 6 Kuhn tets, conductor within r = 0.2 of
+ * the z axis through (0.5, 0.5), voltage ports v_top on z = 1 and 0 V on
+ * z = 0. Not a reference interface: the reference builds the same inputs
+ * with its mesh, binding, DOF-map and sparsity passes. */
+typedef struct aphi_workload aphi_workload;
+int aphi_workload_cylinder(int cells, double v_top, int full_wave, aphi_workload** out);
+void aphi_workload_free(aphi_workload* w);
+/* sizes[0..9]: nodes, tets, edges, unknowns, nnz_upper, num_a, num_phi,
+ * num_ports, num_bodies, num_terms (0 until an assembly is built) */
+int aphi_workload_sizes(const aphi_workload* w, int64_t* sizes);
+/* Read-only views into the workload's arrays (valid until aphi_workload_free).
+ * name: "xyz" (double, 3/node), "tets" (int, 4/tet), "tet_idx" (int, 16/tet),
+ * "tet_coeff" (double, 16/tet), "tet_fixed" (double, 20/tet), "material"
+ * (double, 3/body), "body_ptr" (int), "body_tets" (int), "port_current",
+ * "port_row" (int), "port_amplitude", "port_value" (double, 2/port),
+ * "row_ptr", "col_idx" (int), "edges" (int, 2/edge), "edge_index",
+ * "phi_index" (int), "tet_edges" (int, 6/tet), "body_of_tet" (int). */
+int aphi_workload_array(const aphi_workload* w, const char* name, const void** data, int64_t* count);
+
+/* ---- assembly: element fill + deterministic scatter -----------------------
+ * Replaces refill(SymmetricSystem&, ...) and refill(AssembledSystem&, ...)
+ * (src/assembly.cpp:453-494, scatter at :255-422), element_coefficients and
+ * the three element kernels (src/element_matrix.cpp:10-115), and
+ * ScatterMap::build (src/assembly.cpp:196-232), whose role here is played by a
+ * slot -> contribution list built once per mesh. */
+typedef struct {
+    int num_nodes, num_tets, num_unknowns;
+    const double* xyz;        /* 3 per node */
+    const int* tets;          /* 4 per tet */
+    const int* tet_idx;       /* 16 per tet: DofMap::local_dofs indices, -1 eliminated */
+    const double* tet_coeff;  /* 16 per tet: orientation signs / 1 */
+    const double* tet_fixed;  /* 20 per tet: prescribed Phi (complex), 0 when none */
+    int num_bodies;
+    const double* material;   /* sigma, eps_r, mu_r per body */
+    const int* body_ptr;      /* num_bodies + 1 */
+    const int* body_tets;     /* tets grouped by body, in the order refill visits them */
+    int num_ports;
+    const int* port_current;  /* 1 = current driven, 0 = voltage driven */
+    const int* port_row;
+    const double* port_amplitude; /* complex, BoundPort::amplitude */
+    const double* port_value;     /* complex, DofMap::port_value */
+    int upper_only;           /* pattern stores only col >= row */
+    const int* row_ptr;       /* num_unknowns + 1 */
+    const int* col_idx;
+} aphi_assembly_desc;
+
+typedef struct aphi_assembly aphi_assembly;
+int aphi_assembly_create(const aphi_assembly_desc* desc, aphi_assembly** out);
+int aphi_assembly_destroy(aphi_assembly* a);
+/* info[0..3]: nnz, unknowns, num_terms, device bytes held */
+int aphi_assembly_info(const aphi_assembly* a, int64_t* info);
+/* Formulation scales r, c (complex, 4 doubles) -- formulation_scales,
+ * src/assembly.cpp:12-45. Returns BAD_SHAPE for row_scaled/scaled_phi at omega == 0. */
+int aphi_formulation_scales(int conditioning, double omega, double* rc, int* symmetric);
+/* One frequency: values_dev[2*nnz], rhs_dev[2*N] are overwritten (cleared, then
+ * accumulated in the reference's order: bodies, tets, AA, A-Phi/Phi-A, Phi-Phi,
+ * then port rows). */
+int aphi_refill(aphi_assembly* a, double omega, int conditioning, double* values_dev,
+                double* rhs_dev, void* stream);
+/* nfreq frequencies in one launch pair: values_dev[nfreq][2*nnz], rhs_dev[nfreq][2*N]. */
+int aphi_refill_batch(aphi_assembly* a, int nfreq, const double* omegas, int conditioning,
+                      double* values_dev, double* rhs_dev, void* stream);
+/* Host-buffer form of aphi_refill (copies in and out inside). */
+int aphi_refill_host(aphi_assembly* a, double omega, int conditioning, double* values,
+                     double* rhs);
+/* Element blocks of ntets tets on the device (test hook for
+ * kernel_AA/APhi/PhiPhi): xyz[12 per tet]; coefficients nu (real), alpha,
+ * beta (complex) shared by all; outputs 36/60/100 complex per tet, host. */
+int aphi_element_blocks(int ntets, const double* xyz, double nu, const double* alpha,
+                        const double* beta, double* aa, double* ap, double* pp);
+/* Element coefficients nu, alpha, beta (5 doubles) -- src/element_matrix.cpp:10-25. */
+void aphi_element_coefficients(double sigma, double eps_r, double mu_r, double omega, double* out5);
+
+/* ---- analysis: supernodal schedule from the reference's symbolic pass -----
+ * Consumes the pattern and the reference's permutation (SolverAnalysis::
+ * permutation, include/aphi_solver/symbolic.hpp:69-92), recomputes the
+ * elimination tree and column counts (checked against the caller's when
+ * given), post-orders the tree, groups columns into relaxed supernodes and
+ * lays out the device factor. */
+typedef struct {
+    int relax_small;       /* always merge a child into its parent when both are at most this wide */
+    double relax_fill;     /* otherwise merge while padded zeros stay below this fraction */
+    int relax_max_width;   /* never grow a supernode past this many columns */
+    int small_front;       /* fronts up to this many rows use the one-CTA kernel */
+} aphi_analysis_options;
+
+typedef struct aphi_analysis aphi_analysis;
+void aphi_analysis_default_options(aphi_analysis_options* o);
+/* perm: new -> old (the reference's Permutation::perm). parent/col_count, when
+ * non-NULL, are the reference's etree and column counts in the same
+ * numbering; a disagreement returns PATTERN_MISMATCH. */
+int aphi_analysis_create(int n, const int* row_ptr, const int* col_idx, const int* perm,
+                         const int* parent, const int* col_count, const aphi_analysis_options* opt,
+                         aphi_analysis** out);
+int aphi_analysis_destroy(aphi_analysis* a);
+/* info[0..11]: n, nnz_upper, nnz_L (incl. diagonal, unpadded), stored
+ * entries (padded), supernodes, levels, max front rows, max supernode width,
+ * flops (real, unpadded: 8 * sum c'(c'+1)/2), CB pool entries, device bytes
+ * per factor (fp64), num roots */
+int aphi_analysis_info(const aphi_analysis* a, double* info);
+/* The elimination tree and column counts the analysis computed, in the
+ * caller's permuted numbering. */
+int aphi_analysis_etree(const aphi_analysis* a, int* parent, int* col_count);
+
+/* ---- numeric factorization, solves and refinement --------------------------
+ * A factor holds `batch` independent factorizations sharing one analysis
+ * (frequency batching). precision: 64 = complex128 throughout (the plain
+ * drop-in), 32 = complex64 factor with tensor-core updates, used with FP64
+ * iterative refinement. */
+#define APHI_PREC_FP64 64
+#define APHI_PREC_FP32 32
+
+typedef struct aphi_factor aphi_factor;
+int aphi_factor_create(const aphi_analysis* an, int precision, int batch, aphi_factor** out);
+int aphi_factor_destroy(aphi_factor* f);
+
+typedef struct {
+    int ok;                    /* FactorStats::ok */
+    int columns_done;          /* FactorStats::columns_done */
+    double smallest_pivot;     /* min |D| over completed columns */
+    double largest_pivot;
+    double largest_multiplier; /* max |L(i,j)| */
+    int64_t nnz;               /* L entries plus D, as the reference counts them */
+    double milliseconds;
+    double equilibration_min, equilibration_max;
+} aphi_factor_stats;
+
+/* Equilibrates (equil_iters Ruiz passes, 0 = none; compute_symmetric_
+ * equilibration, src/equilibration.cpp:94-139), then factorizes
+ * P (D A D) P^T = L Dg L^T with no pivoting and no conjugation
+ * (factorize_ldlt, src/factorization.cpp:109-218). values_dev: batch x nnz
+ * complex128 upper-CSR values in the original numbering. pivot_floor stops a
+ * factorization whose |D[j]| <= floor (the reference's convention). stats: one
+ * per batch entry, may be NULL. Returns PIVOT_FLOOR if any entry stopped. */
+int aphi_factorize(aphi_factor* f, const double* values_dev, int equil_iters, double pivot_floor,
+                   aphi_factor_stats* stats, void* stream);
+/* Solves A x = b for each batch entry: b_dev/x_dev are batch x nrhs x N
+ * complex128 in the original numbering (solve, src/factorization.cpp:296-313
+ * plus the equilibration substitution of solve_symmetric, :385-390). */
+int aphi_solve(aphi_factor* f, int nrhs, const double* b_dev, double* x_dev, void* stream);
+/* Copies batch entry k out in the reference's SymmetricFactor layout
+ * (include/aphi_solver/factorization.hpp:34-42): strictly lower CSC of the
+ * permuted, equilibrated matrix, rows ascending, padding dropped, in the
+ * caller's permutation numbering. Sizes: col_ptr[N+1], row_index and
+ * value[nnz_L - N], diagonal[N]. Any pointer may be NULL. d_scale[N] receives
+ * the equilibration vector when non-NULL. */
+int aphi_factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, double* value,
+                       double* diagonal, double* d_scale);
+
+/* ||A x - b|| / ||b|| and ||A x - b|| / (max|A| ||x|| + ||b||) on the original
+ * upper-stored A, per batch entry and rhs (relative_residual and
+ * backward_error, src/factorization.cpp:315-329 and :401-416).
+ * out: batch x nrhs x 2 doubles (host). */
+int aphi_residuals(const aphi_analysis* an, int batch, int nrhs, const double* values_dev,
+                   const double* x_dev, const double* b_dev, double* out, void* stream);
+
+/* Iterative refinement (new; include/aphi_solver/factorization.hpp:27-30 names
+ * it as future work): x <- x + solve(r), r = b - A x in FP64 on the original
+ * system, until backward error <= tol or max_iters; stall (error not halving)
+ * returns IR_STALL. f may be FP32 or FP64. iters/berr: per batch x rhs, host. */
+typedef struct {
+    int max_iters;
+    double tol;               /* target backward error */
+    double stall_ratio;       /* stall when new_err > stall_ratio * old_err */
+} aphi_ir_options;
+int aphi_solve_refined(aphi_factor* f, int nrhs, const double* values_dev, const double* b_dev,
+                       double* x_dev, const aphi_ir_options* opt, int* iters, double* berr,
+                       void* stream);
+
+/* The whole solve_symmetric pipeline (src/factorization.cpp:332-398) on
+ * host buffers, FP64: equilibrate, factorize, solve, unscale, measure.
+ * report[0..12] as SolveReport: ok, backward_error, residual, equil_min,
+ * equil_max, smallest_pivot, largest_pivot, largest_multiplier, factor_nnz,
+ * columns_done, analyze_ms, factorize_ms, solve_ms. Returns PIVOT_FLOOR (x
+ * untouched) when the factorization stopped. */
+int aphi_solve_symmetric_host(const aphi_analysis* an, const double* values, const double* b,
+                              int equil_iters, double pivot_floor, double* x, double* report);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

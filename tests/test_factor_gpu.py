@@ -1,0 +1,263 @@
+"""Device complex-symmetric LDL^T, solves and residuals against the reference.
+
+The reference's known answers (tests/test_factorization.cpp) and its own
+factorize_ldlt / solve_symmetric on the same matrices and the same analysis:
+factor entries and solutions to <= 1e-10 relative, residuals <= 1e-12."""
+import numpy as np
+import pytest
+import torch
+
+import aphi_b200 as ab
+
+pytestmark = pytest.mark.gpu
+
+SMALL_FRONTS = [96, 8]   # 8 sends every front past 8 rows through the blocked kernels
+
+
+def opts(small_front):
+    o = ab.default_analysis_options()
+    o.small_front = small_front
+    return o
+
+
+def dense_to_upper(a):
+    n = a.shape[0]
+    rp, ci, v = [0], [], []
+    for r in range(n):
+        for c in range(r, n):
+            if a[r, c] != 0 or r == c:
+                ci.append(c)
+                v.append(a[r, c])
+        rp.append(len(ci))
+    return np.array(rp, np.int32), np.array(ci, np.int32), np.array(v, np.complex128)
+
+
+def factor_dense(a, perm=None, small_front=96, equil=0, floor=0.0):
+    rp, ci, v = dense_to_upper(a)
+    an = ab.Analysis(rp, ci, perm, options=opts(small_front))
+    f = ab.Factor(an)
+    vals = torch.from_numpy(v).cuda().unsqueeze(0)
+    ok = f.factorize(vals, equil, floor)
+    return an, f, ok, vals
+
+
+def reconstruct(exp, n):
+    L = np.eye(n, dtype=np.complex128)
+    cp, ri, val = exp["col_ptr"], exp["row_index"], exp["value"]
+    for j in range(n):
+        for t in range(cp[j], cp[j + 1]):
+            L[ri[t], j] = val[t]
+    return L @ np.diag(exp["diagonal"]) @ L.T
+
+
+@pytest.mark.parametrize("small_front", SMALL_FRONTS)
+def test_two_by_two_by_hand(small_front, cuda):
+    """tests/test_factorization.cpp:111-136: [[2,3],[3,5]] = L D L^T with
+    L(1,0) = 3/2, D = [2, 1/2]."""
+    a = np.array([[2, 3], [3, 5]], np.complex128)
+    _, f, ok, _ = factor_dense(a, small_front=small_front)
+    assert ok
+    e = f.export()
+    np.testing.assert_allclose(e["diagonal"], [2, 0.5], rtol=1e-15)
+    np.testing.assert_allclose(e["value"], [1.5], rtol=1e-15)
+    assert list(e["col_ptr"]) == [0, 1, 1] and list(e["row_index"]) == [1]
+
+
+def test_zero_pivot_refused_at_column_one(cuda):
+    """tests/test_factorization.cpp:253-276: [[0,1],[1,0]] is nonsingular but
+    has no LDL^T without pivoting; the factorization stops at column 1."""
+    a = np.array([[0, 1], [1, 0]], np.complex128)
+    _, f, ok, _ = factor_dense(a)
+    assert not ok
+    assert f.stats[0]["ok"] == 0 and f.stats[0]["columns_done"] == 1
+    with pytest.raises(ab.LogicError):
+        f.solve(torch.zeros((1, 2), dtype=torch.complex128, device="cuda"))
+
+
+@pytest.mark.parametrize("small_front", SMALL_FRONTS)
+def test_no_conjugation(small_front, cuda):
+    """A complex symmetric, non-Hermitian matrix reconstructs from L D L^T
+    (transpose, not conjugate transpose) to 1e-14 (test_factorization.cpp:141-167)."""
+    a = np.array([[4 + 1j, 1 - 2j, 0.5j], [1 - 2j, 3 - 1j, 2 + 0j], [0.5j, 2 + 0j, 5 + 3j]])
+    _, f, ok, _ = factor_dense(a, small_front=small_front)
+    assert ok
+    r = reconstruct(f.export(), 3)
+    assert np.abs(r - a).max() <= 1e-14 * np.abs(a).max()
+
+
+def random_symmetric(rng, n, fill=0.12):
+    a = np.zeros((n, n), np.complex128)
+    for i in range(n):
+        for j in range(i + 1, n):
+            if rng.random() < fill:
+                a[i, j] = a[j, i] = rng.normal() + 1j * rng.normal()
+    a += np.diag(rng.normal(size=n) + 1j * rng.normal(size=n) + 6 * n + 0.5j * n)
+    return a
+
+
+@pytest.mark.parametrize("small_front", SMALL_FRONTS)
+def test_random_patterns_match_reference(small_front, cuda, ref_or_skip):
+    """Seeded random patterns n = 6..30 (the shape of test_factorization.cpp:169-213):
+    under the reference's own AMD analysis, L and D agree with factorize_ldlt
+    and L D L^T reconstructs P A P^T to 1e-12."""
+    rng = np.random.default_rng(424242)
+    for trial in range(30):
+        n = int(rng.integers(6, 31))
+        a = random_symmetric(rng, n)
+        rp, ci, v = dense_to_upper(a)
+        ref = ref_or_skip.RefProblem.from_pattern(rp, ci, ordering=2)
+        ref.set_values(v)
+        rf = ref.factorize()
+        an_ref = ref.analysis()
+        an = ab.Analysis(rp, ci, an_ref["perm"], an_ref["parent"], an_ref["col_count"], options=opts(small_front))
+        f = ab.Factor(an)
+        assert f.factorize(torch.from_numpy(v).cuda().unsqueeze(0), 0, 0.0)
+        e = f.export()
+        np.testing.assert_array_equal(e["col_ptr"], rf["col_ptr"])
+        np.testing.assert_array_equal(e["row_index"], rf["row_index"])
+        scale = np.abs(rf["value"]).max() if rf["value"].size else 1.0
+        assert np.abs(e["value"] - rf["value"]).max(initial=0) <= 1e-12 * scale
+        assert np.abs(e["diagonal"] - rf["diagonal"]).max() <= 1e-12 * np.abs(rf["diagonal"]).max()
+        p = an_ref["perm"]
+        pap = a[np.ix_(p, p)]
+        assert np.abs(reconstruct(e, n) - pap).max() <= 1e-12 * np.abs(a).max()
+        st = f.stats[0]
+        assert st["nnz"] == rf["stats"]["nnz"]
+        assert abs(st["largest_multiplier"] - rf["stats"]["largest_multiplier"]) <= 1e-12 * rf["stats"]["largest_multiplier"]
+        assert abs(st["smallest_pivot"] - rf["stats"]["smallest_pivot"]) <= 1e-12 * rf["stats"]["smallest_pivot"]
+
+
+OMEGAS = [2 * np.pi * 50.0, 2 * np.pi * 1e4, 2 * np.pi * 1e6]
+
+
+def spmv_extended(rp, ci, v, x):
+    """A x for the upper-stored A in extended precision (numpy clongdouble)."""
+    n = rp.size - 1
+    vl = v.astype(np.clongdouble)
+    xl = x.astype(np.clongdouble)
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    y = np.zeros(n, np.clongdouble)
+    np.add.at(y, rows, vl * xl[ci])
+    off = ci != rows
+    np.add.at(y, ci[off], vl[off] * xl[rows[off]])
+    return y
+
+
+def refined_solution(factor, rp, ci, v, b, x, steps=6):
+    """x* : x refined with residuals in extended precision and corrections
+    from the FP64 factor -- a reference solution accurate well beyond what a
+    plain FP64 solve of an ill-conditioned system gives."""
+    for _ in range(steps):
+        r = np.array(b.astype(np.clongdouble) - spmv_extended(rp, ci, v, x), np.complex128)
+        dx = factor.solve(torch.from_numpy(r).cuda().unsqueeze(0))[0].cpu().numpy()
+        x = np.array(x.astype(np.clongdouble) + dx.astype(np.clongdouble), np.complex128)
+    return x
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("cells,small_front", [(6, 96), (6, 8), (8, 96), (12, 96), (12, 16)])
+def test_cylinder_solve_symmetric_matches_reference(cells, small_front, cuda, ref_or_skip):
+    """solve_symmetric on the cylinder-in-box (10 Ruiz iterations, the
+    reference's AMD analysis) against the reference's solve_symmetric.
+
+    Residual: <= 1e-12 relative. Solution: within 1e-10 of the reference's
+    wherever the reference's own FP64 answer is that accurate; in general at
+    least as accurate as the reference's, both measured against x*, the
+    extended-precision refined solution. The system's conditioning grows with
+    frequency: at 1 MHz the reference's own answer is ~1e-8 from x*, so no
+    FP64 solver can agree with it to 1e-10 there."""
+    w = ab.Workload.cylinder(cells)
+    asm = ab.Assembly(ab.workload_arrays(w))
+    ref = ref_or_skip.RefProblem.cylinder(cells)
+    an_ref = ref.analysis()
+    an = ab.Analysis(w.row_ptr, w.col_idx, an_ref["perm"], an_ref["parent"], an_ref["col_count"],
+                     options=opts(small_front))
+    for omega in OMEGAS:
+        rv, rb = ref.refill(omega)
+        xr, rep_r = ref.solve_symmetric(rb)
+        ok, x, rep = ab.solve_symmetric(an, rv, rb)
+        assert ok and rep_r["ok"]
+        f = ab.Factor(an)
+        assert f.factorize(torch.from_numpy(rv).cuda().unsqueeze(0))
+        xs = refined_solution(f, w.row_ptr, w.col_idx, rv, rb, x)
+        err_ref = rel(xr, xs)
+        err_mine = rel(x, xs)
+        assert err_mine <= max(1e-10, 2.0 * err_ref), (omega, err_mine, err_ref)
+        assert rel(x, xr) <= 1e-10 + 3.0 * err_ref, (omega, rel(x, xr), err_ref)
+        if err_ref <= 1e-11:
+            assert rel(x, xr) <= 1e-10
+        assert rep["residual"] <= 1e-12 and rep["backward_error"] <= 1e-16
+        assert rep["factor_nnz"] == rep_r["factor_nnz"]
+        assert abs(rep["equilibration_min"] / rep_r["equilibration_min"] - 1) < 1e-12
+        assert abs(rep["equilibration_max"] / rep_r["equilibration_max"] - 1) < 1e-12
+        assert abs(rep["smallest_pivot"] / rep_r["smallest_pivot"] - 1) < 1e-9
+        assert abs(rep["largest_pivot"] / rep_r["largest_pivot"] - 1) < 1e-9
+        # the device refill feeds the same numbers
+        v, b = asm.refill(omega)
+        assert np.array_equal(v[0].cpu().numpy(), rv)
+
+
+def test_batched_factorization_equals_single(cuda, ref_or_skip):
+    """Frequency batching: entries factorized together equal the same entries
+    factorized alone, bit for bit (no reduction order depends on the batch)."""
+    w = ab.Workload.cylinder(8)
+    asm = ab.Assembly(ab.workload_arrays(w))
+    an_ref = ref_or_skip.RefProblem.cylinder(8).analysis()
+    an = ab.Analysis(w.row_ptr, w.col_idx, an_ref["perm"])
+    om = np.geomspace(2 * np.pi * 50, 2 * np.pi * 1e6, 4)
+    vals, rhs = asm.refill(om)
+    fb = ab.Factor(an, batch=4)
+    assert fb.factorize(vals)
+    xb = fb.solve(rhs)
+    for k in (0, 3):
+        f1 = ab.Factor(an)
+        assert f1.factorize(vals[k:k + 1])
+        x1 = f1.solve(rhs[k:k + 1])
+        assert bool((x1[0] == xb[k]).all())
+
+
+def test_multiple_rhs_and_residuals(cuda, ref_or_skip):
+    w = ab.Workload.cylinder(6)
+    asm = ab.Assembly(ab.workload_arrays(w))
+    an_ref = ref_or_skip.RefProblem.cylinder(6).analysis()
+    an = ab.Analysis(w.row_ptr, w.col_idx, an_ref["perm"])
+    vals, rhs = asm.refill(OMEGAS[1])
+    f = ab.Factor(an)
+    assert f.factorize(vals)
+    rng = np.random.default_rng(7)
+    b = torch.from_numpy(rng.normal(size=(1, 5, an.n)) + 1j * rng.normal(size=(1, 5, an.n))).cuda()
+    x = f.solve(b)
+    res = ab.residuals(an, vals, x, b)
+    assert res.shape == (1, 5, 2)
+    assert (res[..., 0] <= 1e-12).all() and (res[..., 1] <= 1e-14).all()
+    for k in range(5):
+        xk = f.solve(b[:, k])
+        assert torch.allclose(xk[0], x[0, k], rtol=0, atol=0)
+
+
+def test_fp32_factor_with_fp64_refinement(cuda, ref_or_skip):
+    """FP32 factor + FP64 refinement reaches the FP64 answer: backward error
+    <= 1e-14 and the solution within 1e-10 of the reference's."""
+    w = ab.Workload.cylinder(8)
+    ref = ref_or_skip.RefProblem.cylinder(8)
+    an_ref = ref.analysis()
+    an = ab.Analysis(w.row_ptr, w.col_idx, an_ref["perm"])
+    asm = ab.Assembly(ab.workload_arrays(w))
+    for omega in OMEGAS:
+        vals, rhs = asm.refill(omega)
+        f = ab.Factor(an, precision=ab.PREC_FP32)
+        assert f.factorize(vals)
+        x, iters, berr, ok = f.solve_refined(vals, rhs, tol=1e-15, max_iters=20)
+        rv, rb = ref.refill(omega)
+        xr, _ = ref.solve_symmetric(rb)
+        f64 = ab.Factor(an)
+        assert f64.factorize(vals)
+        xs = refined_solution(f64, w.row_ptr, w.col_idx, rv, rb, xr)
+        err_ref = rel(xr, xs)
+        err = rel(x[0].cpu().numpy(), xs)
+        assert err <= max(1e-10, 2.0 * err_ref), (omega, err, err_ref, iters, berr)
+        res = ab.residuals(an, vals, x, rhs)
+        assert res[0, 0, 0] <= 1e-12

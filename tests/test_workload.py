@@ -1,0 +1,47 @@
+"""The synthetic workload generator against the reference's own host pipeline
+(build_topology, bind_to_mesh with the tree-cotree gauge, build_dof_map,
+local_dofs, build_sparsity): bit-exact, so the GPU path is fed the same
+matrices the reference assembles. CPU only."""
+import numpy as np
+import pytest
+
+import aphi_b200 as ab
+
+
+@pytest.mark.parametrize("cells", [3, 4, 6, 8, 10])
+def test_cylinder_matches_reference_pipeline(cells, ref_or_skip):
+    w = ab.Workload.cylinder(cells)
+    r = ref_or_skip.RefProblem.cylinder(cells, ordering=-1)
+    assert (w.num_nodes, w.num_tets, w.num_edges) == (r.num_nodes, r.num_tets, r.num_edges)
+    assert (w.num_a, w.num_phi, w.num_ports, w.num_unknowns) == (r.num_a, r.num_phi, r.num_ports, r.n)
+    rp, ci = r.pattern()
+    np.testing.assert_array_equal(w.row_ptr, rp)
+    np.testing.assert_array_equal(w.col_idx, ci)
+    idx, co, fx = r.tet_dofs()
+    np.testing.assert_array_equal(w.tet_idx, idx)
+    np.testing.assert_array_equal(w.tet_coeff, co)
+    np.testing.assert_array_equal(w.tet_fixed, fx)
+
+
+def test_config1_sizes():
+    """6^3 cells: the sizes the reference reports for this problem
+    (1,296 tets, 1,358 unknowns = 1,081 A + 275 Phi + 2 ports, 15,164 stored)."""
+    w = ab.Workload.cylinder(6)
+    assert (w.num_tets, w.num_unknowns, w.num_a, w.num_phi, w.num_ports, w.nnz) == (
+        1296, 1358, 1081, 275, 2, 15164)
+
+
+def test_upper_pattern_well_formed():
+    w = ab.Workload.cylinder(5)
+    rp, ci = w.row_ptr, w.col_idx
+    for r in range(w.num_unknowns):
+        row = ci[rp[r]:rp[r + 1]]
+        assert row.size > 0 and row[0] >= r
+        assert np.all(np.diff(row) > 0)
+
+
+def test_refuses_meshes_without_a_conductor():
+    with pytest.raises(ab.AphiError):
+        ab.Workload.cylinder(0)
+    with pytest.raises(ab.AphiError):
+        ab.Workload.cylinder(2)    # no centroid within r = 0.2: the reference refuses too
