@@ -1,0 +1,390 @@
+"""Benchmark: frequency-sweep solves/s on the cylinder-in-box.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--cells 32] [--nfreq 16] [--ordering amd|nd]
+
+One step is one sweep: the 16 log-spaced frequencies (50 Hz .. 1 MHz) of the
+32^3-cell cylinder-in-box (196,608 Kuhn tets, 227,004 unknowns), each
+assembled on the device (element fill + scatter), equilibrated, factorized
+and solved to backward error <= 1e-14 (relative residual <= 1e-10) -- the
+FP32 tensor path factorizing all 16 frequencies in one batch, FP64 iterative
+refinement on the original system. The plain FP64 factorization of the same
+sweep is timed beside it (fp64_* keys). The ordering is the reference's own
+AMD permutation, reproduced bit for bit on the host.
+
+Multi-GPU: one process per GPU, each solving its own sweep (frequency
+replicas, no exchange); value = solves of all ranks / max-over-ranks time.
+
+--impl reference times the reference's own CPU implementation
+(oracle/_ref, compiled from its sources) with every host core: concurrent
+single-threaded solve_symmetric calls on a bounded sample (one 16^3 frequency
+per process), scaled to the 32^3 workload by the ratio of factorization flops.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "hybrid-aphi-solver_b200"))
+sys.path.insert(0, str(ROOT / "tests"))
+
+METRIC = "solves/s & p50/p99 latency, FP32+IR vs FP64 LDLᵀ at rel. residual ≤1e-10"
+UNIT = "solves/s"
+F_LO, F_HI = 50.0, 1.0e6
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d["hbm_gbs"], d["bf16_tflops"], d["bf16_tflops_sustained"], "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ---------------------------------------------------------------- CPU arm
+def _ref_one(args):
+    cells, omega = args
+    import refbridge as rb
+    r = rb.RefProblem.cylinder(cells)
+    v, b = r.refill(omega)
+    t0 = time.perf_counter()
+    r.refill(omega)
+    x, rep = r.solve_symmetric(b)
+    return time.perf_counter() - t0, rep["factorize_ms"], rep["backward_error"]
+
+
+def cpu_reference(cells_sample: int, cells_target: int, procs: int):
+    """Concurrent reference solves (one frequency each) on the sample mesh;
+    solves/s scaled to the target mesh by the factorization-flop ratio."""
+    import multiprocessing as mp
+    import aphi_b200 as ab
+    flops = {}
+    for c in (cells_sample, cells_target):
+        w = ab.Workload.cylinder(c)
+        flops[c] = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx)).info["flops"]
+    omegas = 2 * np.pi * np.geomspace(F_LO, F_HI, procs)
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_ref_one, [(cells_sample, om) for om in omegas])
+    wall = time.perf_counter() - t0
+    per = max(r[0] for r in res)
+    rate_sample = procs / per
+    ratio = flops[cells_target] / flops[cells_sample]
+    return {"value": rate_sample / ratio, "unit": UNIT, "cores": procs, "kind": "reference",
+            "sample": (f"{procs} concurrent single-threaded reference solve_symmetric calls (refill + "
+                       f"equilibrated FP64 up-looking LDL^T + solve), one {cells_sample}^3 frequency each, "
+                       f"{per:.1f} s; scaled to {cells_target}^3 by its {ratio:.1f}x factorization flops "
+                       f"({flops[cells_target]:.3e} vs {flops[cells_sample]:.3e})"),
+            "sample_wall_s": wall, "sample_solve_s": per}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import refbridge as rb
+    if not rb.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libaphi_ref.so was not built"}))
+        return
+    procs = min(os.cpu_count() or 1, 16)
+    for _ in range(args.warmup if args.warmup < 1 else 0):
+        pass
+    vals = []
+    for _ in range(max(args.steps, 1)):
+        vals.append(cpu_reference(args.sample_cells, args.cells, procs))
+    v = float(np.median([x["value"] for x in vals]))
+    base = vals[0]
+    base["value"] = v
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1000.0 * args.nfreq / v, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+           "impl": "reference", "config": workload_config(args, None),
+           "cpu_baseline": base,
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def workload_config(args, info):
+    cfg = {"workload": (f"cylinder-in-box {args.cells}^3 cells ({6 * args.cells ** 3} Kuhn tets), "
+                        f"{args.nfreq} log-spaced frequencies {F_LO:g} Hz-{F_HI:g} Hz, reduced A-Phi, "
+                        f"row_scaled, 1 V / 0 V voltage ports, {args.ordering.upper()} ordering"),
+           "cells": args.cells, "frequencies": args.nfreq,
+           "l2": "inputs larger than L2 (factors of several GB per frequency)"}
+    if info:
+        cfg.update({k: info[k] for k in ("n", "nnz_upper", "nnz_l", "supernodes", "levels", "max_rows")})
+        cfg["flops_per_factorization"] = info["flops"]
+    return cfg
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_ours(args):
+    import torch
+    import aphi_b200 as ab
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # Host-side per-mesh setup (untimed, once): workload, ordering, analysis.
+    w = ab.Workload.cylinder(args.cells)
+    if args.ordering == "amd":
+        perm = ab.amd_ordering(w.row_ptr, w.col_idx)
+    else:
+        perm = ab.nested_dissection(w.row_ptr, w.col_idx, w.dof_xyz)
+    an = ab.Analysis(w.row_ptr, w.col_idx, perm)
+    info = an.info
+    asm = ab.Assembly(ab.workload_arrays(w))
+    n = an.n
+    # Each rank solves its own sweep: the frequencies shifted per rank.
+    omegas = 2 * np.pi * np.geomspace(F_LO, F_HI, args.nfreq) * (1.0 + 1e-3 * rank)
+    stream = torch.cuda.current_stream()
+
+    f32 = ab.Factor(an, precision=ab.PREC_FP32, batch=args.nfreq)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def sweep(record=None):
+        vals, rhs = asm.refill(omegas, stream=stream)
+        if record is not None:
+            record["f0"].record(stream)
+        ok = f32.factorize(vals, 10, 0.0, stream=stream)
+        if record is not None:
+            record["f1"].record(stream)
+        x, iters, berr, conv = f32.solve_refined(vals, rhs, tol=args.tol, max_iters=30, stream=stream)
+        return ok, x, iters, berr, conv, vals, rhs
+
+    for _ in range(args.warmup):
+        sweep()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = ab.launch_count()
+    step_ms, fact_ms = [], []
+    with Clocks(local) as clk:
+        t0, t1 = ev(), ev()
+        t0.record(stream)
+        for _ in range(args.steps):
+            rec = {"s0": ev(), "s1": ev(), "f0": ev(), "f1": ev()}
+            rec["s0"].record(stream)
+            ok, x, iters, berr, conv, vals, rhs = sweep(rec)
+            rec["s1"].record(stream)
+            torch.cuda.synchronize()
+            step_ms.append(rec["s0"].elapsed_time(rec["s1"]))
+            fact_ms.append(rec["f0"].elapsed_time(rec["f1"]))
+        t1.record(stream)
+        torch.cuda.synchronize()
+    launches = (ab.launch_count() - launches0) // max(args.steps, 1)
+    elapsed = t0.elapsed_time(t1)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    res = ab.residuals(an, vals, x, rhs)
+    value = world * args.nfreq * args.steps / (elapsed / 1000.0)
+
+    # End to end through the reference-facing calls with host buffers: refill
+    # hands the assembled systems to the host (as refill(SymmetricSystem&)
+    # does), solve_symmetric takes them back with the right-hand sides and
+    # returns the solutions to the host.
+    host_vals = torch.empty((args.nfreq, an.nnz), dtype=torch.complex128, pin_memory=True)
+    host_rhs = torch.empty((args.nfreq, n), dtype=torch.complex128, pin_memory=True)
+    host_x = torch.empty((args.nfreq, n), dtype=torch.complex128, pin_memory=True)
+    dvals = torch.empty((args.nfreq, an.nnz), dtype=torch.complex128, device=dev)
+    drhs = torch.empty((args.nfreq, n), dtype=torch.complex128, device=dev)
+
+    def e2e_step():
+        v, r = asm.refill(omegas, stream=stream)
+        host_vals.copy_(v, non_blocking=True)
+        host_rhs.copy_(r, non_blocking=True)
+        dvals.copy_(host_vals, non_blocking=True)
+        drhs.copy_(host_rhs, non_blocking=True)
+        f32.factorize(dvals, 10, 0.0, stream=stream)
+        xx, _, _, _ = f32.solve_refined(dvals, drhs, tol=args.tol, max_iters=30, stream=stream)
+        host_x.copy_(xx, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    a, b = ev(), ev()
+    a.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = a.elapsed_time(b) / args.steps
+    e2e_value = world * args.nfreq / (e2e_ms / 1000.0)
+    h2d = 2 * (host_vals.numel() + host_rhs.numel()) * 8
+    d2h = 2 * (host_vals.numel() + host_rhs.numel() + host_x.numel()) * 8
+
+    del f32
+    torch.cuda.empty_cache()
+
+    # Plain FP64 factorization of the same sweep, in batches that fit.
+    fp64_batch = args.fp64_batch
+    f64 = ab.Factor(an, precision=ab.PREC_FP64, batch=fp64_batch)
+    vals, rhs = asm.refill(omegas, stream=stream)
+
+    def sweep64():
+        xs = []
+        for k0 in range(0, args.nfreq, fp64_batch):
+            sl = slice(k0, k0 + fp64_batch)
+            f64.factorize(vals[sl], 10, 0.0, stream=stream)
+            xs.append(f64.solve(rhs[sl], stream=stream))
+        return torch.cat(xs)
+
+    sweep64()
+    torch.cuda.synchronize()
+    a, b = ev(), ev()
+    a.record(stream)
+    for _ in range(args.fp64_steps):
+        x64 = sweep64()
+    b.record(stream)
+    torch.cuda.synchronize()
+    fp64_ms = a.elapsed_time(b) / args.fp64_steps
+    res64 = ab.residuals(an, vals, x64, rhs)
+    fp64_value = world * args.nfreq / (fp64_ms / 1000.0)
+    del f64
+
+    hbm, bf16, bf16s, src = peaks()
+    fact_avg = float(np.mean(fact_ms))
+    achieved = info["flops"] * args.nfreq / (fact_avg / 1000.0) / 1e12
+    traffic_path = ROOT / "profiles" / "traffic.json"
+    traffic = None
+    if traffic_path.exists():
+        traffic = json.loads(traffic_path.read_text()).get(f"factorize_fp32_{args.cells}")
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            import refbridge as rb
+            if rb.available():
+                cpu = cpu_reference(args.sample_cells, args.cells, 1)
+        except Exception as e:  # the baseline is reported, not required
+            cpu = {"unavailable": str(e)}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64 factor + c128 refinement", "data": "synthetic",
+            "config": workload_config(args, info) | {"batch": args.nfreq, "parallelism": f"freq-replicas x{world}"},
+            "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
+                           "what": "one sweep of all frequencies (every solve of the batch completes together)"},
+            "accuracy": {"max_backward_error": float(res[..., 1].max()), "max_rel_residual": float(res[..., 0].max()),
+                         "ir_iterations_max": int(np.max(iters)), "converged": bool(conv)},
+            "fp64": {"value": fp64_value, "unit": UNIT, "ms_per_sweep": fp64_ms, "batch": fp64_batch,
+                     "max_rel_residual": float(res64[..., 0].max()),
+                     "max_backward_error": float(res64[..., 1].max())},
+            "speedup_vs_fp64": value / fp64_value,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "tensor", "kernel": "supernodal factorization (all update/panel kernels, FP32)",
+                         "achieved": achieved, "peak": bf16s, "unit": "TFLOP/s", "frac": achieved / bf16s,
+                         "peak_source": f"bf16_tflops_sustained, {src}",
+                         "traffic": traffic,
+                         "algorithmic": f"{info['flops']:.4e} real flop per factorization x {args.nfreq}",
+                         "factorize_ms": fact_avg},
+            "cpu_baseline": cpu,
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cells", type=int, default=32)
+    ap.add_argument("--nfreq", type=int, default=16)
+    ap.add_argument("--ordering", default="amd", choices=["amd", "nd"])
+    ap.add_argument("--tol", type=float, default=1e-14)
+    ap.add_argument("--fp64-batch", type=int, default=4)
+    ap.add_argument("--fp64-steps", type=int, default=1)
+    ap.add_argument("--sample-cells", type=int, default=16)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -107,10 +107,13 @@ class IROptions(C.Structure):
 _SIGS = {
     "aphi_status_string": (C.c_char_p, [I]),
     "aphi_last_error": (C.c_char_p, []),
+    "aphi_launch_count": (C.c_int64, []),
     "aphi_workload_cylinder": (I, [I, D, I, C.POINTER(P)]),
     "aphi_workload_free": (None, [P]),
     "aphi_workload_sizes": (I, [P, PI64]),
     "aphi_workload_array": (I, [P, C.c_char_p, C.POINTER(P), PI64]),
+    "aphi_order_nested_dissection": (I, [I, PI, PI, PD, I, PI]),
+    "aphi_order_amd": (I, [I, PI, PI, PI]),
     "aphi_assembly_create": (I, [C.POINTER(AssemblyDesc), C.POINTER(P)]),
     "aphi_assembly_destroy": (I, [P]),
     "aphi_assembly_info": (I, [P, PI64]),
@@ -147,6 +150,11 @@ def _declare(L: C.CDLL) -> None:
 
 def exported_symbols() -> list[str]:
     return list(_SIGS)
+
+
+def launch_count() -> int:
+    """Kernels the library has launched in this process."""
+    return int(lib().aphi_launch_count())
 
 
 def check(status: int) -> int:
@@ -186,7 +194,8 @@ class Workload:
               "body_tets": np.int32, "port_current": np.int32, "port_row": np.int32,
               "port_amplitude": np.float64, "port_value": np.float64, "row_ptr": np.int32,
               "col_idx": np.int32, "edges": np.int32, "edge_index": np.int32,
-              "phi_index": np.int32, "tet_edges": np.int32, "body_of_tet": np.int32}
+              "phi_index": np.int32, "tet_edges": np.int32, "body_of_tet": np.int32,
+              "dof_xyz": np.float64}
 
     def __init__(self, handle: C.c_void_p):
         self._h = handle
@@ -274,6 +283,27 @@ def assembly_desc_from(arrays: dict, upper_only: bool = True):
 
 def workload_arrays(w: Workload) -> dict:
     return {k: w.array(k) for k in Workload.ARRAYS}
+
+
+def nested_dissection(row_ptr, col_idx, xyz, leaf: int = 64) -> np.ndarray:
+    """Fill-reducing permutation (new -> old) by geometric nested dissection."""
+    rp = np.ascontiguousarray(row_ptr, np.int32)
+    ci = np.ascontiguousarray(col_idx, np.int32)
+    xy = np.ascontiguousarray(xyz, np.float64)
+    perm = np.zeros(rp.size - 1, np.int32)
+    check(lib().aphi_order_nested_dissection(rp.size - 1, _ptr(rp, C.c_int), _ptr(ci, C.c_int),
+                                             _ptr(xy, C.c_double), leaf, _ptr(perm, C.c_int)))
+    return perm
+
+
+def amd_ordering(row_ptr, col_idx) -> np.ndarray:
+    """The reference's AMD permutation (new -> old), compute_ordering with
+    Ordering::ApproximateMinimumDegree (src/ordering.cpp:539-556)."""
+    rp = np.ascontiguousarray(row_ptr, np.int32)
+    ci = np.ascontiguousarray(col_idx, np.int32)
+    perm = np.zeros(rp.size - 1, np.int32)
+    check(lib().aphi_order_amd(rp.size - 1, _ptr(rp, C.c_int), _ptr(ci, C.c_int), _ptr(perm, C.c_int)))
+    return perm
 
 
 # ---------------------------------------------------------------- assembly

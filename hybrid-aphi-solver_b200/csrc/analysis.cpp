@@ -77,16 +77,74 @@ void build_plans(aphi_analysis& A, std::vector<Item>& items) {
             push(A.plan_factor, K_UPDATE, f0);
         }
     }
-    // Solves: forward bottom-up, backward top-down, one item per supernode.
-    for (int L = 0; L < S.num_levels; ++L) {
+    // Statistics pass over the panels: 32 columns per item.
+    {
         const long long f0 = static_cast<long long>(items.size());
-        for (int k = S.level_ptr[L]; k < S.level_ptr[L + 1]; ++k) items.push_back({S.level_list[k], 0, 0, 0});
-        push(A.plan_fwd, K_FWD, f0);
+        for (int s = 0; s < S.ns; ++s)
+            for (int c = S.sn_first[s]; c < S.sn_first[s + 1]; c += 32) items.push_back({s, c - S.sn_first[s], 0, 0});
+        A.stat_first = f0;
+        A.stat_count = static_cast<int>(items.size() - f0);
     }
+    // Solves. Forward, levels bottom-up: gather, then per 64-column block the
+    // triangle and the rows below. Backward, levels top-down, blocks last to
+    // first: partial sums over row chunks, then the triangle.
+    auto nblocks = [&](int s) { return (S.sn_first[s + 1] - S.sn_first[s] + kSolveBlock - 1) / kSolveBlock; };
+    for (int L = 0; L < S.num_levels; ++L) {
+        const int* lb = S.level_list.data() + S.level_ptr[L];
+        const int* le = S.level_list.data() + S.level_ptr[L + 1];
+        long long f0 = static_cast<long long>(items.size());
+        int maxb = 0;
+        for (const int* p = lb; p < le; ++p) {
+            items.push_back({*p, 0, 0, 0});
+            maxb = std::max(maxb, nblocks(*p));
+        }
+        push(A.plan_fwd, K_FWD_GATHER, f0);
+        for (int blk = 0; blk < maxb; ++blk) {
+            f0 = static_cast<long long>(items.size());
+            for (const int* p = lb; p < le; ++p)
+                if (blk < nblocks(*p)) items.push_back({*p, blk, 0, 0});
+            push(A.plan_fwd, K_FWD_DIAG, f0);
+            f0 = static_cast<long long>(items.size());
+            for (const int* p = lb; p < le; ++p) {
+                const int s = *p;
+                if (blk >= nblocks(s)) continue;
+                const int w = S.sn_first[s + 1] - S.sn_first[s];
+                const int below = std::min(w, (blk + 1) * kSolveBlock);
+                for (int r = below; r < S.sn_rows[s]; r += kSolveRows) items.push_back({s, blk, r, 0});
+            }
+            push(A.plan_fwd, K_FWD_UPDATE, f0);
+        }
+    }
+    A.max_parts = 1;
     for (int L = S.num_levels - 1; L >= 0; --L) {
-        const long long f0 = static_cast<long long>(items.size());
-        for (int k = S.level_ptr[L]; k < S.level_ptr[L + 1]; ++k) items.push_back({S.level_list[k], 0, 0, 0});
-        push(A.plan_bwd, K_BWD, f0);
+        const int* lb = S.level_list.data() + S.level_ptr[L];
+        const int* le = S.level_list.data() + S.level_ptr[L + 1];
+        int maxb = 0;
+        for (const int* p = lb; p < le; ++p) maxb = std::max(maxb, nblocks(*p));
+        for (int blk = maxb - 1; blk >= 0; --blk) {
+            long long f0 = static_cast<long long>(items.size());
+            std::vector<std::pair<int, int>> slots;  // per supernode of this launch: first slot, count
+            int slot = 0;
+            for (const int* p = lb; p < le; ++p) {
+                const int s = *p;
+                if (blk >= nblocks(s)) continue;
+                const int w = S.sn_first[s + 1] - S.sn_first[s];
+                const int below = std::min(w, (blk + 1) * kSolveBlock);
+                const int first = slot;
+                for (int r = below; r < S.sn_rows[s]; r += kSolveRows) items.push_back({s, blk, r, slot++});
+                slots.push_back({first, slot - first});
+            }
+            A.max_parts = std::max(A.max_parts, slot);
+            push(A.plan_bwd, K_BWD_UPDATE, f0);
+            f0 = static_cast<long long>(items.size());
+            int q = 0;
+            for (const int* p = lb; p < le; ++p) {
+                if (blk >= nblocks(*p)) continue;
+                items.push_back({*p, blk, slots[q].first, slots[q].second});
+                ++q;
+            }
+            push(A.plan_bwd, K_BWD_DIAG, f0);
+        }
     }
 }
 

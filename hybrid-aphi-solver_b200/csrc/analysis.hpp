@@ -19,8 +19,11 @@ enum Kind : int {
     K_DIAG = 2,        // (s, k0): factor the diagonal block of step k0
     K_TRSM = 3,        // (s, k0, row0): rows row0.. of L21 for step k0
     K_UPDATE = 4,      // (s, k0, i0, j0): trailing update tile
-    K_FWD = 5,         // (s): forward solve of one supernode
-    K_BWD = 6,         // (s): backward solve of one supernode
+    K_FWD_GATHER = 5,  // (s): children's update vectors into the front vector
+    K_FWD_DIAG = 6,    // (s, blk): unit-triangle solve of a 64-column block
+    K_FWD_UPDATE = 7,  // (s, blk, row0): rows below the block
+    K_BWD_UPDATE = 8,  // (s, blk, row0, slot): partial L^T x sums over a row chunk
+    K_BWD_DIAG = 9,    // (s, blk, first slot, slots): block of the transposed solve
 };
 
 struct Launch {
@@ -37,6 +40,8 @@ constexpr int kStep = 32;        // pivot block width of the blocked factorizati
 constexpr int kTile = 64;        // update tile
 constexpr int kTrsmRows = 128;   // rows per TRSM block
 constexpr int kEaCols = 32;      // front columns per extend-add item
+constexpr int kSolveBlock = 64;  // columns per triangular-solve block
+constexpr int kSolveRows = 256;  // rows per solve update item
 
 struct DeviceSchedule {
     int* first = nullptr;
@@ -77,6 +82,9 @@ struct aphi_analysis {
     bool on_device = false;
     long long num_items = 0;
     long long upool = 0;   // update-vector pool entries (per rhs)
+    int max_parts = 1;
+    long long stat_first = 0;  // items of the statistics pass (s, col0)
+    int stat_count = 0;     // partial-sum slots of the largest backward update launch
     long long device_bytes = 0;
     ~aphi_analysis();
 };

@@ -19,8 +19,14 @@ struct aphi_assembly {
     std::unique_ptr<Assembly> a;
 };
 
+#include <atomic>
+
 namespace aphi_b200 {
 thread_local std::string g_last_error;
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void nested_dissection(int n, const int* row_ptr, const int* col_idx, const double* xyz, int leaf, int* perm);
+void reference_amd(int n, const int* row_ptr, const int* col_idx, int* perm);
 }
 
 extern "C" {
@@ -45,6 +51,8 @@ const char* aphi_status_string(int s) {
 }
 
 const char* aphi_last_error(void) { return g_last_error.c_str(); }
+
+int64_t aphi_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int aphi_workload_cylinder(int cells, double v_top, int full_wave, aphi_workload** out) {
     return guard([&] {
@@ -107,7 +115,20 @@ int aphi_workload_array(const aphi_workload* h, const char* name, const void** d
         else if (n == "phi_index") set(w.phi_index);
         else if (n == "tet_edges") set(w.tet_edges);
         else if (n == "body_of_tet") set(w.body_of_tet);
+        else if (n == "dof_xyz") set(w.dof_xyz);
         else throw Error(APHI_ERR_INVALID, "aphi_workload_array: unknown array '" + n + "'");
+    });
+}
+
+int aphi_order_nested_dissection(int n, const int* row_ptr, const int* col_idx, const double* xyz, int leaf,
+                                 int* perm) {
+    return guard([&] { nested_dissection(n, row_ptr, col_idx, xyz, leaf, perm); });
+}
+
+int aphi_order_amd(int n, const int* row_ptr, const int* col_idx, int* perm) {
+    return guard([&] {
+        if (n < 0 || (n > 0 && (!row_ptr || !col_idx || !perm))) throw Error(APHI_ERR_INVALID, "aphi_order_amd: null argument");
+        if (n > 0) reference_amd(n, row_ptr, col_idx, perm);
     });
 }
 

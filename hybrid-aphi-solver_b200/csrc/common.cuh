@@ -29,7 +29,14 @@ struct Error : std::runtime_error {
         }                                                                                     \
     } while (0)
 
-#define APHI_CHECK_LAUNCH() APHI_CUDA(cudaGetLastError())
+// Every kernel launch site is followed by APHI_CHECK_LAUNCH(), which also
+// counts the launch (aphi_launch_count()).
+void count_launch();
+#define APHI_CHECK_LAUNCH()               \
+    do {                                  \
+        ::aphi_b200::count_launch();      \
+        APHI_CUDA(cudaGetLastError());    \
+    } while (0)
 
 // Complex double as two doubles. The operations below spell out the exact
 // sequence of roundings the host's std::complex<double> performs (no fused

@@ -98,24 +98,32 @@ __global__ void k_extract_d(Sched S, int ns, const int* ref_of_post, const cx<R>
 
 // max |L(i, j)| over the multipliers whose row (in the caller's order) is at
 // most kmax[b] -- the rows the reference had computed when it stopped.
+// Item (s, c0): 32 columns of one panel; one warp per column.
 template <class R>
-__global__ void k_max_multiplier(Sched S, const int* ref_of_post, const cx<R>* Lb, long long lstride,
-                                 const int* kmax, unsigned long long* out) {
-    const int s = blockIdx.x;
+__global__ void __launch_bounds__(256) k_max_multiplier(Sched S, long long item0, const int* ref_of_post,
+                                                        const cx<R>* Lb, long long lstride, const int* kmax,
+                                                        unsigned long long* out) {
+    const Item it = S.items[item0 + blockIdx.x];
+    const int s = it.s, c0 = it.a;
     const int b = blockIdx.y;
     const cx<R>* L = Lb + lstride * b + S.loff[s];
     const int w = S.first[s + 1] - S.first[s];
     const int m = S.rows[s];
     const int* st = S.structs + S.soff[s];
     const int lim = kmax[b];
+    const int n_all = lim >= 0x7fffffff;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double best = 0.0;
-    for (long long e = threadIdx.x; e < static_cast<long long>(m) * w; e += blockDim.x) {
-        const int i = static_cast<int>(e % m), j = static_cast<int>(e / m);
-        if (i <= j) continue;
-        if (ref_of_post[st[i]] > lim) continue;
-        best = fmax(best, cabs_d(L[e]));
+    for (int j = c0 + warp; j < min(c0 + 32, w); j += 8) {
+        const cx<R>* col = L + static_cast<long long>(j) * m;
+        for (int i = j + 1 + lane; i < m; i += 32) {
+            if (!n_all && ref_of_post[st[i]] > lim) continue;
+            best = fmax(best, cabs_d(col[i]));
+        }
     }
-    atomicMax(&out[b], __double_as_longlong(best));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if (lane == 0) atomicMax(&out[b], __double_as_longlong(best));
 }
 
 // y[new] = b[orig] * d[orig]  (permute in, with the equilibration scaling).
@@ -237,8 +245,8 @@ T* dalloc(size_t n) {
 }
 
 template <class R>
-void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_t st, int nrhs,
-              cx<R>* y, cx<R>* U) {
+void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_t st, const SolveArgs* sa,
+              cx<R>* y, cx<R>* U, cx<R>* part) {
     const aphi_analysis* A = f->an;
     const Sched S = sched_of(A->d);
     cx<R>* L = reinterpret_cast<cx<R>*>(f->L);
@@ -255,8 +263,15 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
             case K_UPDATE:
                 k_update_tile<R><<<grid, 256, 2 * kStep * kTile * sizeof(cx<R>), st>>>(S, l.first, L, CB, ls, cs);
                 break;
-            case K_FWD: k_forward<R><<<grid, 256, 0, st>>>(S, l.first, L, ls, y, U, A->S.n, A->upool, nrhs); break;
-            case K_BWD: k_backward<R><<<grid, 256, 0, st>>>(S, l.first, L, ls, y, A->S.n, nrhs); break;
+            case K_FWD_GATHER: k_fwd_gather<R><<<grid, 256, 0, st>>>(S, l.first, *sa, y, U); break;
+            case K_FWD_DIAG:
+                k_fwd_diag<R><<<grid, 256, kSolveDiagSmem * sizeof(cx<R>), st>>>(S, l.first, *sa, L, ls, y);
+                break;
+            case K_FWD_UPDATE: k_fwd_update<R><<<grid, 256, 0, st>>>(S, l.first, *sa, L, ls, y, U); break;
+            case K_BWD_UPDATE: k_bwd_update<R><<<grid, 256, 0, st>>>(S, l.first, *sa, L, ls, y, part); break;
+            case K_BWD_DIAG:
+                k_bwd_diag<R><<<grid, 256, kSolveDiagSmem * sizeof(cx<R>), st>>>(S, l.first, *sa, L, ls, y, part);
+                break;
         }
         APHI_CHECK_LAUNCH();
     }
@@ -270,6 +285,10 @@ void set_smem_limits(int small_front) {
                                    96 * 96 * static_cast<int>(sizeof(cx<R>))));
     APHI_CUDA(cudaFuncSetAttribute(k_update_tile<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    2 * kStep * kTile * static_cast<int>(sizeof(cx<R>))));
+    APHI_CUDA(cudaFuncSetAttribute(k_fwd_diag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   kSolveDiagSmem * static_cast<int>(sizeof(cx<R>))));
+    APHI_CUDA(cudaFuncSetAttribute(k_bwd_diag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   kSolveDiagSmem * static_cast<int>(sizeof(cx<R>))));
     (void)small_front;
     done = true;
 }
@@ -284,7 +303,7 @@ void factorize_numeric(aphi_factor* f, const double* values, cudaStream_t st) {
     k_scatter_a<R><<<g, 256, 0, st>>>(n, A->d.row_ptr, A->d.col_idx, values, A->S.nnz_a, f->dscale, A->d.a_dest,
                                       reinterpret_cast<cx<R>*>(f->L), A->S.stored);
     APHI_CHECK_LAUNCH();
-    run_plan<R>(f, A->plan_factor, st, 0, nullptr, nullptr);
+    run_plan<R>(f, A->plan_factor, st, nullptr, nullptr, nullptr, nullptr);
     k_extract_d<R><<<dim3(A->S.ns, f->batch), 128, 0, st>>>(sched_of(A->d), A->S.ns, A->d.ref_of_post,
                                                           reinterpret_cast<const cx<R>*>(f->L), A->S.stored,
                                                           f->dref, n);
@@ -298,19 +317,26 @@ void solve_numeric(aphi_factor* f, int nrhs, const double* b, double* x, cudaStr
     if (f->nrhs_cap < nrhs) {
         if (f->y) cudaFree(f->y);
         if (f->U) cudaFree(f->U);
-        f->y = f->U = nullptr;
+        if (f->part) cudaFree(f->part);
+        f->y = f->U = f->part = nullptr;
         APHI_CUDA(cudaMalloc(&f->y, static_cast<size_t>(n) * nrhs * f->batch * sizeof(cx<R>) + 16));
         APHI_CUDA(cudaMalloc(&f->U, static_cast<size_t>(std::max<long long>(A->upool, 1)) * nrhs * f->batch *
                                         sizeof(cx<R>)));
+        APHI_CUDA(cudaMalloc(&f->part, static_cast<size_t>(A->max_parts) * kSolveBlock * 8 * f->batch * sizeof(cx<R>)));
         f->nrhs_cap = nrhs;
     }
+    set_smem_limits<R>(A->opt.small_front);
     cx<R>* y = reinterpret_cast<cx<R>*>(f->y);
     cx<R>* U = reinterpret_cast<cx<R>*>(f->U);
+    cx<R>* part = reinterpret_cast<cx<R>*>(f->part);
     const dim3 g(ceil_div(std::max(n, 1), 256), f->batch * nrhs);
     k_permute_in<R><<<g, 256, 0, st>>>(n, nrhs, A->d.orig_of_new, f->dscale, b, y);
     APHI_CHECK_LAUNCH();
-    run_plan<R>(f, A->plan_fwd, st, nrhs, y, U);
-    run_plan<R>(f, A->plan_bwd, st, nrhs, y, U);
+    for (int k0 = 0; k0 < nrhs; k0 += 8) {
+        const SolveArgs sa{n, nrhs, k0, std::min(8, nrhs - k0), A->upool, A->max_parts};
+        run_plan<R>(f, A->plan_fwd, st, &sa, y, U, part);
+        run_plan<R>(f, A->plan_bwd, st, &sa, y, U, part);
+    }
     k_permute_out<R><<<g, 256, 0, st>>>(n, nrhs, A->d.new_of_orig, f->dscale, y, x);
     APHI_CHECK_LAUNCH();
 }
@@ -367,6 +393,7 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
     const dim3 g(ceil_div(std::max(n, 1), kEqThreads), B);
     for (int it = 0; it < equil_iters; ++it) {
         k_eq_rowmax<<<g, kEqThreads, 0, st>>>(n, A->d.row_ptr, A->d.col_idx, values, S.nnz_a, f->dscale, f->rowmax);
+        APHI_CHECK_LAUNCH();
         k_eq_update<<<g, kEqThreads, 0, st>>>(n, f->dscale, f->rowmax);
         APHI_CHECK_LAUNCH();
     }
@@ -386,7 +413,7 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
     APHI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    std::vector<int> kmax(B, n);
+    std::vector<int> kmax(B, 0x7fffffff);
     bool any_fail = false;
     for (int b = 0; b < B; ++b) {
         aphi_factor_stats& s = f->host_stats[b];
@@ -424,15 +451,16 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
     int* d_kmax = dalloc<int>(B);
     APHI_CUDA(cudaMemcpyAsync(d_kmax, kmax.data(), sizeof(int) * B, cudaMemcpyHostToDevice, st));
     APHI_CUDA(cudaMemsetAsync(f->stats, 0, sizeof(unsigned long long) * 4 * B, st));
-    if (S.ns > 0) {
+    if (A->stat_count > 0) {
+        const dim3 gs(A->stat_count, B);
         if (f->precision == 64)
-            k_max_multiplier<double><<<dim3(S.ns, B), 256, 0, st>>>(sched_of(A->d), A->d.ref_of_post,
-                                                                    reinterpret_cast<const cx<double>*>(f->L),
-                                                                    S.stored, d_kmax, f->stats);
+            k_max_multiplier<double><<<gs, 256, 0, st>>>(sched_of(A->d), A->stat_first, A->d.ref_of_post,
+                                                         reinterpret_cast<const cx<double>*>(f->L), S.stored,
+                                                         d_kmax, f->stats);
         else
-            k_max_multiplier<float><<<dim3(S.ns, B), 256, 0, st>>>(sched_of(A->d), A->d.ref_of_post,
-                                                                   reinterpret_cast<const cx<float>*>(f->L),
-                                                                   S.stored, d_kmax, f->stats);
+            k_max_multiplier<float><<<gs, 256, 0, st>>>(sched_of(A->d), A->stat_first, A->d.ref_of_post,
+                                                        reinterpret_cast<const cx<float>*>(f->L), S.stored,
+                                                        d_kmax, f->stats);
         APHI_CHECK_LAUNCH();
     }
     std::vector<unsigned long long> mx(4 * B);
@@ -475,7 +503,9 @@ void residuals(const aphi_analysis* an, int batch, int nrhs, const double* value
     APHI_CUDA(cudaMemsetAsync(amax, 0, sizeof(unsigned long long) * batch, st));
     k_residual<<<dim3(nb, batch * nrhs), 256, 0, st>>>(n, nrhs, an->d.fptr, an->d.fcol, an->d.fmap, values,
                                                        an->S.nnz_a, x, b, nullptr, partial);
+    APHI_CHECK_LAUNCH();
     k_amax<<<dim3(ceil_div(std::max<long long>(an->S.nnz_a, 1), 256), batch), 256, 0, st>>>(values, an->S.nnz_a, amax);
+    APHI_CHECK_LAUNCH();
     k_norms_final<<<batch * nrhs, 256, 0, st>>>(nb, nrhs, partial, amax, norms);
     APHI_CHECK_LAUNCH();
     std::vector<double> h(4 * static_cast<size_t>(batch) * nrhs);
@@ -526,6 +556,7 @@ int solve_refined(aphi_factor* f, int nrhs, const double* values, const double* 
     for (int step = 0;; ++step) {
         k_residual<<<dim3(nb, q), 256, 0, st>>>(n, nrhs, A->d.fptr, A->d.fcol, A->d.fmap, values, A->S.nnz_a, x, b,
                                                 r, f->red);
+        APHI_CHECK_LAUNCH();
         k_norms_final<<<q, 256, 0, st>>>(nb, nrhs, f->red, amax, f->norms);
         APHI_CHECK_LAUNCH();
         APHI_CUDA(cudaMemcpyAsync(h.data(), f->norms, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -638,7 +669,7 @@ void factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, do
 }  // namespace aphi_b200
 
 aphi_factor::~aphi_factor() {
-    void* ptrs[] = {L, CB, dscale, rowmax, stats, dref, y, U, ir, red, norms};
+    void* ptrs[] = {L, CB, dscale, rowmax, stats, dref, y, U, part, ir, red, norms};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }

@@ -23,6 +23,7 @@ struct aphi_factor {
     // Solve scratch, grown on demand: y (batch x nrhs x n), U (batch x nrhs x upool).
     void* y = nullptr;
     void* U = nullptr;
+    void* part = nullptr;  // backward partial sums: batch x max_parts x 64 x 8
     int nrhs_cap = 0;
     // Refinement scratch (FP64): x, r, d, per batch x nrhs x n; norms.
     double* ir = nullptr;

@@ -321,23 +321,40 @@ __global__ void __launch_bounds__(256) k_update_tile(Sched S, long long item0, c
 }
 
 // ---------------------------------------------------------------- solves
-// y, U: per batch entry, nrhs vectors of length n (post-ordered) and upool.
-// Forward: the front vector of s is y[cols of s] plus the children's update
-// vectors (extend-add, children in order); solve with the unit L11, then
-// U_s = (accumulated) - L21 y_s.
+// y, U: per batch entry, nrhs vectors of length n (post-ordered numbering) and
+// upool (update vectors, one segment of m - w entries per supernode). A
+// kernel handles nr <= 8 right-hand sides starting at rhs k0.
+//
+// Forward (L y = b), per level bottom-up: gather the children's update
+// vectors into the front vector (y at the pivot rows, U_s below), then per
+// 64-column block: solve the block's unit triangle, update the rows below.
+// Backward (L^T x = D^-1 y), per level top-down, blocks last to first: partial
+// sums of L[rows below, block]^T x over 256-row chunks, then one CTA adds them
+// in chunk order, scales by D^-1 and solves the block's triangle.
+constexpr int kSolveDiagSmem = (kSolveBlock * kSolveBlock + 8 * kSolveBlock);  // complex entries
+
+struct SolveArgs {
+    int n;
+    int nrhs;      // vectors per batch entry in y / U
+    int k0, nr;    // the rhs handled by this pass
+    long long upool;
+    int max_parts;
+};
+
+__device__ __forceinline__ long long vec_at(const SolveArgs& a, int b, int k) {
+    return static_cast<long long>(b) * a.nrhs + (a.k0 + k);
+}
+
 template <class R>
-__global__ void __launch_bounds__(256) k_forward(Sched S, long long item0, const cx<R>* Lb, long long lstride,
-                                                 cx<R>* yb, cx<R>* Ub, int n, long long upool, int nrhs) {
+__global__ void __launch_bounds__(256) k_fwd_gather(Sched S, long long item0, SolveArgs a, cx<R>* yb, cx<R>* Ub) {
     const int s = S.items[item0 + blockIdx.x].s;
-    const cx<R>* L = Lb + lstride * blockIdx.y;
     const int w = S.first[s + 1] - S.first[s];
     const int m = S.rows[s];
     const int cs = m - w;
     const int f = S.first[s];
-    const cx<R>* Ls = L + S.loff[s];
-    for (int k = 0; k < nrhs; ++k) {
-        cx<R>* y = yb + (static_cast<long long>(blockIdx.y) * nrhs + k) * n;
-        cx<R>* U = Ub + (static_cast<long long>(blockIdx.y) * nrhs + k) * upool;
+    for (int k = 0; k < a.nr; ++k) {
+        cx<R>* y = yb + vec_at(a, blockIdx.y, k) * a.n;
+        cx<R>* U = Ub + vec_at(a, blockIdx.y, k) * a.upool;
         cx<R>* Us = U + S.uoff[s];
         for (int i = threadIdx.x; i < cs; i += blockDim.x) Us[i] = cx<R>{0, 0};
         __syncthreads();
@@ -353,68 +370,165 @@ __global__ void __launch_bounds__(256) k_forward(Sched S, long long item0, const
             }
             __syncthreads();
         }
-        for (int j = 0; j < w; ++j) {
-            const cx<R> yj = y[f + j];
-            const cx<R>* col = Ls + static_cast<long long>(j) * m;
-            for (int i = j + 1 + threadIdx.x; i < w; i += blockDim.x) y[f + i] = fms(y[f + i], col[i], yj);
-            __syncthreads();
-        }
-        for (int i = threadIdx.x; i < cs; i += blockDim.x) {
-            cx<R> acc = Us[i];
-            for (int j = 0; j < w; ++j) acc = fms(acc, Ls[w + i + static_cast<long long>(j) * m], y[f + j]);
-            Us[i] = acc;
-        }
-        __syncthreads();
     }
 }
 
-// Backward: x_s = L11^-T (D^-1 y_s - L21^T x[struct rows below]).
+// Item (s, blk): y[blk] = L_bb^-1 y[blk], one warp per rhs.
 template <class R>
-__global__ void __launch_bounds__(256) k_backward(Sched S, long long item0, const cx<R>* Lb, long long lstride,
-                                                  cx<R>* yb, int n, int nrhs) {
-    __shared__ cx<R> red[8];
-    const int s = S.items[item0 + blockIdx.x].s;
-    const cx<R>* L = Lb + lstride * blockIdx.y;
+__global__ void __launch_bounds__(256) k_fwd_diag(Sched S, long long item0, SolveArgs a, const cx<R>* Lb,
+                                                  long long lstride, cx<R>* yb) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<R>* T = reinterpret_cast<cx<R>*>(smem_raw);
+    cx<R>(*ys)[kSolveBlock] = reinterpret_cast<cx<R>(*)[kSolveBlock]>(T + kSolveBlock * kSolveBlock);
+    const Item it = S.items[item0 + blockIdx.x];
+    const int s = it.s, j0 = it.a * kSolveBlock;
     const int w = S.first[s + 1] - S.first[s];
     const int m = S.rows[s];
     const int f = S.first[s];
-    const cx<R>* Ls = L + S.loff[s];
-    const int* st = S.structs + S.soff[s];
+    const int jb = min(kSolveBlock, w - j0);
+    const cx<R>* P = Lb + lstride * blockIdx.y + S.loff[s] + j0 + static_cast<long long>(j0) * m;
+    for (int e = threadIdx.x; e < jb * jb; e += blockDim.x) {
+        const int i = e % jb, j = e / jb;
+        T[i + j * kSolveBlock] = P[i + static_cast<long long>(j) * m];
+    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int k = 0; k < nrhs; ++k) {
-        cx<R>* y = yb + (static_cast<long long>(blockIdx.y) * nrhs + k) * n;
-        // z_j = y_j / D_j - sum_{i >= w} L[i, j] x[struct_i], one warp per column.
-        for (int j = warp; j < w; j += 8) {
-            const cx<R>* col = Ls + static_cast<long long>(j) * m;
-            cx<R> acc{0, 0};
-            for (int i = w + lane; i < m; i += 32) acc = acc + col[i] * y[st[i]];
+    cx<R>* y = yb + vec_at(a, blockIdx.y, warp) * a.n + f + j0;
+    if (warp < a.nr)
+        for (int i = lane; i < jb; i += 32) ys[warp][i] = y[i];
+    __syncthreads();
+    if (warp >= a.nr) return;
+    for (int j = 0; j < jb; ++j) {
+        const cx<R> yj = ys[warp][j];
+        for (int i = j + 1 + lane; i < jb; i += 32) ys[warp][i] = fms(ys[warp][i], T[i + j * kSolveBlock], yj);
+        __syncwarp();
+    }
+    for (int i = lane; i < jb; i += 32) y[i] = ys[warp][i];
+}
+
+// Item (s, blk, row0): rows row0.. of the supernode minus L[rows, blk] y[blk].
+template <class R>
+__global__ void __launch_bounds__(256) k_fwd_update(Sched S, long long item0, SolveArgs a, const cx<R>* Lb,
+                                                    long long lstride, cx<R>* yb, cx<R>* Ub) {
+    __shared__ cx<R> ys[8][kSolveBlock];
+    const Item it = S.items[item0 + blockIdx.x];
+    const int s = it.s, j0 = it.a * kSolveBlock, row0 = it.b;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int f = S.first[s];
+    const int jb = min(kSolveBlock, w - j0);
+    for (int e = threadIdx.x; e < jb * a.nr; e += blockDim.x) {
+        const int j = e % jb, k = e / jb;
+        ys[k][j] = yb[vec_at(a, blockIdx.y, k) * a.n + f + j0 + j];
+    }
+    __syncthreads();
+    const int r = row0 + threadIdx.x;
+    if (r >= m) return;
+    const cx<R>* P = Lb + lstride * blockIdx.y + S.loff[s] + r + static_cast<long long>(j0) * m;
+    cx<R> acc[8];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                acc.re += __shfl_xor_sync(0xffffffffu, acc.re, o);
-                acc.im += __shfl_xor_sync(0xffffffffu, acc.im, o);
-            }
-            if (lane == 0) y[f + j] = y[f + j] * crecip(col[j]) - acc;
+    for (int k = 0; k < 8; ++k) acc[k] = cx<R>{0, 0};
+    for (int j = 0; j < jb; ++j) {
+        const cx<R> l = P[static_cast<long long>(j) * m];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (k < a.nr) acc[k] = acc[k] + l * ys[k][j];
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        if (k >= a.nr) break;
+        cx<R>* dst = r < w ? yb + vec_at(a, blockIdx.y, k) * a.n + f + r
+                           : Ub + vec_at(a, blockIdx.y, k) * a.upool + S.uoff[s] + (r - w);
+        *dst = *dst - acc[k];
+    }
+}
+
+// Item (s, blk, row0, slot): partial[slot][j][k] = sum over rows row0..row0+255
+// (below the block) of L[row, j0 + j] x_k[row].
+template <class R>
+__global__ void __launch_bounds__(256) k_bwd_update(Sched S, long long item0, SolveArgs a, const cx<R>* Lb,
+                                                    long long lstride, const cx<R>* yb, cx<R>* partb) {
+    __shared__ cx<R> xs[8][kSolveRows];
+    const Item it = S.items[item0 + blockIdx.x];
+    const int s = it.s, j0 = it.a * kSolveBlock, row0 = it.b, slot = it.c;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int f = S.first[s];
+    const int jb = min(kSolveBlock, w - j0);
+    const int nrows = min(kSolveRows, m - row0);
+    const int* st = S.structs + S.soff[s];
+    for (int e = threadIdx.x; e < nrows * a.nr; e += blockDim.x) {
+        const int t = e % nrows, k = e / nrows;
+        const int r = row0 + t;
+        const int g = r < w ? f + r : st[r];
+        xs[k][t] = yb[vec_at(a, blockIdx.y, k) * a.n + g];
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const cx<R>* P = Lb + lstride * blockIdx.y + S.loff[s] + row0 + static_cast<long long>(j0) * m;
+    cx<R>* part = partb + static_cast<long long>(blockIdx.y) * a.max_parts * kSolveBlock * 8 +
+                  static_cast<long long>(slot) * kSolveBlock * 8;
+    for (int j = warp; j < jb; j += 8) {
+        const cx<R>* col = P + static_cast<long long>(j) * m;
+        cx<R> acc[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] = cx<R>{0, 0};
+        for (int t = lane; t < nrows; t += 32) {
+            const cx<R> l = col[t];
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (k < a.nr) acc[k] = acc[k] + l * xs[k][t];
         }
-        __syncthreads();
-        for (int j = w - 1; j >= 0; --j) {
-            const cx<R>* col = Ls + static_cast<long long>(j) * m;
-            cx<R> acc{0, 0};
-            for (int i = j + 1 + threadIdx.x; i < w; i += blockDim.x) acc = acc + col[i] * y[f + i];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k >= a.nr) break;
+            cx<R> v = acc[k];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
-                acc.re += __shfl_xor_sync(0xffffffffu, acc.re, o);
-                acc.im += __shfl_xor_sync(0xffffffffu, acc.im, o);
+                v.re += __shfl_xor_sync(0xffffffffu, v.re, o);
+                v.im += __shfl_xor_sync(0xffffffffu, v.im, o);
             }
-            if (lane == 0) red[warp] = acc;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                cx<R> t{0, 0};
-                for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t = t + red[q];
-                y[f + j] = y[f + j] - t;
-            }
-            __syncthreads();
+            if (lane == 0) part[j * 8 + k] = v;
         }
     }
+}
+
+// Item (s, blk, first_slot, nslots): x[blk] = L_bb^-T (D^-1 y[blk] - sum of partials).
+template <class R>
+__global__ void __launch_bounds__(256) k_bwd_diag(Sched S, long long item0, SolveArgs a, const cx<R>* Lb,
+                                                  long long lstride, cx<R>* yb, const cx<R>* partb) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<R>* T = reinterpret_cast<cx<R>*>(smem_raw);
+    cx<R>(*zs)[kSolveBlock] = reinterpret_cast<cx<R>(*)[kSolveBlock]>(T + kSolveBlock * kSolveBlock);
+    const Item it = S.items[item0 + blockIdx.x];
+    const int s = it.s, j0 = it.a * kSolveBlock, p0 = it.b, np = it.c;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int f = S.first[s];
+    const int jb = min(kSolveBlock, w - j0);
+    const cx<R>* P = Lb + lstride * blockIdx.y + S.loff[s] + j0 + static_cast<long long>(j0) * m;
+    for (int e = threadIdx.x; e < jb * jb; e += blockDim.x) {
+        const int i = e % jb, j = e / jb;
+        T[i + j * kSolveBlock] = P[i + static_cast<long long>(j) * m];
+    }
+    __syncthreads();
+    const cx<R>* part = partb + static_cast<long long>(blockIdx.y) * a.max_parts * kSolveBlock * 8;
+    for (int e = threadIdx.x; e < jb * a.nr; e += blockDim.x) {
+        const int j = e % jb, k = e / jb;
+        cx<R> sum{0, 0};
+        for (int q = 0; q < np; ++q) sum = sum + part[(static_cast<long long>(p0 + q) * kSolveBlock + j) * 8 + k];
+        const cx<R> yv = yb[vec_at(a, blockIdx.y, k) * a.n + f + j0 + j];
+        zs[k][j] = yv * crecip(T[j * (kSolveBlock + 1)]) - sum;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp >= a.nr) return;
+    for (int j = jb - 1; j >= 0; --j) {
+        const cx<R> xj = zs[warp][j];
+        for (int t = lane; t < j; t += 32) zs[warp][t] = fms(zs[warp][t], T[j + t * kSolveBlock], xj);
+        __syncwarp();
+    }
+    cx<R>* y = yb + vec_at(a, blockIdx.y, warp) * a.n + f + j0;
+    for (int i = lane; i < jb; i += 32) y[i] = zs[warp][i];
 }
 
 }  // namespace aphi_b200

@@ -366,6 +366,26 @@ void build_cylinder(Workload& w, int n, double v_top, int full_wave) {
         }
     }
 
+    // Unknown positions.
+    w.dof_xyz.assign(3 * static_cast<size_t>(w.num_total), 0.0);
+    auto p2_xyz = [&](int p2, double* out) {
+        if (p2 < w.num_nodes) {
+            for (int d = 0; d < 3; ++d) out[d] = w.xyz[3 * p2 + d];
+        } else {
+            const int e = p2 - w.num_nodes;
+            for (int d = 0; d < 3; ++d) out[d] = 0.5 * (w.xyz[3 * w.edges[2 * e] + d] + w.xyz[3 * w.edges[2 * e + 1] + d]);
+        }
+    };
+    for (int e = 0; e < w.num_edges; ++e)
+        if (w.edge_index[e] >= 0) p2_xyz(w.num_nodes + e, &w.dof_xyz[3 * w.edge_index[e]]);
+    for (int i = 0; i < num_p2; ++i)
+        if (w.phi_index[i] >= 0) p2_xyz(i, &w.dof_xyz[3 * w.phi_index[i]]);
+    for (int k = 0; k < w.num_ports; ++k) {
+        w.dof_xyz[3 * w.port_row[k]] = 0.5;
+        w.dof_xyz[3 * w.port_row[k] + 1] = 0.5;
+        w.dof_xyz[3 * w.port_row[k] + 2] = k == 0 ? 1.0 : 0.0;
+    }
+
     // Upper-triangle pattern: each tet's live unknowns, sorted and uniqued,
     // give every pair (i <= j); voltage-port rows get their diagonal.
     const int N = w.num_total;

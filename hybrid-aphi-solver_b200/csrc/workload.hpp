@@ -59,6 +59,10 @@ struct Workload {
     std::vector<double> port_amplitude;  // complex, 2 per port
     std::vector<double> port_value;      // complex prescribed value, 2 per port
 
+    // Position of every unknown (edge midpoint, P2 node, port terminal
+    // centroid), 3 per unknown: what a geometric ordering cuts on.
+    std::vector<double> dof_xyz;
+
     // Upper-triangle CSR pattern of the assembled matrix.
     std::vector<int> row_ptr;
     std::vector<int> col_idx;

@@ -51,6 +51,8 @@ extern "C" {
 
 const char* aphi_status_string(int status);
 const char* aphi_last_error(void);
+/* Kernels this library has launched in this process (all threads). */
+int64_t aphi_launch_count(void);
 
 /* Conditioning, as include/aphi_solver/problem.hpp:58-62 numbers it. */
 #define APHI_COND_NATURAL 0
@@ -75,8 +77,25 @@ int aphi_workload_sizes(const aphi_workload* w, int64_t* sizes);
  * (double, 3/body), "body_ptr" (int), "body_tets" (int), "port_current",
  * "port_row" (int), "port_amplitude", "port_value" (double, 2/port),
  * "row_ptr", "col_idx" (int), "edges" (int, 2/edge), "edge_index",
- * "phi_index" (int), "tet_edges" (int, 6/tet), "body_of_tet" (int). */
+ * "phi_index" (int), "tet_edges" (int, 6/tet), "body_of_tet" (int),
+ * "dof_xyz" (double, 3/unknown: edge midpoints, P2 nodes, port terminals). */
 int aphi_workload_array(const aphi_workload* w, const char* name, const void** data, int64_t* count);
+
+/* Fill-reducing permutation (new -> old) by geometric nested dissection over
+ * the unknowns' positions xyz (3 per unknown); parts of at most `leaf`
+ * unknowns are numbered by minimum degree. Not a reference interface: the
+ * reference orders with its own AMD (src/ordering.cpp:220-510), whose
+ * permutation this library consumes unchanged when it is the caller; this
+ * one serves standalone callers. */
+int aphi_order_nested_dissection(int n, const int* row_ptr, const int* col_idx, const double* xyz, int leaf,
+                                 int* perm);
+
+/* The reference's approximate-minimum-degree permutation (new -> old) of an
+ * upper-triangle pattern, reproduced bit for bit -- compute_ordering(pattern,
+ * Ordering::ApproximateMinimumDegree), src/ordering.cpp:220-510 and :539-556 --
+ * so a caller without the reference's host code factorizes in the reference's
+ * column order. */
+int aphi_order_amd(int n, const int* row_ptr, const int* col_idx, int* perm);
 
 /* ---- assembly: element fill + deterministic scatter -----------------------
  * Replaces refill(SymmetricSystem&, ...) and refill(AssembledSystem&, ...)

@@ -1,0 +1,51 @@
+"""The C ABI library loads and exports every function include/aphi_b200.h
+declares; the Python layer binds each one. CPU only (no compute calls)."""
+import ctypes
+import re
+from pathlib import Path
+
+import aphi_b200 as ab
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "aphi_b200.h"
+
+
+def declared():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[\w\s\*]+?\b(aphi_\w+)\s*\(", text, re.M)))
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared()
+    assert len(names) > 25
+    lib = ctypes.CDLL(str(ab.LIB_PATH))
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_layer_binds_every_declared_symbol():
+    assert sorted(set(declared()) - set(ab.exported_symbols())) == []
+
+
+def test_status_strings_and_errors_without_a_gpu():
+    L = ab.lib()
+    assert L.aphi_status_string(ab.ERR_PIVOT_FLOOR).decode() == "pivot at or below the floor"
+    # a refused argument is reported, not thrown across the ABI
+    rc = L.aphi_formulation_scales(ab.COND_ROW_SCALED, 0.0, None, None)
+    assert rc == ab.ERR_BAD_SHAPE and "DC" in L.aphi_last_error().decode()
+
+
+def test_analysis_matches_reference_etree_on_host():
+    w = ab.Workload.cylinder(5)
+    perm = ab.amd_ordering(w.row_ptr, w.col_idx)
+    an = ab.Analysis(w.row_ptr, w.col_idx, perm)
+    parent, cc = an.etree()
+    assert (parent < 0).sum() == an.info["num_roots"]
+    assert int(cc.sum()) == int(an.info["nnz_l"])
+    # a wrong elimination tree handed in is refused as a logic error
+    bad = parent.copy()
+    bad[0] = -1 if bad[0] >= 0 else 1
+    try:
+        ab.Analysis(w.row_ptr, w.col_idx, perm, bad)
+        raise AssertionError("expected a LogicError")
+    except ab.LogicError:
+        pass

@@ -232,10 +232,20 @@ def test_multiple_rhs_and_residuals(cuda, ref_or_skip):
     x = f.solve(b)
     res = ab.residuals(an, vals, x, b)
     assert res.shape == (1, 5, 2)
-    assert (res[..., 0] <= 1e-12).all() and (res[..., 1] <= 1e-14).all()
+    # Random right-hand sides on an ill-conditioned system: judge by the
+    # backward error (the relative residual scales with the condition number).
+    assert (res[..., 1] <= 1e-15).all(), res
     for k in range(5):
         xk = f.solve(b[:, k])
-        assert torch.allclose(xk[0], x[0, k], rtol=0, atol=0)
+        assert bool((xk[0] == x[0, k]).all())     # each rhs independent of the others
+    # ... and the physical right-hand side reaches the tight residual
+    xp = f.solve(rhs)
+    rp = ab.residuals(an, vals, xp, rhs)
+    assert rp[0, 0, 0] <= 1e-12 and rp[0, 0, 1] <= 1e-16
+    # more than 8 right-hand sides take several passes of the solve kernels
+    b12 = torch.cat([b, b, b[:, :2]], dim=1)
+    x12 = f.solve(b12)
+    assert bool((x12[0, 5] == x[0, 0]).all()) and bool((x12[0, 11] == x[0, 1]).all())
 
 
 def test_fp32_factor_with_fp64_refinement(cuda, ref_or_skip):
