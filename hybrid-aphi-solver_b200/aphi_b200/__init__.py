@@ -135,6 +135,7 @@ _SIGS = {
     "aphi_factor_export": (I, [P, I, PI, PI, PD, PD, PD]),
     "aphi_residuals": (I, [P, I, I, P, P, P, PD, P]),
     "aphi_solve_refined": (I, [P, I, P, P, P, C.POINTER(IROptions), PI, PD, P]),
+    "aphi_residuals_noalloc": (I, [P, I, I, P, P, P, PD, P]),
     "aphi_solve_symmetric_host": (I, [P, PD, PD, I, D, PD, PD]),
 }
 

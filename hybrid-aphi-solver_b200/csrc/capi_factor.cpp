@@ -64,6 +64,16 @@ int aphi_residuals(const aphi_analysis* an, int batch, int nrhs, const double* v
     });
 }
 
+int aphi_residuals_noalloc(const aphi_analysis* an, int batch, int nrhs, const double* values_dev,
+                           const double* x_dev, const double* b_dev, double* out, void* stream) {
+    return guard([&] {
+        if (!an || !values_dev || !x_dev || !b_dev || !out)
+            throw Error(APHI_ERR_INVALID, "aphi_residuals_noalloc: null argument");
+        if (batch < 1 || nrhs < 1) throw Error(APHI_ERR_BAD_SHAPE, "aphi_residuals_noalloc: batch and nrhs must be >= 1");
+        residuals_noalloc(an, batch, nrhs, values_dev, x_dev, b_dev, out, as_stream(stream));
+    });
+}
+
 int aphi_solve_refined(aphi_factor* f, int nrhs, const double* values_dev, const double* b_dev, double* x_dev,
                        const aphi_ir_options* opt, int* iters, double* berr, void* stream) {
     int rc = APHI_OK;

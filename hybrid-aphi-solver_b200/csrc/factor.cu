@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -520,6 +521,94 @@ void residuals(const aphi_analysis* an, int batch, int nrhs, const double* value
         const double den = am * xn + bn;
         out[2 * q + 1] = den > 0.0 ? rn / den : rn;
     }
+}
+
+// ---------------------------------------------------------------- allocation-free residuals
+// The same residual and backward-error computation as residuals() above, for
+// callers that cannot allocate device memory while they run: a serving loop
+// whose memory pool has already claimed the device's free memory for factors,
+// or a latency-critical path that cannot absorb the device-wide
+// synchronization cudaFree implies. Its scratch (per-block partial sums, the
+// max|A| words and the final ratios) lives in the file-scope device array
+// below, of fixed size; every GPU that loads this library holds it until the
+// process exits.
+//
+// The array is shared by all calls: calls that overlap on the GPU (on
+// different streams, or from different host threads) race on it, so a caller
+// must order them. The max|A| words are cleared at the start of every call;
+// everything else is fully written before it is read.
+constexpr size_t kResidualScratchDoubles = size_t(1) << 20;  // 8 MiB
+static __device__ __align__(256) double g_residual_scratch[kResidualScratchDoubles];
+
+// Ratios straight into the scratch, so the host copy needs no staging buffer.
+__global__ void k_norm_ratios(int q, const double* norms, double* out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= q) return;
+    const double rn = norms[4 * k], bn = norms[4 * k + 1], xn = norms[4 * k + 2], am = norms[4 * k + 3];
+    out[2 * k] = bn > 0.0 ? rn / bn : rn;
+    const double den = am * xn + bn;
+    out[2 * k + 1] = den > 0.0 ? rn / den : rn;
+}
+
+namespace {
+
+// Device address of the scratch array, looked up once per device with that
+// device current. In host code the array's name stands for a host-side
+// shadow, not a device address, so it is never handed to a kernel directly.
+double* residual_scratch() {
+    static std::mutex mu;
+    static double* ptrs[64] = {};
+    int dev = 0;
+    APHI_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw Error(APHI_ERR_INVALID, "residuals_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptrs[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_residual_scratch);
+        if (e != cudaSuccess || !p)
+            throw Error(APHI_ERR_CUDA, std::string("residuals_noalloc: cudaGetSymbolAddress failed: ") +
+                                           cudaGetErrorString(e));
+        ptrs[dev] = static_cast<double*>(p);
+    }
+    return ptrs[dev];
+}
+
+}  // namespace
+
+void residuals_noalloc(const aphi_analysis* an, int batch, int nrhs, const double* values, const double* x,
+                       const double* b, double* out, cudaStream_t st) {
+    if (!an->on_device)
+        throw Error(APHI_ERR_INVALID,
+                    "residuals_noalloc: the analysis has no device copy yet (create a factor from it first); "
+                    "this entry point does not allocate one");
+    const int n = an->S.n;
+    const long long nb = ceil_div(std::max(n, 1), 256);
+    const long long q = static_cast<long long>(batch) * nrhs;
+    // partial sums, max|A| words (one per batch entry), norms, ratios
+    const long long need = nb * 3 * q + batch + 4 * q + 2 * q;
+    if (need > static_cast<long long>(kResidualScratchDoubles))
+        throw Error(APHI_ERR_BAD_SHAPE,
+                    "residuals_noalloc: " + std::to_string(n) + " unknowns x " + std::to_string(q) +
+                        " right-hand sides need " + std::to_string(need) + " doubles of scratch; the fixed "
+                        "array holds " + std::to_string(kResidualScratchDoubles) +
+                        " (use aphi_residuals, which allocates, or fewer right-hand sides per call)");
+    double* scratch = residual_scratch();
+    double* partial = scratch;
+    unsigned long long* amax = reinterpret_cast<unsigned long long*>(scratch + nb * 3 * q);
+    double* norms = scratch + nb * 3 * q + batch;
+    double* ratios = norms + 4 * q;
+    APHI_CUDA(cudaMemsetAsync(amax, 0, sizeof(unsigned long long) * batch, st));
+    k_residual<<<dim3(static_cast<unsigned>(nb), static_cast<unsigned>(q)), 256, 0, st>>>(
+        n, nrhs, an->d.fptr, an->d.fcol, an->d.fmap, values, an->S.nnz_a, x, b, nullptr, partial);
+    APHI_CHECK_LAUNCH();
+    k_amax<<<dim3(ceil_div(std::max<long long>(an->S.nnz_a, 1), 256), batch), 256, 0, st>>>(values, an->S.nnz_a, amax);
+    APHI_CHECK_LAUNCH();
+    k_norms_final<<<static_cast<unsigned>(q), 256, 0, st>>>(static_cast<int>(nb), nrhs, partial, amax, norms);
+    APHI_CHECK_LAUNCH();
+    k_norm_ratios<<<ceil_div(q, 128), 128, 0, st>>>(static_cast<int>(q), norms, ratios);
+    APHI_CHECK_LAUNCH();
+    APHI_CUDA(cudaMemcpyAsync(out, ratios, sizeof(double) * 2 * q, cudaMemcpyDeviceToHost, st));
+    APHI_CUDA(cudaStreamSynchronize(st));
 }
 
 int solve_refined(aphi_factor* f, int nrhs, const double* values, const double* b, double* x,

@@ -47,6 +47,8 @@ void factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, do
                    double* diagonal, double* d_scale);
 void residuals(const aphi_analysis* an, int batch, int nrhs, const double* values_dev, const double* x_dev,
                const double* b_dev, double* out, cudaStream_t stream);
+void residuals_noalloc(const aphi_analysis* an, int batch, int nrhs, const double* values_dev,
+                       const double* x_dev, const double* b_dev, double* out, cudaStream_t stream);
 int solve_refined(aphi_factor* f, int nrhs, const double* values_dev, const double* b_dev, double* x_dev,
                   const aphi_ir_options& opt, int* iters, double* berr, cudaStream_t stream);
 

@@ -234,6 +234,22 @@ int aphi_factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index
 int aphi_residuals(const aphi_analysis* an, int batch, int nrhs, const double* values_dev,
                    const double* x_dev, const double* b_dev, double* out, void* stream);
 
+/* The same numbers as aphi_residuals, computed without allocating device
+ * memory: for callers that cannot call cudaMalloc while they run -- a serving
+ * loop whose memory pool already owns the device's free memory, or a
+ * latency-critical path that cannot take cudaFree's device-wide
+ * synchronization. No counterpart in the reference. Its scratch is one
+ * fixed-size device array inside this library (8 MiB per GPU that loads it,
+ * held until exit); sizes needing more -- roughly ceil(N/256) * 3 * batch *
+ * nrhs doubles -- are refused with BAD_SHAPE. The analysis must already have
+ * a device copy (any factor created from it makes one), or INVALID is
+ * returned. The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race on it, so
+ * callers must order them. */
+int aphi_residuals_noalloc(const aphi_analysis* an, int batch, int nrhs, const double* values_dev,
+                           const double* x_dev, const double* b_dev, double* out, void* stream);
+
 /* Iterative refinement (new; include/aphi_solver/factorization.hpp:27-30 names
  * it as future work): x <- x + solve(r), r = b - A x in FP64 on the original
  * system, until backward error <= tol or max_iters; stall (error not halving)
