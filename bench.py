@@ -6,10 +6,11 @@
 One step is one sweep: the 16 log-spaced frequencies (50 Hz .. 1 MHz) of the
 32^3-cell cylinder-in-box (196,608 Kuhn tets, 227,004 unknowns), each
 assembled on the device (element fill + scatter), equilibrated, factorized
-and solved to backward error <= 1e-14 (relative residual <= 1e-10) -- the
-FP32 tensor path factorizing all 16 frequencies in one batch, FP64 iterative
-refinement on the original system. The plain FP64 factorization of the same
-sweep is timed beside it (fp64_* keys). The ordering is the reference's own
+and solved to relative residual <= 1e-14 (the bar is 1e-10): all 16
+frequencies factorized in one FP32 batch on the tensor cores, refined by
+FP64 preconditioned COCG on the original systems, and any frequency whose
+refinement stalls refactorized in FP64 automatically. The plain FP64
+factorization of the same sweep is timed beside it (the "fp64" key). The ordering is the reference's own
 AMD permutation, reproduced bit for bit on the host.
 
 Multi-GPU: one process per GPU, each solving its own sweep (frequency
@@ -212,18 +213,12 @@ def run_ours(args):
     omegas = 2 * np.pi * np.geomspace(F_LO, F_HI, args.nfreq) * (1.0 + 1e-3 * rank)
     stream = torch.cuda.current_stream()
 
-    f32 = ab.Factor(an, precision=ab.PREC_FP32, batch=args.nfreq)
+    solver = ab.SweepSolver(an, asm, args.nfreq, "mixed", fp64_batch=args.fp64_batch, rtol=args.rtol,
+                            tol=args.tol)
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
 
-    def sweep(record=None):
-        vals, rhs = asm.refill(omegas, stream=stream)
-        if record is not None:
-            record["f0"].record(stream)
-        ok = f32.factorize(vals, 10, 0.0, stream=stream)
-        if record is not None:
-            record["f1"].record(stream)
-        x, iters, berr, conv = f32.solve_refined(vals, rhs, tol=args.tol, max_iters=30, stream=stream)
-        return ok, x, iters, berr, conv, vals, rhs
+    def sweep():
+        return solver.solve(omegas, stream=stream)
 
     for _ in range(args.warmup):
         sweep()
@@ -231,18 +226,17 @@ def run_ours(args):
     barrier()
     torch.cuda.synchronize()
     launches0 = ab.launch_count()
-    step_ms, fact_ms = [], []
+    step_ms = []
     with Clocks(local) as clk:
         t0, t1 = ev(), ev()
         t0.record(stream)
         for _ in range(args.steps):
-            rec = {"s0": ev(), "s1": ev(), "f0": ev(), "f1": ev()}
-            rec["s0"].record(stream)
-            ok, x, iters, berr, conv, vals, rhs = sweep(rec)
-            rec["s1"].record(stream)
+            s0, s1 = ev(), ev()
+            s0.record(stream)
+            x, vals, rhs, reps = sweep()
+            s1.record(stream)
             torch.cuda.synchronize()
-            step_ms.append(rec["s0"].elapsed_time(rec["s1"]))
-            fact_ms.append(rec["f0"].elapsed_time(rec["f1"]))
+            step_ms.append(s0.elapsed_time(s1))
         t1.record(stream)
         torch.cuda.synchronize()
     launches = (ab.launch_count() - launches0) // max(args.steps, 1)
@@ -254,6 +248,16 @@ def run_ours(args):
         elapsed = float(t.item())
     res = ab.residuals(an, vals, x, rhs)
     value = world * args.nfreq * args.steps / (elapsed / 1000.0)
+    # The dominant kernels alone: the batched FP32 factorization, timed with
+    # events on the stream it runs on.
+    fact_ms = []
+    for _ in range(2):
+        a, b = ev(), ev()
+        a.record(stream)
+        solver.f32.factorize(vals, 10, 0.0, stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        fact_ms.append(a.elapsed_time(b))
 
     # End to end through the reference-facing calls with host buffers: refill
     # hands the assembled systems to the host (as refill(SymmetricSystem&)
@@ -271,8 +275,7 @@ def run_ours(args):
         host_rhs.copy_(r, non_blocking=True)
         dvals.copy_(host_vals, non_blocking=True)
         drhs.copy_(host_rhs, non_blocking=True)
-        f32.factorize(dvals, 10, 0.0, stream=stream)
-        xx, _, _, _ = f32.solve_refined(dvals, drhs, tol=args.tol, max_iters=30, stream=stream)
+        xx, _, _, _ = solver.solve(omegas, stream=stream, values=dvals, rhs=drhs)
         host_x.copy_(xx, non_blocking=True)
 
     e2e_step()
@@ -288,34 +291,24 @@ def run_ours(args):
     h2d = 2 * (host_vals.numel() + host_rhs.numel()) * 8
     d2h = 2 * (host_vals.numel() + host_rhs.numel() + host_x.numel()) * 8
 
-    del f32
+    del solver
     torch.cuda.empty_cache()
 
-    # Plain FP64 factorization of the same sweep, in batches that fit.
-    fp64_batch = args.fp64_batch
-    f64 = ab.Factor(an, precision=ab.PREC_FP64, batch=fp64_batch)
-    vals, rhs = asm.refill(omegas, stream=stream)
-
-    def sweep64():
-        xs = []
-        for k0 in range(0, args.nfreq, fp64_batch):
-            sl = slice(k0, k0 + fp64_batch)
-            f64.factorize(vals[sl], 10, 0.0, stream=stream)
-            xs.append(f64.solve(rhs[sl], stream=stream))
-        return torch.cat(xs)
-
-    sweep64()
+    # Plain FP64 factorization of the same sweep (the drop-in path), in
+    # batches that fit beside the workspace.
+    fp64 = ab.SweepSolver(an, asm, args.nfreq, "fp64", fp64_batch=args.fp64_batch)
+    fp64.solve(omegas, stream=stream)
     torch.cuda.synchronize()
     a, b = ev(), ev()
     a.record(stream)
     for _ in range(args.fp64_steps):
-        x64 = sweep64()
+        x64, vals64, rhs64, _ = fp64.solve(omegas, stream=stream)
     b.record(stream)
     torch.cuda.synchronize()
     fp64_ms = a.elapsed_time(b) / args.fp64_steps
-    res64 = ab.residuals(an, vals, x64, rhs)
+    res64 = ab.residuals(an, vals64, x64, rhs64)
     fp64_value = world * args.nfreq / (fp64_ms / 1000.0)
-    del f64
+    del fp64
 
     hbm, bf16, bf16s, src = peaks()
     fact_avg = float(np.mean(fact_ms))
@@ -343,13 +336,15 @@ def run_ours(args):
             "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                            "what": "one sweep of all frequencies (every solve of the batch completes together)"},
             "accuracy": {"max_backward_error": float(res[..., 1].max()), "max_rel_residual": float(res[..., 0].max()),
-                         "ir_iterations_max": int(np.max(iters)), "converged": bool(conv)},
-            "fp64": {"value": fp64_value, "unit": UNIT, "ms_per_sweep": fp64_ms, "batch": fp64_batch,
+                         "fp32_entries": sum(r["precision"] == "fp32" for r in reps),
+                         "fp64_fallback_entries": sum(r["precision"] == "fp64" for r in reps),
+                         "cocg_iterations": [r["iterations"] for r in reps]},
+            "fp64": {"value": fp64_value, "unit": UNIT, "ms_per_sweep": fp64_ms, "batch": args.fp64_batch,
                      "max_rel_residual": float(res64[..., 0].max()),
                      "max_backward_error": float(res64[..., 1].max())},
             "speedup_vs_fp64": value / fp64_value,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"bound": "tensor", "kernel": "supernodal factorization (all update/panel kernels, FP32)",
+            "roofline": {"bound": "tensor", "kernel": "batched FP32 supernodal factorization (equilibration, extend-add, panel and update kernels)",
                          "achieved": achieved, "peak": bf16s, "unit": "TFLOP/s", "frac": achieved / bf16s,
                          "peak_source": f"bf16_tflops_sustained, {src}",
                          "traffic": traffic,
@@ -374,7 +369,9 @@ def main():
     ap.add_argument("--cells", type=int, default=32)
     ap.add_argument("--nfreq", type=int, default=16)
     ap.add_argument("--ordering", default="amd", choices=["amd", "nd"])
-    ap.add_argument("--tol", type=float, default=1e-14)
+    ap.add_argument("--tol", type=float, default=1e-16, help="backward-error target of the refinement")
+    ap.add_argument("--rtol", type=float, default=1e-14,
+                    help="relative-residual target of the refinement (the FP64 direct solve's own level)")
     ap.add_argument("--fp64-batch", type=int, default=4)
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--sample-cells", type=int, default=16)

@@ -101,7 +101,7 @@ class FactorStats(C.Structure):
 
 
 class IROptions(C.Structure):
-    _fields_ = [("max_iters", I), ("tol", D), ("stall_ratio", D)]
+    _fields_ = [("max_iters", I), ("tol", D), ("stall_ratio", D), ("krylov", I), ("rtol", D)]
 
 
 _SIGS = {
@@ -489,7 +489,11 @@ class Factor:
         check(lib().aphi_solve(self._h, nrhs, dptr(bb), dptr(x), stream_ptr(stream)))
         return x.squeeze(1) if squeeze else x
 
-    def solve_refined(self, values, b, tol=1e-14, max_iters=10, stall_ratio=0.5, stream=None):
+    def solve_refined(self, values, b, tol=1e-16, max_iters=40, stall_ratio=0.5, krylov=True, rtol=1e-14,
+                      stream=None):
+        """Refined solve (aphi_solve_refined): preconditioned COCG (krylov=True)
+        or plain refinement, in FP64 on the original systems. Returns x, the
+        iterations and backward error per system, and whether all converged."""
         import torch
         squeeze = b.dim() == 2
         bb = (b.unsqueeze(1) if squeeze else b).contiguous()
@@ -497,7 +501,7 @@ class Factor:
         x = torch.empty_like(bb)
         it = (C.c_int * (self.batch * nrhs))()
         be = (C.c_double * (self.batch * nrhs))()
-        opt = IROptions(max_iters, tol, stall_ratio)
+        opt = IROptions(max_iters, tol, stall_ratio, 1 if krylov else 0, rtol)
         rc = lib().aphi_solve_refined(self._h, nrhs, dptr(values), dptr(bb), dptr(x), C.byref(opt), it, be,
                                       stream_ptr(stream))
         if rc not in (OK, ERR_IR_STALL):
@@ -571,3 +575,71 @@ def solve_symmetric(analysis: Analysis, values: np.ndarray, b: np.ndarray, equil
         return False, x, report
     check(rc)
     return True, x, report
+
+
+# ---------------------------------------------------------------- frequency sweeps
+class SweepSolver:
+    """Frequency batching over one mesh: every frequency of a sweep shares the
+    pattern and the supernodal schedule, so fills, factorizations and refined
+    solves run as batched launches over all of them.
+
+    precision="mixed": the batch is factorized in FP32 and refined by FP64
+    preconditioned COCG on the original systems to the FP64 direct solve's
+    own residual level (rtol); an entry whose refinement stalls (cond(A) *
+    eps(FP32) too large -- the high-frequency end of the cylinder sweep) is
+    refactorized in FP64 automatically. precision="fp64": the plain FP64
+    factorization for every entry (the drop-in path).
+    """
+
+    def __init__(self, analysis: Analysis, assembly: Assembly, batch: int, precision: str = "mixed",
+                 fp64_batch: int = 4, rtol: float = 1e-14, tol: float = 1e-16, max_iters: int = 40):
+        self.analysis, self.assembly = analysis, assembly
+        self.batch, self.precision = batch, precision
+        self.rtol, self.tol, self.max_iters = rtol, tol, max_iters
+        self.fp64_batch = max(1, min(fp64_batch, batch))
+        self.f32 = Factor(analysis, PREC_FP32, batch) if precision == "mixed" else None
+        self.f64 = Factor(analysis, PREC_FP64, self.fp64_batch)
+
+    def solve(self, omegas, conditioning=COND_ROW_SCALED, stream=None, values=None, rhs=None):
+        """Returns (x [batch, n], values, rhs, per-entry reports), all device
+        tensors. values/rhs, when given, are already-assembled systems (the
+        drop-in flow, where refill handed them to the host and back);
+        otherwise the sweep is assembled on the device first."""
+        import torch
+        om = np.asarray(omegas, dtype=np.float64)
+        if om.size != self.batch:
+            raise InvalidArgument(ERR_BAD_SHAPE, f"SweepSolver: {om.size} frequencies for a batch of {self.batch}")
+        if values is None or rhs is None:
+            vals, rhs = self.assembly.refill(om, conditioning, stream=stream)
+        else:
+            vals = values
+        reports = [dict(omega=float(w), precision="fp32", iterations=0) for w in om]
+        todo = list(range(self.batch))
+        if self.f32 is not None:
+            self.f32.factorize(vals, 10, 0.0, stream=stream)
+            x, iters, berr, _ = self.f32.solve_refined(vals, rhs, tol=self.tol, rtol=self.rtol,
+                                                       max_iters=self.max_iters, stream=stream)
+            res = residuals(self.analysis, vals, x, rhs, stream=stream)
+            todo = []
+            for k in range(self.batch):
+                reports[k]["iterations"] = int(iters[k, 0])
+                if not (res[k, 0, 0] <= self.rtol and res[k, 0, 1] <= self.tol):
+                    todo.append(k)
+        else:
+            x = torch.empty_like(rhs)
+        for c in range(0, len(todo), self.fp64_batch):
+            idx = todo[c:c + self.fp64_batch]
+            sel = torch.tensor(idx, device=vals.device)
+            v = torch.zeros((self.fp64_batch, vals.shape[1]), dtype=vals.dtype, device=vals.device)
+            b = torch.zeros((self.fp64_batch, rhs.shape[1]), dtype=rhs.dtype, device=rhs.device)
+            v[:len(idx)] = vals.index_select(0, sel)
+            b[:len(idx)] = rhs.index_select(0, sel)
+            if len(idx) < self.fp64_batch:      # pad with a copy of the first entry
+                v[len(idx):] = v[0]
+                b[len(idx):] = b[0]
+            self.f64.factorize(v, 10, 0.0, stream=stream)
+            xs = self.f64.solve(b, stream=stream)
+            x.index_copy_(0, sel, xs[:len(idx)])
+            for k in idx:
+                reports[k]["precision"] = "fp64"
+        return x, vals, rhs, reports

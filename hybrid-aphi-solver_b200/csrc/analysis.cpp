@@ -252,6 +252,7 @@ void analysis_info(const aphi_analysis* a, double* info) {
 }  // namespace aphi_b200
 
 aphi_analysis::~aphi_analysis() {
+    if (ws) cudaFree(ws);
     void* ptrs[] = {d.first, d.rows, d.loff, d.cboff, d.soff, d.structs, d.reloff, d.rel, d.child_ptr,
                     d.child_list, d.uoff, d.a_dest, d.row_ptr, d.col_idx, d.new_of_orig, d.orig_of_new,
                     d.ref_of_post, d.fptr, d.fcol, d.fmap, d.items};

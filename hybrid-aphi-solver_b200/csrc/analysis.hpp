@@ -80,6 +80,8 @@ struct aphi_analysis {
     std::vector<int> h_fptr, h_fcol;
     std::vector<long long> h_fmap;
     bool on_device = false;
+    void* ws = nullptr;    // contribution-block workspace shared by this analysis's factors
+    size_t ws_bytes = 0;
     long long num_items = 0;
     long long upool = 0;   // update-vector pool entries (per rhs)
     int max_parts = 1;

@@ -80,7 +80,7 @@ int aphi_solve_refined(aphi_factor* f, int nrhs, const double* values_dev, const
     const int g = guard([&] {
         if (!f || !values_dev || !b_dev || !x_dev || !iters || !berr)
             throw Error(APHI_ERR_INVALID, "aphi_solve_refined: null argument");
-        aphi_ir_options o{10, 1e-14, 0.5};
+        aphi_ir_options o{40, 1e-16, 0.5, 1, 1e-14};
         if (opt) o = *opt;
         rc = solve_refined(f, nrhs, values_dev, b_dev, x_dev, o, iters, berr, as_stream(stream));
         if (rc == APHI_ERR_IR_STALL) g_last_error = "iterative refinement stalled before reaching the tolerance";

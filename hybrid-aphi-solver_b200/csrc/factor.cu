@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -355,13 +356,16 @@ aphi_factor* factor_create(aphi_analysis* an, int precision, int batch) {
         f->precision = precision;
         f->batch = batch;
         f->elem = precision == 64 ? 16 : 8;
+        const char* no_tc = std::getenv("APHI_NO_TC");
+        f->use_tc = !(no_tc && no_tc[0] == '1');
         const Symbolic& S = an->S;
         APHI_CUDA(cudaMalloc(&f->L, static_cast<size_t>(std::max<long long>(S.stored, 1)) * batch * f->elem));
-        APHI_CUDA(cudaMalloc(&f->CB, static_cast<size_t>(std::max<long long>(S.cb_pool, 1)) * batch * f->elem));
         f->dscale = dalloc<double>(static_cast<size_t>(S.n) * batch);
         f->rowmax = dalloc<unsigned long long>(static_cast<size_t>(S.n) * batch);
         f->stats = dalloc<unsigned long long>(4 * static_cast<size_t>(batch));
         f->dref = dalloc<double>(2 * static_cast<size_t>(S.n) * batch);
+        f->err = dalloc<int>(4);
+        APHI_CUDA(cudaMemset(f->err, 0, 4 * sizeof(int)));
         f->host_stats.assign(batch, aphi_factor_stats{});
     } catch (...) {
         delete f;
@@ -397,6 +401,24 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
         APHI_CHECK_LAUNCH();
         k_eq_update<<<g, kEqThreads, 0, st>>>(n, f->dscale, f->rowmax);
         APHI_CHECK_LAUNCH();
+    }
+    // The contribution-block pool is only live during a factorization, so it
+    // is a workspace owned by the analysis and shared by every factor made
+    // from it (their factorizations are ordered on the caller's streams).
+    {
+        aphi_analysis* an = f->an;
+        const size_t need = static_cast<size_t>(std::max<long long>(S.cb_pool, 1)) * B * f->elem;
+        if (an->ws_bytes < need) {
+            if (an->ws) {
+                APHI_CUDA(cudaDeviceSynchronize());
+                cudaFree(an->ws);
+                an->ws = nullptr;
+                an->ws_bytes = 0;
+            }
+            APHI_CUDA(cudaMalloc(&an->ws, need));
+            an->ws_bytes = need;
+        }
+        f->CB = an->ws;
     }
     if (f->precision == 64)
         factorize_numeric<double>(f, values, st);
@@ -611,8 +633,12 @@ void residuals_noalloc(const aphi_analysis* an, int batch, int nrhs, const doubl
     APHI_CUDA(cudaStreamSynchronize(st));
 }
 
+int solve_krylov(aphi_factor* f, int nrhs, const double* values, const double* b, double* x,
+                 const aphi_ir_options& opt, int* iters, double* berr, cudaStream_t st);
+
 int solve_refined(aphi_factor* f, int nrhs, const double* values, const double* b, double* x,
                   const aphi_ir_options& opt, int* iters, double* berr, cudaStream_t st) {
+    if (opt.krylov) return solve_krylov(f, nrhs, values, b, x, opt, iters, berr, st);
     const aphi_analysis* A = f->an;
     const int n = A->S.n;
     const int B = f->batch;
@@ -655,9 +681,10 @@ int solve_refined(aphi_factor* f, int nrhs, const double* values, const double* 
             if (done[k]) continue;
             const double den = h[4 * k + 3] * h[4 * k + 2] + h[4 * k + 1];
             const double e = den > 0.0 ? h[4 * k] / den : h[4 * k];
+            const double rr = h[4 * k + 1] > 0.0 ? h[4 * k] / h[4 * k + 1] : h[4 * k];
             berr[k] = e;
             iters[k] = it[k];
-            if (e <= opt.tol) {
+            if (e <= opt.tol && rr <= opt.rtol) {
                 done[k] = 1;
                 continue;
             }
@@ -677,6 +704,254 @@ int solve_refined(aphi_factor* f, int nrhs, const double* values, const double* 
         APHI_CHECK_LAUNCH();
         for (int k = 0; k < q; ++k)
             if (!done[k]) ++it[k];
+    }
+    return status;
+}
+
+// ---------------------------------------------------------------- Krylov refinement
+// Preconditioned COCG (conjugate orthogonal CG: CG with the unconjugated
+// bilinear form x^T y, valid for complex symmetric A and M) in FP64 on the
+// original system, with the factor as preconditioner M^-1. With an FP32
+// factor this is refinement whose residual, scaling and update stay in FP64;
+// the Krylov recurrence keeps it converging where plain refinement
+// (x += M^-1 r) stalls because cond(A) * eps_fp32 approaches 1. The residual
+// is recomputed from x every iteration (b - A x), so the reported backward
+// error is the true one. Systems are advanced together and frozen one by one
+// as they converge.
+
+// y = A x for q systems.
+__global__ void k_spmv(int n, int nrhs, const int* fptr, const int* fcol, const long long* fmap,
+                       const double* values, long long nnz, const double* x, double* y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    if (i >= n) return;
+    const double* v = values + 2LL * nnz * (k / nrhs);
+    const double* xk = x + 2LL * n * k;
+    double ar = 0, ai = 0;
+    for (int t = fptr[i]; t < fptr[i + 1]; ++t) {
+        const long long q = fmap[t];
+        const double vr = v[2 * q], vi = v[2 * q + 1];
+        const double xr = xk[2 * fcol[t]], xi = xk[2 * fcol[t] + 1];
+        ar += vr * xr - vi * xi;
+        ai += vr * xi + vi * xr;
+    }
+    y[2LL * n * k + 2 * i] = ar;
+    y[2LL * n * k + 2 * i + 1] = ai;
+}
+
+// partial[k][blk] = sum over the block's entries of a_i b_i (unconjugated).
+__global__ void k_dot_partial(int n, const double* a, const double* b, double* partial) {
+    __shared__ double sh[2][256];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    double re = 0, im = 0;
+    if (i < n) {
+        const double ar = a[2LL * n * k + 2 * i], ai = a[2LL * n * k + 2 * i + 1];
+        const double br = b[2LL * n * k + 2 * i], bi = b[2LL * n * k + 2 * i + 1];
+        re = ar * br - ai * bi;
+        im = ar * bi + ai * br;
+    }
+    sh[0][threadIdx.x] = re;
+    sh[1][threadIdx.x] = im;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + o];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partial[2 * (static_cast<long long>(k) * gridDim.x + blockIdx.x)] = sh[0][0];
+        partial[2 * (static_cast<long long>(k) * gridDim.x + blockIdx.x) + 1] = sh[1][0];
+    }
+}
+
+__device__ __forceinline__ void cdiv_dev(double ar, double ai, double br, double bi, double& cr, double& ci) {
+    if (fabs(br) >= fabs(bi)) {
+        const double r = bi / br, den = br + bi * r;
+        cr = (ar + ai * r) / den;
+        ci = (ai - ar * r) / den;
+    } else {
+        const double r = br / bi, den = br * r + bi;
+        cr = (ar * r + ai) / den;
+        ci = (ai * r - ar) / den;
+    }
+}
+
+// Fixed-order sum of the partials, then the COCG scalar of each system.
+//   mode 0: rho = r^T z (start)            -> rho
+//   mode 1: alpha = rho / (p^T A p)        -> alpha (0 for frozen systems)
+//   mode 2: rho' = r^T z, beta = rho'/rho  -> beta, rho = rho'
+__global__ void k_cocg_scalar(int nblocks, const double* partial, const int* active, double* rho, double* alpha,
+                              double* beta, int mode) {
+    __shared__ double sh[2][256];
+    const int k = blockIdx.x;
+    double re = 0, im = 0;
+    for (int t = threadIdx.x; t < nblocks; t += blockDim.x) {
+        re += partial[2 * (static_cast<long long>(k) * nblocks + t)];
+        im += partial[2 * (static_cast<long long>(k) * nblocks + t) + 1];
+    }
+    sh[0][threadIdx.x] = re;
+    sh[1][threadIdx.x] = im;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + o];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    const double sr = sh[0][0], si = sh[1][0];
+    if (mode == 0) {
+        rho[2 * k] = sr;
+        rho[2 * k + 1] = si;
+    } else if (mode == 1) {
+        double ar = 0, ai = 0;
+        if (active[k] && (sr != 0.0 || si != 0.0)) cdiv_dev(rho[2 * k], rho[2 * k + 1], sr, si, ar, ai);
+        alpha[2 * k] = ar;
+        alpha[2 * k + 1] = ai;
+    } else {
+        double br = 0, bi = 0;
+        if (active[k] && (rho[2 * k] != 0.0 || rho[2 * k + 1] != 0.0)) cdiv_dev(sr, si, rho[2 * k], rho[2 * k + 1], br, bi);
+        beta[2 * k] = br;
+        beta[2 * k + 1] = bi;
+        if (active[k]) {
+            rho[2 * k] = sr;
+            rho[2 * k + 1] = si;
+        }
+    }
+}
+
+// x += alpha p (per system).
+__global__ void k_axpy_sys(int n, const double* alpha, const double* p, double* x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    if (i >= n) return;
+    const double ar = alpha[2 * k], ai = alpha[2 * k + 1];
+    if (ar == 0.0 && ai == 0.0) return;
+    const long long at = 2LL * n * k + 2 * i;
+    const double pr = p[at], pi = p[at + 1];
+    x[at] += ar * pr - ai * pi;
+    x[at + 1] += ar * pi + ai * pr;
+}
+
+// p = z + beta p (active systems only).
+__global__ void k_xpby_sys(int n, const int* active, const double* beta, const double* z, double* p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    if (i >= n || !active[k]) return;
+    const double br = beta[2 * k], bi = beta[2 * k + 1];
+    const long long at = 2LL * n * k + 2 * i;
+    const double pr = p[at], pi = p[at + 1];
+    p[at] = z[at] + br * pr - bi * pi;
+    p[at + 1] = z[at + 1] + br * pi + bi * pr;
+}
+
+int solve_krylov(aphi_factor* f, int nrhs, const double* values, const double* b, double* x,
+                 const aphi_ir_options& opt, int* iters, double* berr, cudaStream_t st) {
+    const aphi_analysis* A = f->an;
+    const int n = A->S.n;
+    const int B = f->batch;
+    const int q = B * nrhs;
+    const long long len = 2LL * n * q;
+    const int nb = ceil_div(std::max(n, 1), 256);
+    if (f->kr_cap < nrhs) {
+        if (f->kr) cudaFree(f->kr);
+        // r, z, p, Ap; partials (3 per block per system); norms, rho, alpha,
+        // beta; max|A| words; active flags
+        f->kr = dalloc<double>(static_cast<size_t>(4 * len + 3LL * nb * q + 11LL * q + B + 16));
+        f->kr_cap = nrhs;
+    }
+    double* r = f->kr;
+    double* z = r + len;
+    double* p = z + len;
+    double* Ap = p + len;
+    double* partial = Ap + len;                 // 3 * nb * q
+    double* norms = partial + 3LL * nb * q;     // 4 * q
+    double* rho = norms + 4LL * q;              // 2 * q
+    double* alpha = rho + 2LL * q;              // 2 * q
+    double* beta = alpha + 2LL * q;             // 2 * q
+    unsigned long long* amax = reinterpret_cast<unsigned long long*>(beta + 2LL * q);  // B
+    int* active = reinterpret_cast<int*>(amax + B);                                   // q ints
+    const dim3 gv(nb, q);
+
+    APHI_CUDA(cudaMemsetAsync(amax, 0, sizeof(unsigned long long) * B, st));
+    k_amax<<<dim3(ceil_div(std::max<long long>(A->S.nnz_a, 1), 256), B), 256, 0, st>>>(values, A->S.nnz_a, amax);
+    APHI_CHECK_LAUNCH();
+    std::vector<int> act(q, 1), it(q, 0), since(q, 0);
+    std::vector<double> h(4 * static_cast<size_t>(q)), best(q, INFINITY);
+    APHI_CUDA(cudaMemcpyAsync(active, act.data(), sizeof(int) * q, cudaMemcpyHostToDevice, st));
+
+    auto residual = [&]() {  // r = b - A x; norms to the host
+        k_residual<<<gv, 256, 0, st>>>(n, nrhs, A->d.fptr, A->d.fcol, A->d.fmap, values, A->S.nnz_a, x, b, r,
+                                       partial);
+        APHI_CHECK_LAUNCH();
+        k_norms_final<<<q, 256, 0, st>>>(nb, nrhs, partial, amax, norms);
+        APHI_CHECK_LAUNCH();
+        APHI_CUDA(cudaMemcpyAsync(h.data(), norms, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        APHI_CUDA(cudaStreamSynchronize(st));
+    };
+    auto dot = [&](const double* u, const double* v, int mode) {
+        k_dot_partial<<<gv, 256, 0, st>>>(n, u, v, partial);
+        APHI_CHECK_LAUNCH();
+        k_cocg_scalar<<<q, 256, 0, st>>>(nb, partial, active, rho, alpha, beta, mode);
+        APHI_CHECK_LAUNCH();
+    };
+
+    solve(f, nrhs, b, x, st);  // x0 = M^-1 b
+    residual();
+    int status = APHI_OK;
+    bool started = false;
+    for (;;) {
+        bool any = false;
+        for (int k = 0; k < q; ++k) {
+            if (!act[k]) continue;
+            const double den = h[4 * k + 3] * h[4 * k + 2] + h[4 * k + 1];
+            const double e = den > 0.0 ? h[4 * k] / den : h[4 * k];
+            const double rr = h[4 * k + 1] > 0.0 ? h[4 * k] / h[4 * k + 1] : h[4 * k];
+            berr[k] = e;
+            iters[k] = it[k];
+            if (e <= opt.tol && rr <= opt.rtol) {
+                act[k] = 0;
+                continue;
+            }
+            if (rr < opt.stall_ratio * best[k]) {
+                best[k] = rr;
+                since[k] = 0;
+            } else if (++since[k] >= 3 || !(rr == rr)) {
+                act[k] = 0;
+                status = APHI_ERR_IR_STALL;
+                continue;
+            }
+            if (it[k] >= opt.max_iters) {
+                act[k] = 0;
+                status = APHI_ERR_IR_STALL;
+                continue;
+            }
+            any = true;
+        }
+        if (!any) break;
+        APHI_CUDA(cudaMemcpyAsync(active, act.data(), sizeof(int) * q, cudaMemcpyHostToDevice, st));
+        solve(f, nrhs, r, z, st);  // z = M^-1 r
+        if (!started) {
+            APHI_CUDA(cudaMemcpyAsync(p, z, sizeof(double) * len, cudaMemcpyDeviceToDevice, st));
+            dot(r, z, 0);
+            started = true;
+        } else {
+            dot(r, z, 2);
+            k_xpby_sys<<<gv, 256, 0, st>>>(n, active, beta, z, p);
+            APHI_CHECK_LAUNCH();
+        }
+        k_spmv<<<gv, 256, 0, st>>>(n, nrhs, A->d.fptr, A->d.fcol, A->d.fmap, values, A->S.nnz_a, p, Ap);
+        APHI_CHECK_LAUNCH();
+        dot(p, Ap, 1);
+        k_axpy_sys<<<gv, 256, 0, st>>>(n, alpha, p, x);
+        APHI_CHECK_LAUNCH();
+        for (int k = 0; k < q; ++k)
+            if (act[k]) ++it[k];
+        residual();
     }
     return status;
 }
@@ -758,7 +1033,7 @@ void factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, do
 }  // namespace aphi_b200
 
 aphi_factor::~aphi_factor() {
-    void* ptrs[] = {L, CB, dscale, rowmax, stats, dref, y, U, part, ir, red, norms};
+    void* ptrs[] = {L, dscale, rowmax, stats, dref, y, U, part, ir, red, norms, kr, err};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }

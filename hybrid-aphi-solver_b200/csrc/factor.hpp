@@ -15,7 +15,7 @@ struct aphi_factor {
     int batch = 1;
     size_t elem = 16;          // bytes per complex entry
     void* L = nullptr;         // batch x stored
-    void* CB = nullptr;        // batch x cb_pool
+    void* CB = nullptr;        // batch x cb_pool: the analysis's workspace, set at factorize
     double* dscale = nullptr;  // batch x n, original numbering
     unsigned long long* rowmax = nullptr;  // batch x n (equilibration scratch)
     unsigned long long* stats = nullptr;   // batch x 4 (max|L| bits, ...)
@@ -31,7 +31,11 @@ struct aphi_factor {
     double* red = nullptr;     // reduction partials
     double* norms = nullptr;   // batch x nrhs x 4
     int red_cap = 0;
+    double* kr = nullptr;      // Krylov refinement scratch
+    int kr_cap = 0;
     bool factored = false;
+    bool use_tc = true;         // FP32: tensor-core updates (APHI_NO_TC=1 selects the SIMT kernels)
+    int* err = nullptr;         // device error word (bounded waits)
     std::vector<aphi_factor_stats> host_stats;
     ~aphi_factor();
 };

@@ -251,13 +251,22 @@ int aphi_residuals_noalloc(const aphi_analysis* an, int batch, int nrhs, const d
                            const double* x_dev, const double* b_dev, double* out, void* stream);
 
 /* Iterative refinement (new; include/aphi_solver/factorization.hpp:27-30 names
- * it as future work): x <- x + solve(r), r = b - A x in FP64 on the original
- * system, until backward error <= tol or max_iters; stall (error not halving)
- * returns IR_STALL. f may be FP32 or FP64. iters/berr: per batch x rhs, host. */
+ * it as future work). The residual r = b - A x, the equilibration scaling and
+ * the update stay in FP64 on the original system; the factor (FP32 or FP64)
+ * supplies the correction. krylov = 0: plain refinement x += M^-1 r.
+ * krylov = 1: preconditioned COCG (CG with the unconjugated bilinear form,
+ * for complex symmetric A), which keeps converging where plain refinement
+ * stalls because cond(A) * eps(FP32) approaches 1. A system is done when
+ * its backward error <= tol AND its relative residual ||b - A x|| / ||b|| <=
+ * rtol; one whose relative residual has not dropped by stall_ratio in 3
+ * steps, or that reaches max_iters, is frozen and IR_STALL returned -- the
+ * caller's cue to refactorize it in FP64. iters/berr: per batch x rhs. */
 typedef struct {
     int max_iters;
     double tol;               /* target backward error */
-    double stall_ratio;       /* stall when new_err > stall_ratio * old_err */
+    double stall_ratio;       /* progress needed: new < stall_ratio * best relative residual */
+    int krylov;               /* 0 plain refinement, 1 preconditioned COCG */
+    double rtol;              /* target relative residual */
 } aphi_ir_options;
 int aphi_solve_refined(aphi_factor* f, int nrhs, const double* values_dev, const double* b_dev,
                        double* x_dev, const aphi_ir_options* opt, int* iters, double* berr,
