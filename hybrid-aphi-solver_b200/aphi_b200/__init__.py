@@ -137,6 +137,8 @@ _SIGS = {
     "aphi_solve_refined": (I, [P, I, P, P, P, C.POINTER(IROptions), PI, PD, P]),
     "aphi_residuals_noalloc": (I, [P, I, I, P, P, P, PD, P]),
     "aphi_solve_symmetric_host": (I, [P, PD, PD, I, D, PD, PD]),
+    "aphi_selftest_tc_tile": (I, [I, I, I, I, P, P, P]),
+    "aphi_analysis_plan_stats": (I, [P, I, PI64, PI64]),
 }
 
 
@@ -421,6 +423,17 @@ class Analysis:
         self.nnz = int(self.info["nnz_upper"])
         self.row_ptr, self.col_idx = rp, ci
 
+    PLAN_KINDS = ["extend_add", "small_front", "diag_block", "panel_rows", "update_wide", "fwd_gather", "fwd_diag",
+                  "fwd_update", "bwd_update", "bwd_diag", "update_panel", "update_tc"]
+
+    def plan_stats(self, plan: int) -> dict:
+        """{kind: (launches, items)} of launch plan `plan` (0 factorization,
+        1 tensor-core factorization, 2 forward solve, 3 backward solve)."""
+        la = np.zeros(12, np.int64)
+        it = np.zeros(12, np.int64)
+        check(lib().aphi_analysis_plan_stats(self._h, plan, la.ctypes.data_as(PI64), it.ctypes.data_as(PI64)))
+        return {k: (int(a), int(b)) for k, a, b in zip(self.PLAN_KINDS, la, it) if a}
+
     def etree(self):
         parent = np.zeros(self.n, np.int32)
         cc = np.zeros(self.n, np.int32)
@@ -547,6 +560,20 @@ def residuals(analysis: Analysis, values, x, b, stream=None) -> np.ndarray:
     check(lib().aphi_residuals(analysis._h, batch, nrhs, dptr(values), dptr(xx.contiguous()),
                                dptr(bb.contiguous()), out.ctypes.data_as(PD), None))
     return out
+
+
+def tc_tile_selftest(P: np.ndarray, i0: int, j0: int, d: np.ndarray | None = None) -> np.ndarray:
+    """One tensor-core update tile: the 128 x 64 complex64 block
+    sum_k (P[i0 + r, k] d[k]) P[j0 + c, k] (rows of P past its end read as
+    zero), computed by the kernel the FP32 factorization uses."""
+    Pc = np.asfortranarray(P, np.complex64)
+    rows, K = Pc.shape
+    dd = None if d is None else np.ascontiguousarray(d, np.complex64)
+    out = np.zeros((64, 128), np.complex64)
+    check(lib().aphi_selftest_tc_tile(rows, K, i0, j0, C.c_void_p(Pc.ctypes.data),
+                                      None if dd is None else C.c_void_p(dd.ctypes.data),
+                                      C.c_void_p(out.ctypes.data)))
+    return out.T
 
 
 REPORT_KEYS = ["ok", "backward_error", "residual", "equilibration_min", "equilibration_max", "smallest_pivot",

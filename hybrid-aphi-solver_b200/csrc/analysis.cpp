@@ -3,6 +3,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "tc_config.hpp"
 
 namespace aphi_b200 {
 
@@ -18,12 +19,18 @@ T* upload(const std::vector<T>& h, long long& bytes) {
     return d;
 }
 
-// The factorization plan: per level, extend-add items, then one-CTA fronts,
-// then the blocked steps of the large fronts (diagonal block, panel rows,
-// trailing update), step by step.
-void build_plans(aphi_analysis& A, std::vector<Item>& items) {
+// The factorization plans: per level, extend-add items, then one-CTA fronts,
+// then the blocked steps of the large fronts. A large front is processed in
+// 128-column panels; each 32-column step of a panel factors its diagonal
+// block, solves the panel rows below it and updates the rest of the panel's
+// own columns. Once a panel is complete, its trailing update -- every column
+// to its right, K = panel width -- runs as 128 x 64 tiles: `trailing` is
+// K_UPDATE_WIDE (SIMT, either precision) or K_UPDATE_TC (tensor cores, FP32).
+// Updating the trailing front once per 128 columns instead of once per 32
+// reads and writes it a quarter as often.
+void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing, std::vector<Launch>& plan) {
     const Symbolic& S = A.S;
-    auto push = [&](std::vector<Launch>& plan, int kind, long long first) {
+    auto push = [&](int kind, long long first) {
         const int count = static_cast<int>(items.size() - first);
         if (count > 0) plan.push_back({kind, first, count});
     };
@@ -40,7 +47,7 @@ void build_plans(aphi_analysis& A, std::vector<Item>& items) {
             for (int c = c0 - (c0 % kEaCols); c < m; c += kEaCols)
                 if (kids || m > w) items.push_back({s, c, 0, 0});
         }
-        push(A.plan_factor, K_EXTEND_ADD, f0);
+        push(K_EXTEND_ADD, f0);
         f0 = static_cast<long long>(items.size());
         std::vector<int> large;
         for (const int* p = lb; p < le; ++p) {
@@ -49,34 +56,62 @@ void build_plans(aphi_analysis& A, std::vector<Item>& items) {
             else
                 large.push_back(*p);
         }
-        push(A.plan_factor, K_SMALL, f0);
+        push(K_SMALL, f0);
         int maxw = 0;
         for (int s : large) maxw = std::max(maxw, S.sn_first[s + 1] - S.sn_first[s]);
+        auto width = [&](int s) { return S.sn_first[s + 1] - S.sn_first[s]; };
         for (int k0 = 0; k0 < maxw; k0 += kStep) {
             f0 = static_cast<long long>(items.size());
             for (int s : large)
-                if (k0 < S.sn_first[s + 1] - S.sn_first[s]) items.push_back({s, k0, 0, 0});
-            push(A.plan_factor, K_DIAG, f0);
+                if (k0 < width(s)) items.push_back({s, k0, 0, 0});
+            push(K_DIAG, f0);
             f0 = static_cast<long long>(items.size());
             for (int s : large) {
-                const int w = S.sn_first[s + 1] - S.sn_first[s];
+                const int w = width(s);
                 if (k0 >= w) continue;
                 const int k1 = std::min(w, k0 + kStep);
                 for (int r = k1; r < S.sn_rows[s]; r += kTrsmRows) items.push_back({s, k0, r, 0});
             }
-            push(A.plan_factor, K_TRSM, f0);
+            push(K_TRSM, f0);
             f0 = static_cast<long long>(items.size());
             for (int s : large) {
-                const int w = S.sn_first[s + 1] - S.sn_first[s];
+                const int w = width(s);
                 if (k0 >= w) continue;
                 const int k1 = std::min(w, k0 + kStep);
                 const int m = S.sn_rows[s];
-                for (int j = k1; j < m; j += kTile)
+                const int jend = std::min(w, (k0 / kTcPanel) * kTcPanel + kTcPanel);
+                for (int j = k1; j < jend; j += kTile)
                     for (int i = j; i < m; i += kTile) items.push_back({s, k0, i, j});
             }
-            push(A.plan_factor, K_UPDATE, f0);
+            push(K_UPDATE_PANEL, f0);
+            // A panel's trailing update follows its last 32-column step.
+            f0 = static_cast<long long>(items.size());
+            for (int s : large) {
+                const int w = width(s);
+                if (k0 >= w) continue;
+                const bool panel_done = (k0 + kStep) % kTcPanel == 0 || k0 + kStep >= w;
+                if (!panel_done) continue;
+                const int p0 = (k0 / kTcPanel) * kTcPanel;
+                const int pe = std::min(w, p0 + kTcPanel);
+                const int m = S.sn_rows[s];
+                for (int j = pe; j < m; j += kTcN)
+                    for (int i = pe; i < m; i += kTcM)
+                        if (i + kTcM > j) items.push_back({s, p0, i, j});
+            }
+            push(trailing, f0);
         }
     }
+}
+
+// The solve plans and the statistics pass.
+void build_plans(aphi_analysis& A, std::vector<Item>& items) {
+    const Symbolic& S = A.S;
+    auto push = [&](std::vector<Launch>& plan, int kind, long long first) {
+        const int count = static_cast<int>(items.size() - first);
+        if (count > 0) plan.push_back({kind, first, count});
+    };
+    build_factor_plan(A, items, K_UPDATE_WIDE, A.plan_factor);
+    build_factor_plan(A, items, K_UPDATE_TC, A.plan_factor_tc);
     // Statistics pass over the panels: 32 columns per item.
     {
         const long long f0 = static_cast<long long>(items.size());

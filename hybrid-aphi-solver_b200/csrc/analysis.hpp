@@ -18,12 +18,14 @@ enum Kind : int {
     K_SMALL = 1,       // (s): whole front in shared memory
     K_DIAG = 2,        // (s, k0): factor the diagonal block of step k0
     K_TRSM = 3,        // (s, k0, row0): rows row0.. of L21 for step k0
-    K_UPDATE = 4,      // (s, k0, i0, j0): trailing update tile
+    K_UPDATE_WIDE = 4,  // (s, p0, i0, j0): SIMT trailing update by a whole panel
     K_FWD_GATHER = 5,  // (s): children's update vectors into the front vector
     K_FWD_DIAG = 6,    // (s, blk): unit-triangle solve of a 64-column block
     K_FWD_UPDATE = 7,  // (s, blk, row0): rows below the block
     K_BWD_UPDATE = 8,  // (s, blk, row0, slot): partial L^T x sums over a row chunk
     K_BWD_DIAG = 9,    // (s, blk, first slot, slots): block of the transposed solve
+    K_UPDATE_PANEL = 10,  // (s, k0, i0, j0): update tile restricted to the current 128-column panel
+    K_UPDATE_TC = 11,     // (s, p0, i0, j0): tensor-core trailing update by a whole panel
 };
 
 struct Launch {
@@ -73,7 +75,7 @@ struct aphi_analysis {
     aphi_b200::Symbolic S;
     aphi_analysis_options opt{};
     aphi_b200::DeviceSchedule d;
-    std::vector<aphi_b200::Launch> plan_factor, plan_fwd, plan_bwd;
+    std::vector<aphi_b200::Launch> plan_factor, plan_factor_tc, plan_fwd, plan_bwd;
     std::vector<aphi_b200::Item> h_items;
     std::vector<long long> h_uoff;
     std::vector<int> h_row_ptr, h_col_idx;

@@ -47,4 +47,18 @@ int aphi_analysis_etree(const aphi_analysis* a, int* parent, int* col_count) {
     });
 }
 
+int aphi_analysis_plan_stats(const aphi_analysis* a, int plan, int64_t* launches, int64_t* items) {
+    return guard([&] {
+        if (!a || !launches || !items) throw Error(APHI_ERR_INVALID, "aphi_analysis_plan_stats: null argument");
+        const std::vector<Launch>* plans[] = {&a->plan_factor, &a->plan_factor_tc, &a->plan_fwd, &a->plan_bwd};
+        if (plan < 0 || plan > 3) throw Error(APHI_ERR_BAD_SHAPE, "aphi_analysis_plan_stats: plan is 0..3");
+        for (int k = 0; k < APHI_PLAN_KINDS; ++k) launches[k] = items[k] = 0;
+        for (const Launch& l : *plans[plan]) {
+            if (l.kind < 0 || l.kind >= APHI_PLAN_KINDS) continue;
+            ++launches[l.kind];
+            items[l.kind] += l.count;
+        }
+    });
+}
+
 }  // extern "C"

@@ -262,8 +262,17 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
             case K_SMALL: k_small_front<R><<<grid, 256, smallsm, st>>>(S, l.first, L, CB, ls, cs); break;
             case K_DIAG: k_diag_block<R><<<grid, 128, 0, st>>>(S, l.first, L, ls); break;
             case K_TRSM: k_panel_trsm<R><<<grid, kTrsmRows, 0, st>>>(S, l.first, L, ls); break;
-            case K_UPDATE:
-                k_update_tile<R><<<grid, 256, 2 * kStep * kTile * sizeof(cx<R>), st>>>(S, l.first, L, CB, ls, cs);
+            case K_UPDATE_WIDE:
+                k_update_wide<R><<<grid, 256, wide_smem<R>(), st>>>(S, l.first, L, CB, ls, cs);
+                break;
+            case K_UPDATE_PANEL:
+                k_update_panel<R><<<grid, 256, 2 * kStep * kTile * sizeof(cx<R>), st>>>(S, l.first, L, CB, ls, cs);
+                break;
+            case K_UPDATE_TC:
+                if constexpr (sizeof(R) == 4)
+                    k_update_tc<<<grid, kTcThreads, kTcSmem, st>>>(S, l.first, L, CB, ls, cs, f->err);
+                else
+                    throw Error(APHI_ERR_INVALID, "tensor-core update planned for an FP64 factor");
                 break;
             case K_FWD_GATHER: k_fwd_gather<R><<<grid, 256, 0, st>>>(S, l.first, *sa, y, U); break;
             case K_FWD_DIAG:
@@ -285,8 +294,11 @@ void set_smem_limits(int small_front) {
     if (done) return;
     APHI_CUDA(cudaFuncSetAttribute(k_small_front<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    96 * 96 * static_cast<int>(sizeof(cx<R>))));
-    APHI_CUDA(cudaFuncSetAttribute(k_update_tile<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    APHI_CUDA(cudaFuncSetAttribute(k_update_panel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    2 * kStep * kTile * static_cast<int>(sizeof(cx<R>))));
+    APHI_CUDA(cudaFuncSetAttribute(k_update_wide<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem<R>()));
+    if constexpr (sizeof(R) == 4)
+        APHI_CUDA(cudaFuncSetAttribute(k_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
     APHI_CUDA(cudaFuncSetAttribute(k_fwd_diag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    kSolveDiagSmem * static_cast<int>(sizeof(cx<R>))));
     APHI_CUDA(cudaFuncSetAttribute(k_bwd_diag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -305,7 +317,8 @@ void factorize_numeric(aphi_factor* f, const double* values, cudaStream_t st) {
     k_scatter_a<R><<<g, 256, 0, st>>>(n, A->d.row_ptr, A->d.col_idx, values, A->S.nnz_a, f->dscale, A->d.a_dest,
                                       reinterpret_cast<cx<R>*>(f->L), A->S.stored);
     APHI_CHECK_LAUNCH();
-    run_plan<R>(f, A->plan_factor, st, nullptr, nullptr, nullptr, nullptr);
+    const bool tc = sizeof(R) == 4 && f->use_tc;
+    run_plan<R>(f, tc ? A->plan_factor_tc : A->plan_factor, st, nullptr, nullptr, nullptr, nullptr);
     k_extract_d<R><<<dim3(A->S.ns, f->batch), 128, 0, st>>>(sched_of(A->d), A->S.ns, A->d.ref_of_post,
                                                           reinterpret_cast<const cx<R>*>(f->L), A->S.stored,
                                                           f->dref, n);
@@ -431,7 +444,16 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
     std::vector<double> dref(2 * static_cast<size_t>(n) * B), dsc(static_cast<size_t>(n) * B);
     APHI_CUDA(cudaMemcpyAsync(dref.data(), f->dref, dref.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     APHI_CUDA(cudaMemcpyAsync(dsc.data(), f->dscale, dsc.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    int err_word = 0;
+    APHI_CUDA(cudaMemcpyAsync(&err_word, f->err, sizeof(int), cudaMemcpyDeviceToHost, st));
     APHI_CUDA(cudaStreamSynchronize(st));
+    if (err_word != 0) {
+        APHI_CUDA(cudaMemsetAsync(f->err, 0, sizeof(int), st));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        f->factored = false;
+        throw Error(APHI_ERR_TIMEOUT, "factorize: a tensor-core tile's bounded wait expired");
+    }
     float ms = 0;
     APHI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     cudaEventDestroy(e0);

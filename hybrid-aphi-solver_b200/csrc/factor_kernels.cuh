@@ -16,6 +16,7 @@
 
 #include "analysis.hpp"
 #include "common.cuh"
+#include "tc_update.cuh"
 
 namespace aphi_b200 {
 
@@ -254,11 +255,13 @@ __global__ void __launch_bounds__(kTrsmRows) k_panel_trsm(Sched S, long long ite
         if (j < kb) P[i + static_cast<long long>(j) * m] = x[j] * Dinv[j];
 }
 
-// Trailing update tile (i0, j0) of step k0: F[i, j] -= sum_t L[i,t] D[t] L[j,t]
-// for i >= j >= k0 + kb. Columns below w are panel columns, the rest CB.
+// In-panel update tile (i0, j0) of step k0: F[i, j] -= sum_t L[i,t] D[t] L[j,t]
+// over the step's kb columns t, for i >= j >= k0 + kb and j inside the
+// current 128-column panel (the columns to its right get the whole panel's
+// update at once when the panel is complete).
 template <class R>
-__global__ void __launch_bounds__(256) k_update_tile(Sched S, long long item0, cx<R>* Lb, cx<R>* CBb,
-                                                     long long lstride, long long cbstride) {
+__global__ void __launch_bounds__(256) k_update_panel(Sched S, long long item0, cx<R>* Lb, cx<R>* CBb,
+                                                      long long lstride, long long cbstride) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<R>* As = reinterpret_cast<cx<R>*>(smem_raw);  // [kStep][kTile], scaled by D
     cx<R>* Bs = As + kStep * kTile;                  // [kStep][kTile]
@@ -305,19 +308,186 @@ __global__ void __launch_bounds__(256) k_update_tile(Sched S, long long item0, c
     }
     cx<R>* Ls = L + S.loff[s];
     cx<R>* CBs = CB + (cs > 0 ? S.cboff[s] : 0);
+    const int jend = min(w, (k0 / kTcPanel) * kTcPanel + kTcPanel);
+    // Read-modify-write: all 16 loads first, so their latencies overlap.
+    cx<R>* dst[4][4];
+    cx<R> old[4][4];
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
         const int j = j0 + ty + 16 * b;
-        if (j >= m) continue;
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
             const int i = i0 + tx + 16 * a;
-            if (i >= m || i < j) continue;
-            cx<R>* dst = (j < w) ? Ls + i + static_cast<long long>(j) * m
-                                 : CBs + (i - w) + static_cast<long long>(j - w) * cs;
-            *dst = *dst - acc[a][b];
+            dst[a][b] = nullptr;
+            if (j < jend && i < m && i >= j)
+                dst[a][b] = (j < w) ? Ls + i + static_cast<long long>(j) * m
+                                    : CBs + (i - w) + static_cast<long long>(j - w) * cs;
+            if (dst[a][b]) old[a][b] = *dst[a][b];
         }
     }
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+            if (dst[a][b]) *dst[a][b] = old[a][b] - acc[a][b];
+}
+
+// SIMT trailing update of a complete panel (either precision). Item
+// (s, p0, i0, j0): F[i, j] -= sum_{t in panel} L[i,t] D[t] L[j,t] over the
+// 128 x 64 tile at rows i0.., columns j0.. (i >= j); K is the panel width
+// (<= 128), consumed 8 columns at a time through double-buffered shared
+// memory, the next chunk's loads in flight while the current one is used.
+// 256 threads, each an 8 x 4 block of complex accumulators (rows tx + 16a,
+// columns ty + 16b): per column t a thread reads 12 shared entries for 32
+// complex multiply-adds.
+constexpr int kWideM = 128, kWideN = 64, kWideKC = 8;
+
+template <class R>
+constexpr int wide_smem() {
+    return 2 * kWideKC * (kWideM + kWideN) * static_cast<int>(sizeof(cx<R>));
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_update_wide(Sched S, long long item0, cx<R>* Lb, cx<R>* CBb,
+                                                     long long lstride, long long cbstride) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<R>* As = reinterpret_cast<cx<R>*>(smem_raw);   // [2][KC][128], scaled by D
+    cx<R>* Bs = As + 2 * kWideKC * kWideM;            // [2][KC][64]
+    const Item it = S.items[item0 + blockIdx.x];
+    const int s = it.s, p0 = it.a, i0 = it.b, j0 = it.c;
+    cx<R>* L = Lb + lstride * blockIdx.y;
+    cx<R>* CB = CBb + cbstride * blockIdx.y;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int cs = m - w;
+    const int K = min(kTcPanel, w - p0);
+    cx<R>* Ls = L + S.loff[s];
+    cx<R>* CBs = CB + (cs > 0 ? S.cboff[s] : 0);
+    const cx<R>* P = Ls + static_cast<long long>(p0) * m;
+    const cx<R>* dg = Ls + p0 + static_cast<long long>(p0) * m;  // pivot t at dg[t * (m + 1)]
+    const int tid = threadIdx.x;
+    // Loader: A chunk entry (k = tid / 128 + 2q, r = tid % 128), q < 4; B chunk
+    // entry (k = tid / 64 + 4q, r = tid % 64), q < 2.
+    cx<R> pa[4], pb[2];
+    auto load = [&](int kbase) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int k = kbase + (tid >> 7) + 2 * q, r = tid & 127;
+            pa[q] = cx<R>{0, 0};
+            if (k < K && i0 + r < m)
+                pa[q] = P[static_cast<long long>(k) * m + i0 + r] * dg[static_cast<long long>(k) * (m + 1)];
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int k = kbase + (tid >> 6) + 4 * q, r = tid & 63;
+            pb[q] = cx<R>{0, 0};
+            if (k < K && j0 + r < m) pb[q] = P[static_cast<long long>(k) * m + j0 + r];
+        }
+    };
+    auto stash = [&](int buf) {
+        cx<R>* A = As + buf * kWideKC * kWideM;
+        cx<R>* B = Bs + buf * kWideKC * kWideN;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) A[((tid >> 7) + 2 * q) * kWideM + (tid & 127)] = pa[q];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) B[((tid >> 6) + 4 * q) * kWideN + (tid & 63)] = pb[q];
+    };
+    const int tx = tid & 15, ty = tid >> 4;
+    cx<R> acc[8][4];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = cx<R>{0, 0};
+    const int nc = (K + kWideKC - 1) / kWideKC;
+    load(0);
+    stash(0);
+    __syncthreads();
+    for (int c = 0; c < nc; ++c) {
+        if (c + 1 < nc) load((c + 1) * kWideKC);
+        const cx<R>* A = As + (c & 1) * kWideKC * kWideM;
+        const cx<R>* B = Bs + (c & 1) * kWideKC * kWideN;
+#pragma unroll
+        for (int k = 0; k < kWideKC; ++k) {
+            cx<R> av[8], bv[4];
+#pragma unroll
+            for (int a = 0; a < 8; ++a) av[a] = A[k * kWideM + tx + 16 * a];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) bv[b] = B[k * kWideN + ty + 16 * b];
+#pragma unroll
+            for (int a = 0; a < 8; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    acc[a][b].re += av[a].re * bv[b].re - av[a].im * bv[b].im;
+                    acc[a][b].im += av[a].re * bv[b].im + av[a].im * bv[b].re;
+                }
+        }
+        if (c + 1 < nc) stash((c + 1) & 1);
+        __syncthreads();
+    }
+    // Read-modify-write, one column block at a time: 8 loads, then 8 stores.
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        const int j = j0 + ty + 16 * b;
+        cx<R>* dst[8];
+        cx<R> old[8];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const int i = i0 + tx + 16 * a;
+            dst[a] = nullptr;
+            if (j < m && i < m && i >= j)
+                dst[a] = (j < w) ? Ls + i + static_cast<long long>(j) * m
+                                 : CBs + (i - w) + static_cast<long long>(j - w) * cs;
+            if (dst[a]) old[a] = *dst[a];
+        }
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+            if (dst[a]) *dst[a] = old[a] - acc[a][b];
+    }
+}
+
+// Tensor-core trailing update of a complete panel (FP32 factors). Item
+// (s, p0, i0, j0): F[i, j] -= sum_{t in panel} L[i,t] D[t] L[j,t] over the
+// 128 x 64 tile at rows i0.., columns j0.. (i >= j). K is the panel width
+// (<= 128). A bounded wait that expires sets err[0] and leaves the tile
+// unchanged; the host reports it.
+__global__ void __launch_bounds__(kTcThreads) k_update_tc(Sched S, long long item0, cx<float>* Lb, cx<float>* CBb,
+                                                          long long lstride, long long cbstride, int* err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Item it = S.items[item0 + blockIdx.x];
+    const int s = it.s, p0 = it.a, i0 = it.b, j0 = it.c;
+    cx<float>* L = Lb + lstride * blockIdx.y;
+    cx<float>* CB = CBb + cbstride * blockIdx.y;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int cs = m - w;
+    const int K = min(kTcPanel, w - p0);
+    cx<float>* Ls = L + S.loff[s];
+    cx<float>* CBs = CB + (cs > 0 ? S.cboff[s] : 0);
+    const float2* P = reinterpret_cast<const float2*>(Ls + static_cast<long long>(p0) * m);
+    const float2* dk = reinterpret_cast<const float2*>(Ls + p0 + static_cast<long long>(p0) * m);
+    // Read-modify-write of 16 entries of row i: all loads first, so their
+    // latencies overlap, then the stores.
+    const bool ok = tc_tile(smem_raw, P, m, m, K, i0, j0, dk, static_cast<long long>(m) + 1,
+                            [&](int r, int c0, const float(&re)[16], const float(&im)[16]) {
+                                const int i = i0 + r;
+                                if (i >= m) return;
+                                float2* dst[16];
+                                float2 old[16];
+#pragma unroll
+                                for (int c = 0; c < 16; ++c) {
+                                    const int j = j0 + c0 + c;
+                                    dst[c] = nullptr;
+                                    if (j < m && i >= j)
+                                        dst[c] = reinterpret_cast<float2*>(
+                                            (j < w) ? Ls + i + static_cast<long long>(j) * m
+                                                    : CBs + (i - w) + static_cast<long long>(j - w) * cs);
+                                    if (dst[c]) old[c] = *dst[c];
+                                }
+#pragma unroll
+                                for (int c = 0; c < 16; ++c)
+                                    if (dst[c]) *dst[c] = make_float2(old[c].x - re[c], old[c].y - im[c]);
+                            });
+    if (!ok && threadIdx.x == 0) atomicExch(err, 1);
 }
 
 // ---------------------------------------------------------------- solves

@@ -281,6 +281,25 @@ int aphi_solve_refined(aphi_factor* f, int nrhs, const double* values_dev, const
 int aphi_solve_symmetric_host(const aphi_analysis* an, const double* values, const double* b,
                               int equil_iters, double pivot_floor, double* x, double* report);
 
+/* ---- Diagnostics ---------------------------------------------------------
+ * Launch plans of an analysis: plan 0 the FP64 / SIMT factorization, 1 the
+ * FP32 tensor-core factorization, 2 the forward solve, 3 the backward solve.
+ * launches[k], items[k] for each of the APHI_PLAN_KINDS kernel kinds: 0
+ * extend-add, 1 one-CTA front, 2 diagonal block, 3 panel rows, 4 SIMT trailing
+ * update tile,
+ * 5-9 solve kernels (gather, forward diagonal, forward update, backward
+ * update, backward diagonal), 10 panel-restricted update tile, 11
+ * tensor-core update tile. */
+#define APHI_PLAN_KINDS 12
+int aphi_analysis_plan_stats(const aphi_analysis* a, int plan, int64_t* launches, int64_t* items);
+
+/* One tensor-core update tile on host data: out (128 x 64 complex64,
+ * column-major, leading dimension 128) = sum_{k<K} (P[i0+r, k] d[k])
+ * P[j0+c, k], where P is rows x K complex64 column-major and d (K entries,
+ * NULL for ones). Rows of P at or beyond `rows` read as zero. K <= 128. The
+ * kernel the FP32 factorization uses for its trailing updates. */
+int aphi_selftest_tc_tile(int rows, int K, int i0, int j0, const float* P, const float* d, float* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,99 @@
+"""The tensor-core (tcgen05) update tile and the FP32 factorization built on it.
+
+The tile computes sum_k (P[i0+r, k] d_k) P[j0+c, k] with complex64 operands
+from a three-way TF32 split of each real operand (six cross products kept);
+each entry must be within 1e-5 of the sum of magnitudes |P d||P| -- the
+accuracy of an FP32 dot product of that length -- against the same product
+in FP64 on the host.
+
+The tensor core's FP32 accumulation truncates instead of rounding to nearest,
+so a tile's error has a bias (measured: -6e-7 relative at K = 128 for
+all-positive products, none for a rounded FP32 sum) that accumulates over the
+panels of a large front. The factorization built on it is therefore up to
+~8x less accurate than the SIMT FP32 factorization (measured 4.9x on 10^3 and
+14^3 cylinders after the main products were given their own accumulator);
+the test bounds the ratio at 10 and requires the refined solve to reach
+relative residual 1e-13 with it as the preconditioner."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import aphi_b200 as ab
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(256, 128, 0, 0), (300, 96, 64, 32), (200, 17, 100, 180), (128, 32, 0, 64), (517, 128, 389, 200),
+          (90, 5, 0, 0)]
+
+
+def host_tile(P, i0, j0, d):
+    rows, K = P.shape
+    Pd = P.astype(np.complex128)
+    dd = np.ones(K) if d is None else d.astype(np.complex128)
+    A = np.zeros((128, K), np.complex128)
+    B = np.zeros((64, K), np.complex128)
+    ra = np.arange(i0, min(i0 + 128, rows))
+    rb = np.arange(j0, min(j0 + 64, rows))
+    A[:ra.size] = Pd[ra] * dd
+    B[:rb.size] = Pd[rb]
+    mag = np.abs(A) @ np.abs(B).T
+    return A @ B.T, mag
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("with_d", [False, True])
+def test_tile_against_host_product(shape, with_d, cuda):
+    rows, K, i0, j0 = shape
+    rng = np.random.default_rng(rows * 1000 + K)
+    P = (rng.normal(size=(rows, K)) + 1j * rng.normal(size=(rows, K))).astype(np.complex64)
+    d = (rng.normal(size=K) + 1j * rng.normal(size=K)).astype(np.complex64) if with_d else None
+    out = ab.tc_tile_selftest(P, i0, j0, d)
+    ref, mag = host_tile(P, i0, j0, d)
+    err = np.abs(out.astype(np.complex128) - ref)
+    assert (err <= 1e-5 * mag + 1e-30).all(), (err / np.maximum(mag, 1e-30)).max()
+
+
+def test_split_keeps_more_than_tf32(cuda):
+    """Values that TF32 alone would round (10-bit mantissas) come out to FP32
+    accuracy: the split carries the low bits through the tensor cores."""
+    rng = np.random.default_rng(5)
+    P = (1.0 + rng.uniform(0, 1e-3, size=(128, 64)) + 1j * rng.uniform(0, 1e-3, size=(128, 64))).astype(np.complex64)
+    out = ab.tc_tile_selftest(P, 0, 0)
+    ref, mag = host_tile(P, 0, 0, None)
+    worst = (np.abs(out - ref) / mag).max()
+    assert worst < 2e-6, worst
+
+
+def _factor_solution(an, vals, rhs, precision, tc):
+    old = os.environ.get("APHI_NO_TC")
+    os.environ["APHI_NO_TC"] = "0" if tc else "1"
+    try:
+        f = ab.Factor(an, precision=precision, batch=vals.shape[0])
+    finally:
+        if old is None:
+            del os.environ["APHI_NO_TC"]
+        else:
+            os.environ["APHI_NO_TC"] = old
+    assert f.factorize(vals)
+    return f, f.solve(rhs)
+
+
+@pytest.mark.parametrize("cells", [10, 14])
+def test_tc_factor_as_accurate_as_simt(cells, cuda):
+    w = ab.Workload.cylinder(cells)
+    an = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx))
+    assert an.info["max_rows"] > 200        # large fronts reach the tensor-core tiles
+    asm = ab.Assembly(ab.workload_arrays(w))
+    vals, rhs = asm.refill(2 * np.pi * np.array([50.0, 1.0e3]))
+    _, x64 = _factor_solution(an, vals, rhs, ab.PREC_FP64, False)
+    _, xs = _factor_solution(an, vals, rhs, ab.PREC_FP32, False)
+    ftc, xt = _factor_solution(an, vals, rhs, ab.PREC_FP32, True)
+    for k in range(2):
+        e_simt = (torch.linalg.norm(xs[k] - x64[k]) / torch.linalg.norm(x64[k])).item()
+        e_tc = (torch.linalg.norm(xt[k] - x64[k]) / torch.linalg.norm(x64[k])).item()
+        assert e_tc <= 10.0 * e_simt + 1e-6, (k, e_tc, e_simt)
+    x, iters, berr, ok = ftc.solve_refined(vals, rhs, tol=1e-16, rtol=1e-13, max_iters=40, krylov=True)
+    res = ab.residuals(an, vals, x, rhs)
+    assert ok and (res[:, 0, 0] <= 1e-13).all(), (iters, res)
