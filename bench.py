@@ -223,9 +223,13 @@ def run_ours(args):
     for _ in range(args.warmup):
         sweep()
     torch.cuda.synchronize()
+    live_peaks = ab.measure_peaks()
     barrier()
     torch.cuda.synchronize()
     launches0 = ab.launch_count()
+    # Per-kind device time of the factorizations inside the timed steps: CUDA
+    # events around each launch, on the stream the kernels run on.
+    solver.profile(True)
     step_ms = []
     with Clocks(local) as clk:
         t0, t1 = ev(), ev()
@@ -240,6 +244,9 @@ def run_ours(args):
         t1.record(stream)
         torch.cuda.synchronize()
     launches = (ab.launch_count() - launches0) // max(args.steps, 1)
+    kind_ms = solver.profile_read()
+    entries = {"fp32": solver.factorized[ab.PREC_FP32], "fp64": solver.factorized[ab.PREC_FP64]}
+    solver.profile(False)
     elapsed = t0.elapsed_time(t1)
     if world > 1:
         import torch.distributed as dist
@@ -248,16 +255,27 @@ def run_ours(args):
         elapsed = float(t.item())
     res = ab.residuals(an, vals, x, rhs)
     value = world * args.nfreq * args.steps / (elapsed / 1000.0)
-    # The dominant kernels alone: the batched FP32 factorization, timed with
-    # events on the stream it runs on.
-    fact_ms = []
-    for _ in range(2):
-        a, b = ev(), ev()
-        a.record(stream)
-        solver.f32.factorize(vals, 10, 0.0, stream=stream)
-        b.record(stream)
-        torch.cuda.synchronize()
-        fact_ms.append(a.elapsed_time(b))
+
+    # The dominant kernel of the timed steps and its roofline: useful
+    # Schur-update flops (lower-triangle entries of the fronts, 8 real flops
+    # per complex multiply-add) of every factorization it served, over its
+    # summed launch durations.
+    plan_flops = {"fp32": an.plan_stats(1, flops=True), "fp64": an.plan_stats(0, flops=True)}
+    kernels = []
+    for prec, kinds in kind_ms.items():
+        for kind, (n_launch, ms) in kinds.items():
+            st = plan_flops[prec].get(kind)
+            useful = st[2] * entries[prec] if st else 0.0
+            kernels.append({"precision": prec, "kind": kind, "launches": n_launch, "ms": ms,
+                            "share_of_step": ms / elapsed, "useful_tflop": useful / 1e12,
+                            "tflops": useful / (ms / 1000.0) / 1e12 if useful else None})
+    kernels.sort(key=lambda k: -k["ms"])
+    top = kernels[0]
+    name = {"update_wide": "k_update_wide_dmma (FP64 DMMA trailing update)" if top["precision"] == "fp64"
+            else "k_update_wide<float> (SIMT trailing update)",
+            "update_tc": "k_update_tc (tcgen05 split-TF32 trailing update)"}.get(top["kind"], top["kind"])
+    peak_key = {"fp64": "fp64_dmma", "fp32": "tf32_tc_n256" if top["kind"] == "update_tc" else "fp32_ffma"}[
+        top["precision"]]
 
     # End to end through the reference-facing calls with host buffers: refill
     # hands the assembled systems to the host (as refill(SymmetricSystem&)
@@ -291,11 +309,11 @@ def run_ours(args):
     h2d = 2 * (host_vals.numel() + host_rhs.numel()) * 8
     d2h = 2 * (host_vals.numel() + host_rhs.numel() + host_x.numel()) * 8
 
+    solver.close()
     del solver
     torch.cuda.empty_cache()
 
-    # Plain FP64 factorization of the same sweep (the drop-in path), in
-    # batches that fit beside the workspace.
+    # Plain FP64 factorization of the same sweep (the drop-in path).
     fp64 = ab.SweepSolver(an, asm, args.nfreq, "fp64", fp64_batch=args.fp64_batch)
     fp64.solve(omegas, stream=stream)
     torch.cuda.synchronize()
@@ -308,15 +326,14 @@ def run_ours(args):
     fp64_ms = a.elapsed_time(b) / args.fp64_steps
     res64 = ab.residuals(an, vals64, x64, rhs64)
     fp64_value = world * args.nfreq / (fp64_ms / 1000.0)
+    fp64.close()
     del fp64
 
     hbm, bf16, bf16s, src = peaks()
-    fact_avg = float(np.mean(fact_ms))
-    achieved = info["flops"] * args.nfreq / (fact_avg / 1000.0) / 1e12
     traffic_path = ROOT / "profiles" / "traffic.json"
     traffic = None
     if traffic_path.exists():
-        traffic = json.loads(traffic_path.read_text()).get(f"factorize_fp32_{args.cells}")
+        traffic = json.loads(traffic_path.read_text()).get(f"{top['precision']}_{top['kind']}_{args.cells}")
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -331,25 +348,32 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "c64 factor + c128 refinement", "data": "synthetic",
+            "dtype": "c64 or c128 factor, c128 refinement", "data": "synthetic",
             "config": workload_config(args, info) | {"batch": args.nfreq, "parallelism": f"freq-replicas x{world}"},
             "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                            "what": "one sweep of all frequencies (every solve of the batch completes together)"},
             "accuracy": {"max_backward_error": float(res[..., 1].max()), "max_rel_residual": float(res[..., 0].max()),
                          "fp32_entries": sum(r["precision"] == "fp32" for r in reps),
-                         "fp64_fallback_entries": sum(r["precision"] == "fp64" for r in reps),
+                         "fp64_entries": sum(r["precision"] == "fp64" for r in reps),
+                         "fp64_predicted_entries": sum(r["predicted_fp64"] for r in reps),
                          "cocg_iterations": [r["iterations"] for r in reps]},
             "fp64": {"value": fp64_value, "unit": UNIT, "ms_per_sweep": fp64_ms, "batch": args.fp64_batch,
                      "max_rel_residual": float(res64[..., 0].max()),
                      "max_backward_error": float(res64[..., 1].max())},
             "speedup_vs_fp64": value / fp64_value,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"bound": "tensor", "kernel": "batched FP32 supernodal factorization (equilibration, extend-add, panel and update kernels)",
-                         "achieved": achieved, "peak": bf16s, "unit": "TFLOP/s", "frac": achieved / bf16s,
-                         "peak_source": f"bf16_tflops_sustained, {src}",
+            "roofline": {"bound": "tensor", "kernel": name, "achieved": top["tflops"],
+                         "peak": live_peaks[peak_key], "unit": "TFLOP/s",
+                         "frac": top["tflops"] / live_peaks[peak_key],
+                         "peak_source": (f"{peak_key}: measured live on this device by aphi_measure_peaks "
+                                         f"(MEASURED_PEAKS.json has only HBM and bf16: bf16 {bf16:.0f} TF/s, {src})"),
                          "traffic": traffic,
-                         "algorithmic": f"{info['flops']:.4e} real flop per factorization x {args.nfreq}",
-                         "factorize_ms": fact_avg},
+                         "algorithmic": (f"useful Schur-update flops: {plan_flops[top['precision']][top['kind']][2]:.4e} "
+                                         f"per factorization x {entries[top['precision']]} factorizations in the "
+                                         f"timed steps"),
+                         "launches": top["launches"], "kernel_ms": top["ms"]},
+            "kernels": kernels[:8],
+            "live_peaks_tflops": live_peaks,
             "cpu_baseline": cpu,
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
@@ -372,7 +396,7 @@ def main():
     ap.add_argument("--tol", type=float, default=1e-16, help="backward-error target of the refinement")
     ap.add_argument("--rtol", type=float, default=1e-14,
                     help="relative-residual target of the refinement (the FP64 direct solve's own level)")
-    ap.add_argument("--fp64-batch", type=int, default=4)
+    ap.add_argument("--fp64-batch", type=int, default=8)
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--sample-cells", type=int, default=16)
     ap.add_argument("--no-cpu", action="store_true")

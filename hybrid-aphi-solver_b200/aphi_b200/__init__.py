@@ -138,7 +138,10 @@ _SIGS = {
     "aphi_residuals_noalloc": (I, [P, I, I, P, P, P, PD, P]),
     "aphi_solve_symmetric_host": (I, [P, PD, PD, I, D, PD, PD]),
     "aphi_selftest_tc_tile": (I, [I, I, I, I, P, P, P]),
-    "aphi_analysis_plan_stats": (I, [P, I, PI64, PI64]),
+    "aphi_analysis_plan_stats": (I, [P, I, PI64, PI64, PD, PD]),
+    "aphi_factor_profile": (I, [P, I]),
+    "aphi_measure_peaks": (I, [PD]),
+    "aphi_factor_profile_read": (I, [P, PD, PI64]),
 }
 
 
@@ -426,12 +429,21 @@ class Analysis:
     PLAN_KINDS = ["extend_add", "small_front", "diag_block", "panel_rows", "update_wide", "fwd_gather", "fwd_diag",
                   "fwd_update", "bwd_update", "bwd_diag", "update_panel", "update_tc"]
 
-    def plan_stats(self, plan: int) -> dict:
+    def plan_stats(self, plan: int, flops: bool = False) -> dict:
         """{kind: (launches, items)} of launch plan `plan` (0 factorization,
-        1 tensor-core factorization, 2 forward solve, 3 backward solve)."""
+        1 tensor-core factorization, 2 forward solve, 3 backward solve); with
+        flops=True, {kind: (launches, items, useful_flops, executed_flops)}
+        (flops counted for the update kinds only)."""
         la = np.zeros(12, np.int64)
         it = np.zeros(12, np.int64)
-        check(lib().aphi_analysis_plan_stats(self._h, plan, la.ctypes.data_as(PI64), it.ctypes.data_as(PI64)))
+        us = np.zeros(12)
+        ex = np.zeros(12)
+        check(lib().aphi_analysis_plan_stats(self._h, plan, la.ctypes.data_as(PI64), it.ctypes.data_as(PI64),
+                                             us.ctypes.data_as(PD) if flops else None,
+                                             ex.ctypes.data_as(PD) if flops else None))
+        if flops:
+            return {k: (int(a), int(b), float(u), float(e)) for k, a, b, u, e in zip(self.PLAN_KINDS, la, it, us, ex)
+                    if a}
         return {k: (int(a), int(b)) for k, a, b in zip(self.PLAN_KINDS, la, it) if a}
 
     def etree(self):
@@ -522,6 +534,17 @@ class Factor:
         x = x.squeeze(1) if squeeze else x
         return x, np.array(list(it)).reshape(self.batch, nrhs), np.array(list(be)).reshape(self.batch, nrhs), rc == OK
 
+    def profile(self, enable: bool = True) -> None:
+        """Per-kind device timing of later factorizations (clears the totals)."""
+        check(lib().aphi_factor_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self) -> dict:
+        """{kind: (launches, ms)} accumulated since profile(True)."""
+        ms = np.zeros(12)
+        la = np.zeros(12, np.int64)
+        check(lib().aphi_factor_profile_read(self._h, ms.ctypes.data_as(PD), la.ctypes.data_as(PI64)))
+        return {k: (int(a), float(t)) for k, a, t in zip(Analysis.PLAN_KINDS, la, ms) if a}
+
     def export(self, k: int = 0) -> dict:
         """Entry k in the reference's SymmetricFactor layout (strictly lower
         CSC, rows ascending, caller's permuted numbering) plus D and the
@@ -560,6 +583,13 @@ def residuals(analysis: Analysis, values, x, b, stream=None) -> np.ndarray:
     check(lib().aphi_residuals(analysis._h, batch, nrhs, dptr(values), dptr(xx.contiguous()),
                                dptr(bb.contiguous()), out.ctypes.data_as(PD), None))
     return out
+
+
+def measure_peaks() -> dict:
+    """Arithmetic peaks of the current device in TFLOP/s (aphi_measure_peaks)."""
+    out = np.zeros(5)
+    check(lib().aphi_measure_peaks(out.ctypes.data_as(PD)))
+    return dict(zip(["fp64_dmma", "fp64_dfma", "fp32_ffma", "tf32_tc_n64", "tf32_tc_n256"], out.tolist()))
 
 
 def tc_tile_selftest(P: np.ndarray, i0: int, j0: int, d: np.ndarray | None = None) -> np.ndarray:
@@ -610,22 +640,100 @@ class SweepSolver:
     pattern and the supernodal schedule, so fills, factorizations and refined
     solves run as batched launches over all of them.
 
-    precision="mixed": the batch is factorized in FP32 and refined by FP64
-    preconditioned COCG on the original systems to the FP64 direct solve's
-    own residual level (rtol); an entry whose refinement stalls (cond(A) *
-    eps(FP32) too large -- the high-frequency end of the cylinder sweep) is
-    refactorized in FP64 automatically. precision="fp64": the plain FP64
-    factorization for every entry (the drop-in path).
+    precision="mixed": the frequencies are factorized together in FP32 and
+    refined by FP64 preconditioned COCG on the original systems to the FP64
+    direct solve's own residual level (rtol); an entry whose refinement
+    stalls (cond(A) * eps(FP32) too large -- the high-frequency end of the
+    cylinder sweep) is refactorized in FP64 automatically. The solver
+    remembers the lowest frequency at which that happened: later sweeps send
+    that frequency and every higher one straight to FP64 instead of spending
+    an FP32 factorization on them (predict=False disables this).
+    precision="fp64": the plain FP64 factorization for every entry (the
+    drop-in path).
+
+    Factor batches are sized to the entries they hold, split evenly into at
+    most fp64_batch (FP64) or fp32_batch (FP32) entries per factorization, so
+    no factorization is spent on padding.
     """
 
     def __init__(self, analysis: Analysis, assembly: Assembly, batch: int, precision: str = "mixed",
-                 fp64_batch: int = 4, rtol: float = 1e-14, tol: float = 1e-16, max_iters: int = 40):
+                 fp64_batch: int = 8, rtol: float = 1e-14, tol: float = 1e-16, max_iters: int = 40,
+                 fp32_batch: int | None = None, predict: bool = True):
+        if precision not in ("mixed", "fp64"):
+            raise InvalidArgument(ERR_BAD_SHAPE, f"SweepSolver: precision {precision!r} is not 'mixed' or 'fp64'")
         self.analysis, self.assembly = analysis, assembly
         self.batch, self.precision = batch, precision
         self.rtol, self.tol, self.max_iters = rtol, tol, max_iters
         self.fp64_batch = max(1, min(fp64_batch, batch))
-        self.f32 = Factor(analysis, PREC_FP32, batch) if precision == "mixed" else None
-        self.f64 = Factor(analysis, PREC_FP64, self.fp64_batch)
+        self.fp32_batch = max(1, min(fp32_batch or batch, batch))
+        self.predict = predict
+        self.stall_omega = None      # lowest frequency whose FP32 refinement stalled
+        self._factors = {}
+        self._profile = False
+        self._prof_done = {}         # precision -> {kind: (launches, ms)} of factors since replaced
+        self.factorized = {PREC_FP32: 0, PREC_FP64: 0}   # entries factorized since profile(True)
+
+    def _factor(self, precision: int, size: int) -> Factor:
+        f = self._factors.get(precision)
+        if f is None or f.batch != size:
+            if f is not None:
+                self._fold_profile(precision, f)
+                f.close()
+                self._factors.pop(precision)
+            f = Factor(self.analysis, precision, size)
+            if self._profile:
+                f.profile(True)
+            self._factors[precision] = f
+        return f
+
+    def _fold_profile(self, precision, f):
+        if not self._profile:
+            return
+        acc = self._prof_done.setdefault(precision, {})
+        for k, (n, ms) in f.profile_read().items():
+            a = acc.get(k, (0, 0.0))
+            acc[k] = (a[0] + n, a[1] + ms)
+
+    def profile(self, enable: bool = True) -> None:
+        """Per-kind device timing of every factorization from now on."""
+        self._profile = enable
+        self._prof_done = {}
+        self.factorized = {PREC_FP32: 0, PREC_FP64: 0}
+        for f in self._factors.values():
+            f.profile(enable)
+
+    def profile_read(self) -> dict:
+        """{"fp32" | "fp64": {kind: (launches, ms)}} since profile(True)."""
+        out = {}
+        for prec, name in ((PREC_FP32, "fp32"), (PREC_FP64, "fp64")):
+            acc = dict(self._prof_done.get(prec, {}))
+            f = self._factors.get(prec)
+            if f is not None:
+                for k, (n, ms) in f.profile_read().items():
+                    a = acc.get(k, (0, 0.0))
+                    acc[k] = (a[0] + n, a[1] + ms)
+            if acc:
+                out[name] = acc
+        return out
+
+    @property
+    def f32(self):
+        return self._factors.get(PREC_FP32)
+
+    @property
+    def f64(self):
+        return self._factors.get(PREC_FP64)
+
+    @staticmethod
+    def _chunks(idx, cap):
+        nb = -(-len(idx) // cap) if idx else 0
+        size = -(-len(idx) // nb) if nb else 0
+        return [idx[c:c + size] for c in range(0, len(idx), size)] if size else []
+
+    def close(self):
+        for f in self._factors.values():
+            f.close()
+        self._factors = {}
 
     def solve(self, omegas, conditioning=COND_ROW_SCALED, stream=None, values=None, rhs=None):
         """Returns (x [batch, n], values, rhs, per-entry reports), all device
@@ -640,33 +748,45 @@ class SweepSolver:
             vals, rhs = self.assembly.refill(om, conditioning, stream=stream)
         else:
             vals = values
-        reports = [dict(omega=float(w), precision="fp32", iterations=0) for w in om]
-        todo = list(range(self.batch))
-        if self.f32 is not None:
-            self.f32.factorize(vals, 10, 0.0, stream=stream)
-            x, iters, berr, _ = self.f32.solve_refined(vals, rhs, tol=self.tol, rtol=self.rtol,
-                                                       max_iters=self.max_iters, stream=stream)
-            res = residuals(self.analysis, vals, x, rhs, stream=stream)
-            todo = []
-            for k in range(self.batch):
-                reports[k]["iterations"] = int(iters[k, 0])
-                if not (res[k, 0, 0] <= self.rtol and res[k, 0, 1] <= self.tol):
+        reports = [dict(omega=float(w), precision="fp64", iterations=0, predicted_fp64=False) for w in om]
+        x = torch.empty_like(rhs)
+        fp32_idx, todo = [], []
+        for k in range(self.batch):
+            if self.precision == "mixed" and not (self.predict and self.stall_omega is not None
+                                                  and om[k] >= self.stall_omega):
+                fp32_idx.append(k)
+            else:
+                todo.append(k)
+                reports[k]["predicted_fp64"] = self.precision == "mixed"
+        for idx in self._chunks(fp32_idx, self.fp32_batch):
+            f = self._factor(PREC_FP32, len(idx))
+            whole = len(idx) == self.batch
+            sel = None if whole else torch.tensor(idx, device=vals.device)
+            v = vals if whole else vals.index_select(0, sel)
+            b = rhs if whole else rhs.index_select(0, sel)
+            f.factorize(v, 10, 0.0, stream=stream)
+            self.factorized[PREC_FP32] += len(idx)
+            xs, iters, berr, _ = f.solve_refined(v, b, tol=self.tol, rtol=self.rtol, max_iters=self.max_iters,
+                                                 stream=stream)
+            res = residuals(self.analysis, v, xs, b, stream=stream)
+            if whole:
+                x.copy_(xs)
+            else:
+                x.index_copy_(0, sel, xs)
+            for q, k in enumerate(idx):
+                reports[k]["iterations"] = int(iters[q, 0])
+                if res[q, 0, 0] <= self.rtol and res[q, 0, 1] <= self.tol:
+                    reports[k]["precision"] = "fp32"
+                else:
                     todo.append(k)
-        else:
-            x = torch.empty_like(rhs)
-        for c in range(0, len(todo), self.fp64_batch):
-            idx = todo[c:c + self.fp64_batch]
+                    if self.stall_omega is None or om[k] < self.stall_omega:
+                        self.stall_omega = float(om[k])
+        todo.sort()
+        for idx in self._chunks(todo, self.fp64_batch):
+            f = self._factor(PREC_FP64, len(idx))
             sel = torch.tensor(idx, device=vals.device)
-            v = torch.zeros((self.fp64_batch, vals.shape[1]), dtype=vals.dtype, device=vals.device)
-            b = torch.zeros((self.fp64_batch, rhs.shape[1]), dtype=rhs.dtype, device=rhs.device)
-            v[:len(idx)] = vals.index_select(0, sel)
-            b[:len(idx)] = rhs.index_select(0, sel)
-            if len(idx) < self.fp64_batch:      # pad with a copy of the first entry
-                v[len(idx):] = v[0]
-                b[len(idx):] = b[0]
-            self.f64.factorize(v, 10, 0.0, stream=stream)
-            xs = self.f64.solve(b, stream=stream)
-            x.index_copy_(0, sel, xs[:len(idx)])
-            for k in idx:
-                reports[k]["precision"] = "fp64"
+            f.factorize(vals.index_select(0, sel), 10, 0.0, stream=stream)
+            self.factorized[PREC_FP64] += len(idx)
+            xs = f.solve(rhs.index_select(0, sel), stream=stream)
+            x.index_copy_(0, sel, xs)
         return x, vals, rhs, reports

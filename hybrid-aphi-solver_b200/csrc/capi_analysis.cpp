@@ -1,6 +1,9 @@
 // C ABI: analysis (supernodal schedule) creation and queries.
 #include "analysis.hpp"
 #include "capi_util.hpp"
+#include "tc_config.hpp"
+
+#include <algorithm>
 
 using namespace aphi_b200;
 
@@ -47,16 +50,47 @@ int aphi_analysis_etree(const aphi_analysis* a, int* parent, int* col_count) {
     });
 }
 
-int aphi_analysis_plan_stats(const aphi_analysis* a, int plan, int64_t* launches, int64_t* items) {
+int aphi_analysis_plan_stats(const aphi_analysis* a, int plan, int64_t* launches, int64_t* items, double* useful,
+                             double* executed) {
     return guard([&] {
         if (!a || !launches || !items) throw Error(APHI_ERR_INVALID, "aphi_analysis_plan_stats: null argument");
         const std::vector<Launch>* plans[] = {&a->plan_factor, &a->plan_factor_tc, &a->plan_fwd, &a->plan_bwd};
         if (plan < 0 || plan > 3) throw Error(APHI_ERR_BAD_SHAPE, "aphi_analysis_plan_stats: plan is 0..3");
-        for (int k = 0; k < APHI_PLAN_KINDS; ++k) launches[k] = items[k] = 0;
+        const Symbolic& S = a->S;
+        for (int k = 0; k < APHI_PLAN_KINDS; ++k) {
+            launches[k] = items[k] = 0;
+            if (useful) useful[k] = 0;
+            if (executed) executed[k] = 0;
+        }
+        // Lower-triangle entries (i >= j) of rows [r0, r1) x columns [c0, c1).
+        auto lower = [](long long r0, long long r1, long long c0, long long c1) {
+            double n = 0;
+            for (long long j = c0; j < c1; ++j) n += static_cast<double>(std::max(0LL, r1 - std::max(r0, j)));
+            return n;
+        };
         for (const Launch& l : *plans[plan]) {
             if (l.kind < 0 || l.kind >= APHI_PLAN_KINDS) continue;
             ++launches[l.kind];
             items[l.kind] += l.count;
+            if (!useful && !executed) continue;
+            for (long long t = l.first; t < l.first + l.count; ++t) {
+                const Item& it = a->h_items[t];
+                const int w = S.sn_first[it.s + 1] - S.sn_first[it.s];
+                const int m = S.sn_rows[it.s];
+                double u = 0, e = 0;
+                if (l.kind == K_UPDATE_WIDE || l.kind == K_UPDATE_TC) {
+                    const int K = std::min(kTcPanel, w - it.a);
+                    u = 8.0 * K * lower(it.b, std::min(m, it.b + kTcM), it.c, std::min(m, it.c + kTcN));
+                    e = 8.0 * K * kTcM * kTcN;
+                } else if (l.kind == K_UPDATE_PANEL) {
+                    const int kb = std::min(kStep, w - it.a);
+                    const int jend = std::min(w, (it.a / kTcPanel) * kTcPanel + kTcPanel);
+                    u = 8.0 * kb * lower(it.b, std::min(m, it.b + kTile), it.c, std::min(jend, it.c + kTile));
+                    e = 8.0 * kb * kTile * kTile;
+                }
+                if (useful) useful[l.kind] += u;
+                if (executed) executed[l.kind] += e;
+            }
         }
     });
 }

@@ -46,6 +46,23 @@ int aphi_solve(aphi_factor* f, int nrhs, const double* b_dev, double* x_dev, voi
     });
 }
 
+int aphi_factor_profile(aphi_factor* f, int enable) {
+    return guard([&] {
+        if (!f) throw Error(APHI_ERR_INVALID, "aphi_factor_profile: null factor");
+        factor_profile(f, enable != 0);
+    });
+}
+
+int aphi_factor_profile_read(const aphi_factor* f, double* ms, int64_t* launches) {
+    return guard([&] {
+        if (!f || !ms || !launches) throw Error(APHI_ERR_INVALID, "aphi_factor_profile_read: null argument");
+        for (int k = 0; k < APHI_PLAN_KINDS; ++k) {
+            ms[k] = f->prof_ms[k];
+            launches[k] = f->prof_launches[k];
+        }
+    });
+}
+
 int aphi_factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, double* value,
                        double* diagonal, double* d_scale) {
     return guard([&] {

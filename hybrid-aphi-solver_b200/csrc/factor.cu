@@ -255,15 +255,29 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
     cx<R>* CB = reinterpret_cast<cx<R>*>(f->CB);
     const long long ls = A->S.stored, cs = A->S.cb_pool;
     const int smallsm = A->opt.small_front * A->opt.small_front * static_cast<int>(sizeof(cx<R>));
+    aphi_factor* fm = const_cast<aphi_factor*>(f);
+    const bool prof = f->profile && !sa;
     for (const Launch& l : plan) {
         dim3 grid(l.count, f->batch);
+        if (prof) {
+            cudaEvent_t e[2];
+            APHI_CUDA(cudaEventCreate(&e[0]));
+            APHI_CUDA(cudaEventCreate(&e[1]));
+            fm->prof_events.push_back(e[0]);
+            fm->prof_events.push_back(e[1]);
+            fm->prof_kinds.push_back(l.kind);
+            APHI_CUDA(cudaEventRecord(e[0], st));
+        }
         switch (l.kind) {
             case K_EXTEND_ADD: k_extend_add<R><<<grid, 256, 0, st>>>(S, l.first, L, CB, ls, cs); break;
             case K_SMALL: k_small_front<R><<<grid, 256, smallsm, st>>>(S, l.first, L, CB, ls, cs); break;
             case K_DIAG: k_diag_block<R><<<grid, 128, 0, st>>>(S, l.first, L, ls); break;
             case K_TRSM: k_panel_trsm<R><<<grid, kTrsmRows, 0, st>>>(S, l.first, L, ls); break;
             case K_UPDATE_WIDE:
-                k_update_wide<R><<<grid, 256, wide_smem<R>(), st>>>(S, l.first, L, CB, ls, cs);
+                if constexpr (sizeof(R) == 8)
+                    k_update_wide_dmma<<<grid, 256, kDmmaSmem, st>>>(S, l.first, L, CB, ls, cs);
+                else
+                    k_update_wide<R><<<grid, 256, wide_smem<R>(), st>>>(S, l.first, L, CB, ls, cs);
                 break;
             case K_UPDATE_PANEL:
                 k_update_panel<R><<<grid, 256, 2 * kStep * kTile * sizeof(cx<R>), st>>>(S, l.first, L, CB, ls, cs);
@@ -285,7 +299,22 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
                 break;
         }
         APHI_CHECK_LAUNCH();
+        if (prof) APHI_CUDA(cudaEventRecord(fm->prof_events.back(), st));
     }
+}
+
+// Adds the per-launch durations of the last factorization to the totals
+// (after the stream has been synchronized).
+void collect_profile(aphi_factor* f) {
+    for (size_t q = 0; q < f->prof_kinds.size(); ++q) {
+        float ms = 0;
+        APHI_CUDA(cudaEventElapsedTime(&ms, f->prof_events[2 * q], f->prof_events[2 * q + 1]));
+        f->prof_ms[f->prof_kinds[q]] += ms;
+        ++f->prof_launches[f->prof_kinds[q]];
+    }
+    for (cudaEvent_t e : f->prof_events) cudaEventDestroy(e);
+    f->prof_events.clear();
+    f->prof_kinds.clear();
 }
 
 template <class R>
@@ -297,6 +326,8 @@ void set_smem_limits(int small_front) {
     APHI_CUDA(cudaFuncSetAttribute(k_update_panel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    2 * kStep * kTile * static_cast<int>(sizeof(cx<R>))));
     APHI_CUDA(cudaFuncSetAttribute(k_update_wide<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem<R>()));
+    if constexpr (sizeof(R) == 8)
+        APHI_CUDA(cudaFuncSetAttribute(k_update_wide_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, kDmmaSmem));
     if constexpr (sizeof(R) == 4)
         APHI_CUDA(cudaFuncSetAttribute(k_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
     APHI_CUDA(cudaFuncSetAttribute(k_fwd_diag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -389,6 +420,14 @@ aphi_factor* factor_create(aphi_analysis* an, int precision, int batch) {
 
 void factor_destroy(aphi_factor* f) { delete f; }
 
+void factor_profile(aphi_factor* f, bool enable) {
+    f->profile = enable;
+    for (int k = 0; k < APHI_PLAN_KINDS; ++k) {
+        f->prof_ms[k] = 0;
+        f->prof_launches[k] = 0;
+    }
+}
+
 int factorize(aphi_factor* f, const double* values, int equil_iters, double pivot_floor,
               aphi_factor_stats* stats_out, cudaStream_t st) {
     const aphi_analysis* A = f->an;
@@ -448,12 +487,14 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
     APHI_CUDA(cudaMemcpyAsync(&err_word, f->err, sizeof(int), cudaMemcpyDeviceToHost, st));
     APHI_CUDA(cudaStreamSynchronize(st));
     if (err_word != 0) {
+        if (f->profile) collect_profile(f);
         APHI_CUDA(cudaMemsetAsync(f->err, 0, sizeof(int), st));
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         f->factored = false;
         throw Error(APHI_ERR_TIMEOUT, "factorize: a tensor-core tile's bounded wait expired");
     }
+    if (f->profile) collect_profile(f);
     float ms = 0;
     APHI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     cudaEventDestroy(e0);
@@ -1055,6 +1096,7 @@ void factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, do
 }  // namespace aphi_b200
 
 aphi_factor::~aphi_factor() {
+    for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
     void* ptrs[] = {L, dscale, rowmax, stats, dref, y, U, part, ir, red, norms, kr, err};
     for (void* p : ptrs)
         if (p) cudaFree(p);

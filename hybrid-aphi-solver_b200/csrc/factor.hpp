@@ -36,6 +36,12 @@ struct aphi_factor {
     bool factored = false;
     bool use_tc = true;         // FP32: tensor-core updates (APHI_NO_TC=1 selects the SIMT kernels)
     int* err = nullptr;         // device error word (bounded waits)
+    // Per-kind launch timing (aphi_factor_profile).
+    bool profile = false;
+    std::vector<cudaEvent_t> prof_events;  // pairs, one per launch of the current factorization
+    std::vector<int> prof_kinds;
+    double prof_ms[APHI_PLAN_KINDS] = {};
+    long long prof_launches[APHI_PLAN_KINDS] = {};
     std::vector<aphi_factor_stats> host_stats;
     ~aphi_factor();
 };
@@ -44,6 +50,7 @@ namespace aphi_b200 {
 
 aphi_factor* factor_create(aphi_analysis* an, int precision, int batch);
 void factor_destroy(aphi_factor* f);
+void factor_profile(aphi_factor* f, bool enable);
 int factorize(aphi_factor* f, const double* values_dev, int equil_iters, double pivot_floor,
               aphi_factor_stats* stats, cudaStream_t stream);
 void solve(aphi_factor* f, int nrhs, const double* b_dev, double* x_dev, cudaStream_t stream);

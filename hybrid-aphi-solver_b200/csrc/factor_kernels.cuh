@@ -368,14 +368,17 @@ __global__ void __launch_bounds__(256) k_update_wide(Sched S, long long item0, c
     const int tid = threadIdx.x;
     // Loader: A chunk entry (k = tid / 128 + 2q, r = tid % 128), q < 4; B chunk
     // entry (k = tid / 64 + 4q, r = tid % 64), q < 2.
-    cx<R> pa[4], pb[2];
+    cx<R> pa[4], pd[4], pb[2];
     auto load = [&](int kbase) {
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int k = kbase + (tid >> 7) + 2 * q, r = tid & 127;
             pa[q] = cx<R>{0, 0};
-            if (k < K && i0 + r < m)
-                pa[q] = P[static_cast<long long>(k) * m + i0 + r] * dg[static_cast<long long>(k) * (m + 1)];
+            pd[q] = cx<R>{0, 0};
+            if (k < K && i0 + r < m) {
+                pa[q] = P[static_cast<long long>(k) * m + i0 + r];
+                pd[q] = dg[static_cast<long long>(k) * (m + 1)];
+            }
         }
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
@@ -388,7 +391,7 @@ __global__ void __launch_bounds__(256) k_update_wide(Sched S, long long item0, c
         cx<R>* A = As + buf * kWideKC * kWideM;
         cx<R>* B = Bs + buf * kWideKC * kWideN;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) A[((tid >> 7) + 2 * q) * kWideM + (tid & 127)] = pa[q];
+        for (int q = 0; q < 4; ++q) A[((tid >> 7) + 2 * q) * kWideM + (tid & 127)] = pa[q] * pd[q];
 #pragma unroll
         for (int q = 0; q < 2; ++q) B[((tid >> 6) + 4 * q) * kWideN + (tid & 63)] = pb[q];
     };
@@ -442,6 +445,137 @@ __global__ void __launch_bounds__(256) k_update_wide(Sched S, long long item0, c
 #pragma unroll
         for (int a = 0; a < 8; ++a)
             if (dst[a]) *dst[a] = old[a] - acc[a][b];
+    }
+}
+
+// FP64 trailing update of a complete panel on the FP64 tensor path (DMMA,
+// mma.sync m8n8k4). Same items, tile and K as k_update_wide. 8 warps in a 4 x 2
+// grid, each a 32 x 32 complex block of the tile: 4 x 4 blocks of 8 x 8, each
+// four real products (Cr += Ar Br - Ai Bi, Ci += Ar Bi + Ai Br; the minus by
+// a negated copy of Ai's fragment). Operands are staged as complex pairs
+// (k-major rows, 130 / 66 entries apart so that one quarter-warp's 16-byte
+// fragment loads touch distinct banks), 8 columns of K per double-buffered
+// chunk; a k-step of 4 costs a warp 8 shared loads for 64 DMMA.
+constexpr int kDmmaLdA = kWideM + 2, kDmmaLdB = kWideN + 2;
+constexpr int kDmmaSmem = 2 * kWideKC * (kDmmaLdA + kDmmaLdB) * 16;
+
+__device__ __forceinline__ void dmma884(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long item0, cx<double>* Lb,
+                                                          cx<double>* CBb, long long lstride, long long cbstride) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<double>* As = reinterpret_cast<cx<double>*>(smem_raw);   // [2][KC][kDmmaLdA], scaled by D
+    cx<double>* Bs = As + 2 * kWideKC * kDmmaLdA;                // [2][KC][kDmmaLdB]
+    const Item it = S.items[item0 + blockIdx.x];
+    const int s = it.s, p0 = it.a, i0 = it.b, j0 = it.c;
+    cx<double>* L = Lb + lstride * blockIdx.y;
+    cx<double>* CB = CBb + cbstride * blockIdx.y;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int cs = m - w;
+    const int K = min(kTcPanel, w - p0);
+    cx<double>* Ls = L + S.loff[s];
+    cx<double>* CBs = CB + (cs > 0 ? S.cboff[s] : 0);
+    const cx<double>* P = Ls + static_cast<long long>(p0) * m;
+    const cx<double>* dg = Ls + p0 + static_cast<long long>(p0) * m;
+    const int tid = threadIdx.x;
+    // Raw values stay in registers until the stash, so the loads' latency is
+    // covered by the chunk being computed.
+    cx<double> pa[4], pd[4], pb[2];
+    auto load = [&](int kbase) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int k = kbase + (tid >> 7) + 2 * q, r = tid & 127;
+            pa[q] = cx<double>{0, 0};
+            pd[q] = cx<double>{0, 0};
+            if (k < K && i0 + r < m) {
+                pa[q] = P[static_cast<long long>(k) * m + i0 + r];
+                pd[q] = dg[static_cast<long long>(k) * (m + 1)];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int k = kbase + (tid >> 6) + 4 * q, r = tid & 63;
+            pb[q] = cx<double>{0, 0};
+            if (k < K && j0 + r < m) pb[q] = P[static_cast<long long>(k) * m + j0 + r];
+        }
+    };
+    auto stash = [&](int buf) {
+        cx<double>* A = As + buf * kWideKC * kDmmaLdA;
+        cx<double>* B = Bs + buf * kWideKC * kDmmaLdB;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) A[((tid >> 7) + 2 * q) * kDmmaLdA + (tid & 127)] = pa[q] * pd[q];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) B[((tid >> 6) + 4 * q) * kDmmaLdB + (tid & 63)] = pb[q];
+    };
+    const int warp = tid >> 5, lane = tid & 31;
+    const int wm = warp & 3, wn = warp >> 2;
+    const int g = lane >> 2, t4 = lane & 3;
+    double cr[4][4][2], ci[4][4][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) cr[a][b][0] = cr[a][b][1] = ci[a][b][0] = ci[a][b][1] = 0.0;
+    const int nc = (K + kWideKC - 1) / kWideKC;
+    load(0);
+    stash(0);
+    __syncthreads();
+    for (int c = 0; c < nc; ++c) {
+        if (c + 1 < nc) load((c + 1) * kWideKC);
+        const cx<double>* A = As + (c & 1) * kWideKC * kDmmaLdA;
+        const cx<double>* B = Bs + (c & 1) * kWideKC * kDmmaLdB;
+#pragma unroll
+        for (int ks = 0; ks < kWideKC; ks += 4) {
+            cx<double> af[4], bf[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) af[a] = A[(ks + t4) * kDmmaLdA + 32 * wm + 8 * a + g];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) bf[b] = B[(ks + t4) * kDmmaLdB + 32 * wn + 8 * b + g];
+            // One real product over all 16 blocks before the next, so that
+            // consecutive MMAs never feed one another.
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) dmma884(cr[a][b], af[a].re, bf[b].re);
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) dmma884(ci[a][b], af[a].re, bf[b].im);
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) dmma884(cr[a][b], -af[a].im, bf[b].im);
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) dmma884(ci[a][b], af[a].im, bf[b].re);
+        }
+        if (c + 1 < nc) stash((c + 1) & 1);
+        __syncthreads();
+    }
+    // Thread holds C[g][2 t4 + e] of each 8 x 8 block: rows i0 + 32 wm + 8a + g,
+    // columns j0 + 32 wn + 8b + 2 t4 + e. Read-modify-write per block row.
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int i = i0 + 32 * wm + 8 * a + g;
+        cx<double>* dst[8];
+        cx<double> old[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int j = j0 + 32 * wn + 8 * (q >> 1) + 2 * t4 + (q & 1);
+            dst[q] = nullptr;
+            if (j < m && i < m && i >= j)
+                dst[q] = (j < w) ? Ls + i + static_cast<long long>(j) * m
+                                 : CBs + (i - w) + static_cast<long long>(j - w) * cs;
+            if (dst[q]) old[q] = *dst[q];
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            if (dst[q]) *dst[q] = cx<double>{old[q].re - cr[a][q >> 1][q & 1], old[q].im - ci[a][q >> 1][q & 1]};
     }
 }
 

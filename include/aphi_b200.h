@@ -289,9 +289,27 @@ int aphi_solve_symmetric_host(const aphi_analysis* an, const double* values, con
  * update tile,
  * 5-9 solve kernels (gather, forward diagonal, forward update, backward
  * update, backward diagonal), 10 panel-restricted update tile, 11
- * tensor-core update tile. */
+ * tensor-core update tile. useful[k] (may be NULL): the real flops of the
+ * update kinds' Schur-complement work, counting only lower-triangle entries
+ * (8 per complex multiply-add); executed[k] (may be NULL): the flops their
+ * tiles perform, padding included. */
 #define APHI_PLAN_KINDS 12
-int aphi_analysis_plan_stats(const aphi_analysis* a, int plan, int64_t* launches, int64_t* items);
+int aphi_analysis_plan_stats(const aphi_analysis* a, int plan, int64_t* launches, int64_t* items, double* useful,
+                             double* executed);
+
+/* Per-kind device time of a factor's factorizations: while enabled, every
+ * launch of the factorization plan is bracketed by CUDA events on its stream
+ * and its duration added to ms[kind] (launch counts in launches[kind]).
+ * Enabling clears the totals. Costs two events per launch: for measurement
+ * runs, not for timed ones. */
+int aphi_factor_profile(aphi_factor* f, int enable);
+int aphi_factor_profile_read(const aphi_factor* f, double* ms, int64_t* launches);
+
+/* Arithmetic peaks of the current device, measured by short register- or
+ * shared-memory-resident loops (2 CTAs per SM, CUDA events): tflops[0] FP64
+ * on the DMMA path (mma.sync m8n8k4), [1] FP64 DFMA, [2] FP32 FFMA, [3] TF32
+ * tcgen05 M128 N64, [4] TF32 tcgen05 M128 N256 (TFLOP/s, 2 per multiply-add). */
+int aphi_measure_peaks(double* tflops);
 
 /* One tensor-core update tile on host data: out (128 x 64 complex64,
  * column-major, leading dimension 128) = sum_{k<K} (P[i0+r, k] d[k])

@@ -49,3 +49,23 @@ def test_analysis_matches_reference_etree_on_host():
         raise AssertionError("expected a LogicError")
     except ab.LogicError:
         pass
+
+
+def test_plan_stats_account_for_the_same_update_work():
+    """Both factorization plans (SIMT trailing tiles, tensor-core trailing
+    tiles) do the same Schur-complement work: equal useful flops per kind,
+    never more useful than executed, and each uses only its own tile kind."""
+    w = ab.Workload.cylinder(10)
+    an = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx))
+    simt = an.plan_stats(0, flops=True)
+    tc = an.plan_stats(1, flops=True)
+    assert "update_tc" not in simt and "update_wide" not in tc
+    assert simt["update_wide"][1] == tc["update_tc"][1]
+    assert simt["update_wide"][2] == tc["update_tc"][2]
+    assert simt["update_panel"] == tc["update_panel"]
+    for st in (simt, tc):
+        for kind, (_, _, useful, executed) in st.items():
+            assert useful <= executed
+    # the trailing and in-panel updates carry (almost) all of the factorization's flops
+    total = simt["update_wide"][2] + simt["update_panel"][2]
+    assert 0.9 * an.info["flops"] <= total <= 1.5 * an.info["flops"]

@@ -288,3 +288,28 @@ def test_cocg_refinement_converges(cuda):
     x, iters, berr, ok = f.solve_refined(vals, rhs, tol=1e-16, rtol=1e-13, max_iters=40, krylov=True)
     res = ab.residuals(an, vals, x, rhs)
     assert ok and (res[:, 0, 0] <= 1e-13).all(), (iters, res)
+
+
+def test_factor_profile_counts_every_planned_launch(cuda):
+    """aphi_factor_profile: one factorization with timing on records exactly
+    the launches its plan holds, per kind, with positive durations."""
+    w = ab.Workload.cylinder(10)
+    an = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx))
+    asm = ab.Assembly(ab.workload_arrays(w))
+    vals, _ = asm.refill(2 * np.pi * np.array([50.0, 1e3]))
+    for prec, plan in ((ab.PREC_FP64, 0), (ab.PREC_FP32, 1)):
+        f = ab.Factor(an, precision=prec, batch=2)
+        f.profile(True)
+        assert f.factorize(vals)
+        got = f.profile_read()
+        want = an.plan_stats(plan)
+        assert {k: v[0] for k, v in got.items()} == {k: v[0] for k, v in want.items()}
+        assert all(ms > 0 for _, ms in got.values())
+        f.profile(False)
+
+
+def test_measured_peaks_are_plausible(cuda):
+    p = ab.measure_peaks()
+    assert 10 < p["fp64_dmma"] < 100 and 10 < p["fp64_dfma"] < 100
+    assert 30 < p["fp32_ffma"] < 200
+    assert 200 < p["tf32_tc_n64"] <= p["tf32_tc_n256"] * 1.05 < 3000
