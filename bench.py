@@ -231,6 +231,7 @@ def run_ours(args):
     # events around each launch, on the stream the kernels run on.
     solver.profile(True)
     step_ms = []
+    torch.cuda.nvtx.range_push("timed")   # ncu --nvtx --nvtx-include "timed/" captures exactly these steps
     with Clocks(local) as clk:
         t0, t1 = ev(), ev()
         t0.record(stream)
@@ -243,6 +244,7 @@ def run_ours(args):
             step_ms.append(s0.elapsed_time(s1))
         t1.record(stream)
         torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     launches = (ab.launch_count() - launches0) // max(args.steps, 1)
     kind_ms = solver.profile_read()
     entries = {"fp32": solver.factorized[ab.PREC_FP32], "fp64": solver.factorized[ab.PREC_FP64]}
@@ -333,7 +335,8 @@ def run_ours(args):
     traffic_path = ROOT / "profiles" / "traffic.json"
     traffic = None
     if traffic_path.exists():
-        traffic = json.loads(traffic_path.read_text()).get(f"{top['precision']}_{top['kind']}_{args.cells}")
+        t = json.loads(traffic_path.read_text()).get(f"{top['precision']}_{top['kind']}_{args.cells}")
+        traffic = t["bytes_per_launch"] if t else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
