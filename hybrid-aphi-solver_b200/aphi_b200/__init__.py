@@ -141,6 +141,9 @@ _SIGS = {
     "aphi_analysis_plan_stats": (I, [P, I, PI64, PI64, PD, PD]),
     "aphi_factor_profile": (I, [P, I]),
     "aphi_measure_peaks": (I, [PD]),
+    "aphi_factorize_host": (I, [P, PD, I, D, C.POINTER(FactorStats)]),
+    "aphi_solve_host": (I, [P, I, PD, PD]),
+    "aphi_residuals_host": (I, [P, I, I, PD, PD, PD, PD]),
     "aphi_factor_profile_read": (I, [P, PD, PI64]),
 }
 

@@ -22,7 +22,13 @@ struct aphi_assembly {
 #include <atomic>
 
 namespace aphi_b200 {
-thread_local std::string g_last_error;
+thread_local char g_last_error[kLastErrorBytes];
+
+void set_last_error(const char* msg) {
+    size_t i = 0;
+    for (; msg && msg[i] && i + 1 < static_cast<size_t>(kLastErrorBytes); ++i) g_last_error[i] = msg[i];
+    g_last_error[i] = 0;
+}
 static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 void nested_dissection(int n, const int* row_ptr, const int* col_idx, const double* xyz, int leaf, int* perm);
@@ -50,7 +56,7 @@ const char* aphi_status_string(int s) {
     return "unknown status";
 }
 
-const char* aphi_last_error(void) { return g_last_error.c_str(); }
+const char* aphi_last_error(void) { return g_last_error; }
 
 int64_t aphi_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 

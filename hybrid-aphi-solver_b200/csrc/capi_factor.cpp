@@ -33,7 +33,7 @@ int aphi_factorize(aphi_factor* f, const double* values_dev, int equil_iters, do
         if (!f) throw Error(APHI_ERR_INVALID, "aphi_factorize: null factor");
         rc = factorize(f, values_dev, equil_iters, pivot_floor, stats, as_stream(stream));
         if (rc == APHI_ERR_PIVOT_FLOOR)
-            g_last_error = "factorize_ldlt: a pivot at or below the floor stopped the factorization";
+            set_last_error("factorize_ldlt: a pivot at or below the floor stopped the factorization");
     });
     if (g != APHI_OK) return g;
     return rc;
@@ -100,10 +100,81 @@ int aphi_solve_refined(aphi_factor* f, int nrhs, const double* values_dev, const
         aphi_ir_options o{40, 1e-16, 0.5, 1, 1e-14};
         if (opt) o = *opt;
         rc = solve_refined(f, nrhs, values_dev, b_dev, x_dev, o, iters, berr, as_stream(stream));
-        if (rc == APHI_ERR_IR_STALL) g_last_error = "iterative refinement stalled before reaching the tolerance";
+        if (rc == APHI_ERR_IR_STALL) set_last_error("iterative refinement stalled before reaching the tolerance");
     });
     if (g != APHI_OK) return g;
     return rc;
+}
+
+namespace {
+double* grow(double*& buf, size_t& have, size_t need) {
+    if (have < need) {
+        if (buf) cudaFree(buf);
+        buf = nullptr;
+        have = 0;
+        APHI_CUDA(cudaMalloc(&buf, std::max<size_t>(need, 16)));
+        have = need;
+    }
+    return buf;
+}
+}  // namespace
+
+int aphi_factorize_host(aphi_factor* f, const double* values, int equil_iters, double pivot_floor,
+                        aphi_factor_stats* stats) {
+    int rc = APHI_OK;
+    const int g = guard([&] {
+        if (!f || !values) throw Error(APHI_ERR_INVALID, "aphi_factorize_host: null argument");
+        const size_t bytes = sizeof(double) * 2 * static_cast<size_t>(f->an->S.nnz_a) * f->batch;
+        double* dv = grow(f->hvals, f->hvals_bytes, bytes);
+        APHI_CUDA(cudaMemcpy(dv, values, bytes, cudaMemcpyHostToDevice));
+        rc = factorize(f, dv, equil_iters, pivot_floor, stats, nullptr);
+        if (rc == APHI_ERR_PIVOT_FLOOR)
+            set_last_error("factorize_ldlt: a pivot at or below the floor stopped the factorization");
+    });
+    if (g != APHI_OK) return g;
+    return rc;
+}
+
+int aphi_solve_host(aphi_factor* f, int nrhs, const double* b, double* x) {
+    return guard([&] {
+        if (!f || !b || !x) throw Error(APHI_ERR_INVALID, "aphi_solve_host: null argument");
+        if (nrhs < 1) throw Error(APHI_ERR_BAD_SHAPE, "aphi_solve_host: nrhs must be >= 1");
+        const size_t len = sizeof(double) * 2 * static_cast<size_t>(f->an->S.n) * nrhs * f->batch;
+        double* d = grow(f->hvec, f->hvec_bytes, 2 * len);
+        APHI_CUDA(cudaMemcpy(d, b, len, cudaMemcpyHostToDevice));
+        solve(f, nrhs, d, d + len / sizeof(double), nullptr);
+        APHI_CUDA(cudaMemcpy(x, d + len / sizeof(double), len, cudaMemcpyDeviceToHost));
+    });
+}
+
+int aphi_residuals_host(const aphi_analysis* an_c, int batch, int nrhs, const double* values, const double* x,
+                        const double* b, double* out) {
+    return guard([&] {
+        if (!an_c || !values || !x || !b || !out) throw Error(APHI_ERR_INVALID, "aphi_residuals_host: null argument");
+        if (batch < 1 || nrhs < 1) throw Error(APHI_ERR_BAD_SHAPE, "aphi_residuals_host: batch and nrhs must be >= 1");
+        auto* an = const_cast<aphi_analysis*>(an_c);
+        analysis_ensure_device(an);
+        const size_t vb = sizeof(double) * 2 * static_cast<size_t>(an->S.nnz_a) * batch;
+        const size_t xb = sizeof(double) * 2 * static_cast<size_t>(an->S.n) * nrhs * batch;
+        double *dv = nullptr, *dx = nullptr, *db = nullptr;
+        try {
+            APHI_CUDA(cudaMalloc(&dv, std::max<size_t>(vb, 16)));
+            APHI_CUDA(cudaMalloc(&dx, std::max<size_t>(xb, 16)));
+            APHI_CUDA(cudaMalloc(&db, std::max<size_t>(xb, 16)));
+            APHI_CUDA(cudaMemcpy(dv, values, vb, cudaMemcpyHostToDevice));
+            APHI_CUDA(cudaMemcpy(dx, x, xb, cudaMemcpyHostToDevice));
+            APHI_CUDA(cudaMemcpy(db, b, xb, cudaMemcpyHostToDevice));
+            residuals(an, batch, nrhs, dv, dx, db, out, nullptr);
+        } catch (...) {
+            cudaFree(dv);
+            cudaFree(dx);
+            cudaFree(db);
+            throw;
+        }
+        cudaFree(dv);
+        cudaFree(dx);
+        cudaFree(db);
+    });
 }
 
 int aphi_solve_symmetric_host(const aphi_analysis* an_c, const double* values, const double* b, int equil_iters,
@@ -146,7 +217,7 @@ int aphi_solve_symmetric_host(const aphi_analysis* an_c, const double* values, c
                 report[0] = 1.0;
                 APHI_CUDA(cudaMemcpy(x, dx, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost));
             } else {
-                g_last_error = "factorize_ldlt: a pivot at or below the floor stopped the factorization";
+                set_last_error("factorize_ldlt: a pivot at or below the floor stopped the factorization");
             }
         } catch (...) {
             cudaFree(dv);

@@ -9,25 +9,32 @@
 
 namespace aphi_b200 {
 
-extern thread_local std::string g_last_error;
+// The calling thread's last error message. A plain character array, so that
+// it stays usable while the process tears down: a caller may release handles
+// from its own static destructors, after the thread's C++ thread_local
+// objects have been destroyed.
+constexpr int kLastErrorBytes = 1024;
+extern thread_local char g_last_error[kLastErrorBytes];
+void set_last_error(const char* msg);
+inline void set_last_error(const std::string& msg) { set_last_error(msg.c_str()); }
 
 template <class F>
 int guard(F&& body) {
     try {
         body();
-        g_last_error.clear();
+        g_last_error[0] = 0;
         return APHI_OK;
     } catch (const Error& e) {
-        g_last_error = e.what();
+        set_last_error(e.what());
         return e.status;
     } catch (const std::bad_alloc& e) {
-        g_last_error = std::string("host allocation failed: ") + e.what();
+        set_last_error(std::string("host allocation failed: ") + e.what());
         return APHI_ERR_OOM;
     } catch (const std::exception& e) {
-        g_last_error = e.what();
+        set_last_error(e.what());
         return APHI_ERR_INVALID;
     } catch (...) {
-        g_last_error = "unknown exception";
+        set_last_error("unknown exception");
         return APHI_ERR_INVALID;
     }
 }

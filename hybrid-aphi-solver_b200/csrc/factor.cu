@@ -1097,7 +1097,7 @@ void factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, do
 
 aphi_factor::~aphi_factor() {
     for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
-    void* ptrs[] = {L, dscale, rowmax, stats, dref, y, U, part, ir, red, norms, kr, err};
+    void* ptrs[] = {L, dscale, rowmax, stats, dref, y, U, part, ir, red, norms, kr, err, hvals, hvec};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }

@@ -42,6 +42,11 @@ struct aphi_factor {
     std::vector<int> prof_kinds;
     double prof_ms[APHI_PLAN_KINDS] = {};
     long long prof_launches[APHI_PLAN_KINDS] = {};
+    // Host-buffer entry points stage through these (grown on demand).
+    double* hvals = nullptr;
+    size_t hvals_bytes = 0;
+    double* hvec = nullptr;    // b then x
+    size_t hvec_bytes = 0;
     std::vector<aphi_factor_stats> host_stats;
     ~aphi_factor();
 };

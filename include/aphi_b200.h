@@ -272,6 +272,17 @@ int aphi_solve_refined(aphi_factor* f, int nrhs, const double* values_dev, const
                        double* x_dev, const aphi_ir_options* opt, int* iters, double* berr,
                        void* stream);
 
+/* Host-buffer forms of aphi_factorize, aphi_solve and aphi_residuals for
+ * callers that hold no device memory (the drop-in C++ layer): the same
+ * arguments with host pointers; the data is staged through device buffers the
+ * factor keeps (grown on demand) and the calls return when the results are on
+ * the host. */
+int aphi_factorize_host(aphi_factor* f, const double* values, int equil_iters, double pivot_floor,
+                        aphi_factor_stats* stats);
+int aphi_solve_host(aphi_factor* f, int nrhs, const double* b, double* x);
+int aphi_residuals_host(const aphi_analysis* an, int batch, int nrhs, const double* values, const double* x,
+                        const double* b, double* out);
+
 /* The whole solve_symmetric pipeline (src/factorization.cpp:332-398) on
  * host buffers, FP64: equilibrate, factorize, solve, unscale, measure.
  * report[0..12] as SolveReport: ok, backward_error, residual, equil_min,
