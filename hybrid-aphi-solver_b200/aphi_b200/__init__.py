@@ -140,6 +140,7 @@ _SIGS = {
     "aphi_selftest_tc_tile": (I, [I, I, I, I, P, P, P]),
     "aphi_analysis_plan_stats": (I, [P, I, PI64, PI64, PD, PD]),
     "aphi_factor_profile": (I, [P, I]),
+    "aphi_factor_set_batch": (I, [P, I]),
     "aphi_measure_peaks": (I, [PD]),
     "aphi_factorize_host": (I, [P, PD, I, D, C.POINTER(FactorStats)]),
     "aphi_solve_host": (I, [P, I, PD, PD]),
@@ -487,6 +488,7 @@ class Factor:
         self.analysis = analysis
         self.precision = precision
         self.batch = batch
+        self.capacity = batch
         self.n = analysis.n
         self._h = P()
         check(lib().aphi_factor_create(analysis._h, precision, batch, C.byref(self._h)))
@@ -537,6 +539,11 @@ class Factor:
         x = x.squeeze(1) if squeeze else x
         return x, np.array(list(it)).reshape(self.batch, nrhs), np.array(list(be)).reshape(self.batch, nrhs), rc == OK
 
+    def set_batch(self, batch: int) -> None:
+        """Process `batch` (1..capacity) entries from now on, without reallocating."""
+        check(lib().aphi_factor_set_batch(self._h, batch))
+        self.batch = batch
+
     def profile(self, enable: bool = True) -> None:
         """Per-kind device timing of later factorizations (clears the totals)."""
         check(lib().aphi_factor_profile(self._h, 1 if enable else 0))
@@ -584,7 +591,7 @@ def residuals(analysis: Analysis, values, x, b, stream=None) -> np.ndarray:
     batch, nrhs = bb.shape[0], bb.shape[1]
     out = np.zeros((batch, nrhs, 2))
     check(lib().aphi_residuals(analysis._h, batch, nrhs, dptr(values), dptr(xx.contiguous()),
-                               dptr(bb.contiguous()), out.ctypes.data_as(PD), None))
+                               dptr(bb.contiguous()), out.ctypes.data_as(PD), stream_ptr(stream)))
     return out
 
 

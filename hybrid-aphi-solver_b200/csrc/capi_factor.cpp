@@ -46,6 +46,13 @@ int aphi_solve(aphi_factor* f, int nrhs, const double* b_dev, double* x_dev, voi
     });
 }
 
+int aphi_factor_set_batch(aphi_factor* f, int batch) {
+    return guard([&] {
+        if (!f) throw Error(APHI_ERR_INVALID, "aphi_factor_set_batch: null factor");
+        factor_set_batch(f, batch);
+    });
+}
+
 int aphi_factor_profile(aphi_factor* f, int enable) {
     return guard([&] {
         if (!f) throw Error(APHI_ERR_INVALID, "aphi_factor_profile: null factor");

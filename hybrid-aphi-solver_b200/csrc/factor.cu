@@ -317,9 +317,13 @@ void collect_profile(aphi_factor* f) {
     f->prof_kinds.clear();
 }
 
+// Opt-in shared-memory limits, set once per process; serialized because
+// factors are used from several host threads at once (one stream each).
 template <class R>
 void set_smem_limits(int small_front) {
+    static std::mutex mu;
     static bool done = false;
+    std::lock_guard<std::mutex> lock(mu);
     if (done) return;
     APHI_CUDA(cudaFuncSetAttribute(k_small_front<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    96 * 96 * static_cast<int>(sizeof(cx<R>))));
@@ -365,10 +369,10 @@ void solve_numeric(aphi_factor* f, int nrhs, const double* b, double* x, cudaStr
         if (f->U) cudaFree(f->U);
         if (f->part) cudaFree(f->part);
         f->y = f->U = f->part = nullptr;
-        APHI_CUDA(cudaMalloc(&f->y, static_cast<size_t>(n) * nrhs * f->batch * sizeof(cx<R>) + 16));
-        APHI_CUDA(cudaMalloc(&f->U, static_cast<size_t>(std::max<long long>(A->upool, 1)) * nrhs * f->batch *
+        APHI_CUDA(cudaMalloc(&f->y, static_cast<size_t>(n) * nrhs * f->capacity * sizeof(cx<R>) + 16));
+        APHI_CUDA(cudaMalloc(&f->U, static_cast<size_t>(std::max<long long>(A->upool, 1)) * nrhs * f->capacity *
                                         sizeof(cx<R>)));
-        APHI_CUDA(cudaMalloc(&f->part, static_cast<size_t>(A->max_parts) * kSolveBlock * 8 * f->batch * sizeof(cx<R>)));
+        APHI_CUDA(cudaMalloc(&f->part, static_cast<size_t>(A->max_parts) * kSolveBlock * 8 * f->capacity * sizeof(cx<R>)));
         f->nrhs_cap = nrhs;
     }
     set_smem_limits<R>(A->opt.small_front);
@@ -399,6 +403,7 @@ aphi_factor* factor_create(aphi_analysis* an, int precision, int batch) {
         f->an = an;
         f->precision = precision;
         f->batch = batch;
+        f->capacity = batch;
         f->elem = precision == 64 ? 16 : 8;
         const char* no_tc = std::getenv("APHI_NO_TC");
         f->use_tc = !(no_tc && no_tc[0] == '1');
@@ -409,6 +414,7 @@ aphi_factor* factor_create(aphi_analysis* an, int precision, int batch) {
         f->stats = dalloc<unsigned long long>(4 * static_cast<size_t>(batch));
         f->dref = dalloc<double>(2 * static_cast<size_t>(S.n) * batch);
         f->err = dalloc<int>(4);
+        f->kmax = dalloc<int>(batch);
         APHI_CUDA(cudaMemset(f->err, 0, 4 * sizeof(int)));
         f->host_stats.assign(batch, aphi_factor_stats{});
     } catch (...) {
@@ -419,6 +425,13 @@ aphi_factor* factor_create(aphi_analysis* an, int precision, int batch) {
 }
 
 void factor_destroy(aphi_factor* f) { delete f; }
+
+void factor_set_batch(aphi_factor* f, int batch) {
+    if (batch < 1 || batch > f->capacity)
+        throw Error(APHI_ERR_BAD_SHAPE, "factor_set_batch: the active batch must be 1.." + std::to_string(f->capacity));
+    f->batch = batch;
+    f->factored = false;
+}
 
 void factor_profile(aphi_factor* f, bool enable) {
     f->profile = enable;
@@ -534,7 +547,7 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
         }
     }
     // Largest multiplier, over the rows the reference would have reached.
-    int* d_kmax = dalloc<int>(B);
+    int* d_kmax = f->kmax;
     APHI_CUDA(cudaMemcpyAsync(d_kmax, kmax.data(), sizeof(int) * B, cudaMemcpyHostToDevice, st));
     APHI_CUDA(cudaMemsetAsync(f->stats, 0, sizeof(unsigned long long) * 4 * B, st));
     if (A->stat_count > 0) {
@@ -552,7 +565,6 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
     std::vector<unsigned long long> mx(4 * B);
     APHI_CUDA(cudaMemcpyAsync(mx.data(), f->stats, sizeof(unsigned long long) * 4 * B, cudaMemcpyDeviceToHost, st));
     APHI_CUDA(cudaStreamSynchronize(st));
-    cudaFree(d_kmax);
     for (int b = 0; b < B; ++b) {
         double v;
         std::memcpy(&v, &mx[b], sizeof(double));
@@ -567,8 +579,8 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
 void solve(aphi_factor* f, int nrhs, const double* b, double* x, cudaStream_t st) {
     if (!f->factored) throw Error(APHI_ERR_INVALID, "solve: the factor holds no factorization");
     if (nrhs < 1) throw Error(APHI_ERR_BAD_SHAPE, "solve: nrhs must be at least 1");
-    for (const aphi_factor_stats& s : f->host_stats)
-        if (!s.ok)
+    for (int k = 0; k < f->batch; ++k)
+        if (!f->host_stats[k].ok)
             throw Error(APHI_ERR_ZERO_PIVOT,
                         "solve_in_place: the factorization stopped at a pivot at or below the floor, so "
                         "this factor cannot be used.");
@@ -578,14 +590,40 @@ void solve(aphi_factor* f, int nrhs, const double* b, double* x, cudaStream_t st
         solve_numeric<float>(f, nrhs, b, x, st);
 }
 
+// Per-thread device scratch that only grows: freeing device memory
+// synchronizes the whole device, which would stall work other threads have
+// in flight on their own streams.
+struct ThreadScratch {
+    double* p = nullptr;
+    size_t doubles = 0;
+    int device = -1;
+    ~ThreadScratch() {
+        if (p) cudaFree(p);
+    }
+    double* get(size_t need) {
+        int dev = 0;
+        APHI_CUDA(cudaGetDevice(&dev));
+        if (need > doubles || dev != device) {
+            if (p) cudaFree(p);
+            p = nullptr;
+            doubles = 0;
+            p = dalloc<double>(need);
+            doubles = need;
+            device = dev;
+        }
+        return p;
+    }
+};
+thread_local ThreadScratch t_residual_scratch;
+
 void residuals(const aphi_analysis* an, int batch, int nrhs, const double* values, const double* x,
                const double* b, double* out, cudaStream_t st) {
-    // Uses per-call scratch: residuals are off the hot loop.
     const int n = an->S.n;
     const int nb = ceil_div(std::max(n, 1), 256);
-    double* partial = dalloc<double>(static_cast<size_t>(nb) * 3 * batch * nrhs);
-    unsigned long long* amax = dalloc<unsigned long long>(batch);
-    double* norms = dalloc<double>(4 * static_cast<size_t>(batch) * nrhs);
+    const size_t np = static_cast<size_t>(nb) * 3 * batch * nrhs;
+    double* partial = t_residual_scratch.get(np + batch + 4 * static_cast<size_t>(batch) * nrhs);
+    unsigned long long* amax = reinterpret_cast<unsigned long long*>(partial + np);
+    double* norms = partial + np + batch;
     APHI_CUDA(cudaMemsetAsync(amax, 0, sizeof(unsigned long long) * batch, st));
     k_residual<<<dim3(nb, batch * nrhs), 256, 0, st>>>(n, nrhs, an->d.fptr, an->d.fcol, an->d.fmap, values,
                                                        an->S.nnz_a, x, b, nullptr, partial);
@@ -597,9 +635,6 @@ void residuals(const aphi_analysis* an, int batch, int nrhs, const double* value
     std::vector<double> h(4 * static_cast<size_t>(batch) * nrhs);
     APHI_CUDA(cudaMemcpyAsync(h.data(), norms, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     APHI_CUDA(cudaStreamSynchronize(st));
-    cudaFree(partial);
-    cudaFree(amax);
-    cudaFree(norms);
     for (int q = 0; q < batch * nrhs; ++q) {
         const double rn = h[4 * q], bn = h[4 * q + 1], xn = h[4 * q + 2], am = h[4 * q + 3];
         out[2 * q] = bn > 0.0 ? rn / bn : rn;
@@ -705,10 +740,11 @@ int solve_refined(aphi_factor* f, int nrhs, const double* values, const double* 
     const aphi_analysis* A = f->an;
     const int n = A->S.n;
     const int B = f->batch;
+    const int C = f->capacity;  // scratch is sized for the capacity, used for the active batch
     const long long len = 2LL * n * nrhs * B;
     if (f->ir_cap < nrhs) {
         if (f->ir) cudaFree(f->ir);
-        f->ir = dalloc<double>(static_cast<size_t>(len) * 2);
+        f->ir = dalloc<double>(static_cast<size_t>(2LL * n * nrhs * C) * 2);
         f->ir_cap = nrhs;
     }
     double* r = f->ir;
@@ -717,8 +753,8 @@ int solve_refined(aphi_factor* f, int nrhs, const double* values, const double* 
     if (f->red_cap < nrhs) {
         if (f->red) cudaFree(f->red);
         if (f->norms) cudaFree(f->norms);
-        f->red = dalloc<double>(static_cast<size_t>(nb) * 3 * B * nrhs + B + 1);
-        f->norms = dalloc<double>(4 * static_cast<size_t>(B) * nrhs);
+        f->red = dalloc<double>(static_cast<size_t>(nb) * 3 * C * nrhs + C + 1);
+        f->norms = dalloc<double>(4 * static_cast<size_t>(C) * nrhs);
         f->red_cap = nrhs;
     }
     unsigned long long* amax = reinterpret_cast<unsigned long long*>(f->red + static_cast<size_t>(nb) * 3 * B * nrhs);
@@ -923,8 +959,9 @@ int solve_krylov(aphi_factor* f, int nrhs, const double* values, const double* b
     if (f->kr_cap < nrhs) {
         if (f->kr) cudaFree(f->kr);
         // r, z, p, Ap; partials (3 per block per system); norms, rho, alpha,
-        // beta; max|A| words; active flags
-        f->kr = dalloc<double>(static_cast<size_t>(4 * len + 3LL * nb * q + 11LL * q + B + 16));
+        // beta; max|A| words; active flags -- sized for the capacity.
+        const long long qc = static_cast<long long>(f->capacity) * nrhs;
+        f->kr = dalloc<double>(static_cast<size_t>(4 * 2LL * n * qc + 3LL * nb * qc + 11LL * qc + f->capacity + 16));
         f->kr_cap = nrhs;
     }
     double* r = f->kr;
@@ -1097,7 +1134,7 @@ void factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, do
 
 aphi_factor::~aphi_factor() {
     for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
-    void* ptrs[] = {L, dscale, rowmax, stats, dref, y, U, part, ir, red, norms, kr, err, hvals, hvec};
+    void* ptrs[] = {L, dscale, rowmax, stats, dref, y, U, part, ir, red, norms, kr, err, kmax, hvals, hvec};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }

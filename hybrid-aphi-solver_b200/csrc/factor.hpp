@@ -12,7 +12,8 @@
 struct aphi_factor {
     aphi_analysis* an = nullptr;
     int precision = 64;
-    int batch = 1;
+    int batch = 1;             // active entries (<= capacity): what factorize/solve process
+    int capacity = 1;          // entries the buffers are sized for
     size_t elem = 16;          // bytes per complex entry
     void* L = nullptr;         // batch x stored
     void* CB = nullptr;        // batch x cb_pool: the analysis's workspace, set at factorize
@@ -36,6 +37,7 @@ struct aphi_factor {
     bool factored = false;
     bool use_tc = true;         // FP32: tensor-core updates (APHI_NO_TC=1 selects the SIMT kernels)
     int* err = nullptr;         // device error word (bounded waits)
+    int* kmax = nullptr;        // capacity: the column where each entry's factorization stopped
     // Per-kind launch timing (aphi_factor_profile).
     bool profile = false;
     std::vector<cudaEvent_t> prof_events;  // pairs, one per launch of the current factorization
@@ -56,6 +58,7 @@ namespace aphi_b200 {
 aphi_factor* factor_create(aphi_analysis* an, int precision, int batch);
 void factor_destroy(aphi_factor* f);
 void factor_profile(aphi_factor* f, bool enable);
+void factor_set_batch(aphi_factor* f, int batch);
 int factorize(aphi_factor* f, const double* values_dev, int equil_iters, double pivot_floor,
               aphi_factor_stats* stats, cudaStream_t stream);
 void solve(aphi_factor* f, int nrhs, const double* b_dev, double* x_dev, cudaStream_t stream);

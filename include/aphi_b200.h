@@ -191,8 +191,15 @@ int aphi_analysis_etree(const aphi_analysis* a, int* parent, int* col_count);
 #define APHI_PREC_FP32 32
 
 typedef struct aphi_factor aphi_factor;
+/* A factor holds `batch` numeric factorizations of one analysis (its
+ * capacity); every buffer is sized for it once. */
 int aphi_factor_create(const aphi_analysis* an, int precision, int batch, aphi_factor** out);
 int aphi_factor_destroy(aphi_factor* f);
+/* Sets how many entries (1..capacity) later calls process, without
+ * reallocating: values, right-hand sides and solutions then hold `batch`
+ * entries. Discards the current factorization. For continuous batching,
+ * where each batch's size is known only when it is formed. */
+int aphi_factor_set_batch(aphi_factor* f, int batch);
 
 typedef struct {
     int ok;                    /* FactorStats::ok */

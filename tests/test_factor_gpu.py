@@ -313,3 +313,46 @@ def test_measured_peaks_are_plausible(cuda):
     assert 10 < p["fp64_dmma"] < 100 and 10 < p["fp64_dfma"] < 100
     assert 30 < p["fp32_ffma"] < 200
     assert 200 < p["tf32_tc_n64"] <= p["tf32_tc_n256"] * 1.05 < 3000
+
+
+def test_set_batch_uses_part_of_the_capacity(cuda):
+    """aphi_factor_set_batch: a factor made for 8 entries and used for 3
+    (first use, and after a full batch) gives exactly the factorization and
+    solutions of a factor made for 3."""
+    w = ab.Workload.cylinder(6)
+    an = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx))
+    asm = ab.Assembly(ab.workload_arrays(w))
+    vals, rhs = asm.refill(2 * np.pi * np.array([50.0, 7e2, 9e3]))
+    ref = ab.Factor(an, batch=3)
+    assert ref.factorize(vals)
+    xr = ref.solve(rhs)
+    big = ab.Factor(an, batch=8)
+    for first in (True, False):
+        if not first:
+            v8, _ = asm.refill(2 * np.pi * np.geomspace(50, 1e4, 8))
+            big.set_batch(8)
+            assert big.factorize(v8)
+        big.set_batch(3)
+        assert big.factorize(vals)
+        assert bool((big.solve(rhs) == xr).all())
+    with pytest.raises(ab.InvalidArgument):
+        big.set_batch(9)
+
+
+def test_every_call_follows_the_callers_stream(cuda):
+    """refill, factorize, solve and residuals all run on the stream they are
+    given: on a non-blocking side stream, with no synchronization between
+    the calls, the residual still sees the finished solution."""
+    w = ab.Workload.cylinder(8)
+    an = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx))
+    asm = ab.Assembly(ab.workload_arrays(w))
+    f = ab.Factor(an, batch=16)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        vals, rhs = asm.refill(2 * np.pi * np.geomspace(50, 1e8, 16), stream=s)
+        assert f.factorize(vals, stream=s)
+        b = (torch.exp(1j * torch.linspace(0, 3, 8, dtype=torch.float64, device="cuda"))[None, :, None]
+             * rhs[:, None, :]).contiguous()
+        x = f.solve(b, stream=s)
+        res = ab.residuals(an, vals, x, b, stream=s)
+    assert (res[..., 0] <= 1e-12).all(), res[..., 0].max()
