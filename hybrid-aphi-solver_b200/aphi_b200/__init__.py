@@ -141,6 +141,10 @@ _SIGS = {
     "aphi_analysis_plan_stats": (I, [P, I, PI64, PI64, PD, PD]),
     "aphi_factor_profile": (I, [P, I]),
     "aphi_factor_set_batch": (I, [P, I]),
+    "aphi_fronts_create": (I, [I, PI, PI, C.POINTER(AnalysisOptions), C.POINTER(P)]),
+    "aphi_fronts_layout": (I, [P, PI64, PI64]),
+    "aphi_factorize_fronts": (I, [P, P, C.POINTER(FactorStats), P]),
+    "aphi_fronts_read": (I, [P, I, P, P, P]),
     "aphi_measure_peaks": (I, [PD]),
     "aphi_factorize_host": (I, [P, PD, I, D, C.POINTER(FactorStats)]),
     "aphi_solve_host": (I, [P, I, PD, PD]),
@@ -475,6 +479,46 @@ STATS_KEYS = ["ok", "columns_done", "smallest_pivot", "largest_pivot", "largest_
               "milliseconds", "equilibration_min", "equilibration_max"]
 
 
+class Fronts:
+    """Independent dense fronts (the supernode-update microbenchmark's
+    shape): front s has rows[s] rows, the first widths[s] its pivots. A
+    Factor made from it factorizes the fronts' panels and leaves each
+    contribution block as -L21 D L21^T (see aphi_fronts_create)."""
+
+    def __init__(self, rows, widths, options=None):
+        self.rows = np.ascontiguousarray(rows, np.int32)
+        self.widths = np.ascontiguousarray(widths, np.int32)
+        opt = options if options is not None else default_analysis_options()
+        self._h = P()
+        check(lib().aphi_fronts_create(self.rows.size, _ptr(self.rows, C.c_int), _ptr(self.widths, C.c_int),
+                                       C.byref(opt), C.byref(self._h)))
+        info = (C.c_double * 12)()
+        check(lib().aphi_analysis_info(self._h, info))
+        self.info = dict(zip(Analysis.INFO, list(info)))
+        self.n = int(self.info["n"])
+        self.stored, self.cb_pool = int(self.info["stored"]), int(self.info["cb_pool"])
+        self.panel_offset = np.zeros(self.rows.size, np.int64)
+        self.cb_offset = np.zeros(self.rows.size, np.int64)
+        check(lib().aphi_fronts_layout(self._h, self.panel_offset.ctypes.data_as(PI64),
+                                       self.cb_offset.ctypes.data_as(PI64)))
+
+    PLAN_KINDS = Analysis.PLAN_KINDS
+
+    def plan_stats(self, plan: int, flops: bool = False) -> dict:
+        return Analysis.plan_stats(self, plan, flops)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().aphi_analysis_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def _stats_dict(s: FactorStats) -> dict:
     return {k: getattr(s, k) for k in STATS_KEYS}
 
@@ -538,6 +582,26 @@ class Factor:
             check(rc)
         x = x.squeeze(1) if squeeze else x
         return x, np.array(list(it)).reshape(self.batch, nrhs), np.array(list(be)).reshape(self.batch, nrhs), rc == OK
+
+    def factorize_fronts(self, panels, stream=None) -> bool:
+        """Dense fronts: panels is a complex128 device tensor [batch, stored]
+        in the Fronts' panel layout. Returns False if a pivot was zero."""
+        st = (FactorStats * self.batch)()
+        rc = lib().aphi_factorize_fronts(self._h, dptr(panels), st, stream_ptr(stream))
+        self.stats = [_stats_dict(s) for s in st]
+        if rc == ERR_PIVOT_FLOOR:
+            return False
+        check(rc)
+        return True
+
+    def read_fronts(self, k: int = 0, stream=None):
+        """Entry k's factored panels and contribution blocks (complex128 device tensors)."""
+        import torch
+        a = self.analysis
+        panels = torch.empty(a.stored, dtype=torch.complex128, device="cuda")
+        cb = torch.empty(max(a.cb_pool, 1), dtype=torch.complex128, device="cuda")
+        check(lib().aphi_fronts_read(self._h, k, dptr(panels), dptr(cb), stream_ptr(stream)))
+        return panels, cb
 
     def set_batch(self, batch: int) -> None:
         """Process `batch` (1..capacity) entries from now on, without reallocating."""

@@ -233,6 +233,30 @@ aphi_analysis* analysis_create(int n, const int* row_ptr, const int* col_idx, co
     return A;
 }
 
+aphi_analysis* analysis_create_fronts(int count, const int* rows, const int* widths, const aphi_analysis_options& o) {
+    auto* A = new aphi_analysis;
+    try {
+        A->opt = o;
+        if (A->opt.small_front < 1) A->opt.small_front = 1;
+        if (A->opt.small_front > 96) A->opt.small_front = 96;
+        A->S = fronts_symbolic(count, rows, widths);
+        A->fronts = true;
+        build_plans(*A, A->h_items);
+        A->num_items = static_cast<long long>(A->h_items.size());
+        const Symbolic& S = A->S;
+        A->h_uoff.assign(S.ns + 1, 0);
+        for (int s = 0; s < S.ns; ++s)
+            A->h_uoff[s + 1] = A->h_uoff[s] + (S.sn_rows[s] - (S.sn_first[s + 1] - S.sn_first[s]));
+        A->upool = A->h_uoff[S.ns];
+        A->h_row_ptr.assign(S.n + 1, 0);
+        A->h_fptr.assign(S.n + 1, 0);
+    } catch (...) {
+        delete A;
+        throw;
+    }
+    return A;
+}
+
 void analysis_destroy(aphi_analysis* a) { delete a; }
 
 // Device copies are made when the first factor is created, so an analysis can

@@ -82,6 +82,7 @@ struct aphi_analysis {
     std::vector<int> h_fptr, h_fcol;
     std::vector<long long> h_fmap;
     bool on_device = false;
+    bool fronts = false;   // built from independent dense fronts (no matrix pattern)
     void* ws = nullptr;    // contribution-block workspace shared by this analysis's factors
     size_t ws_bytes = 0;
     long long num_items = 0;
@@ -96,6 +97,7 @@ struct aphi_analysis {
 namespace aphi_b200 {
 aphi_analysis* analysis_create(int n, const int* row_ptr, const int* col_idx, const int* perm,
                                const int* parent, const int* col_count, const aphi_analysis_options& o);
+aphi_analysis* analysis_create_fronts(int count, const int* rows, const int* widths, const aphi_analysis_options& o);
 void analysis_destroy(aphi_analysis* a);
 void analysis_ensure_device(aphi_analysis* a);
 void analysis_info(const aphi_analysis* a, double* info);

@@ -28,6 +28,28 @@ int aphi_analysis_create(int n, const int* row_ptr, const int* col_idx, const in
     });
 }
 
+int aphi_fronts_create(int count, const int* rows, const int* widths, const aphi_analysis_options* opt,
+                       aphi_analysis** out) {
+    return guard([&] {
+        if (!out || !rows || !widths) throw Error(APHI_ERR_INVALID, "aphi_fronts_create: null argument");
+        aphi_analysis_options o;
+        aphi_analysis_default_options(&o);
+        if (opt) o = *opt;
+        *out = analysis_create_fronts(count, rows, widths, o);
+    });
+}
+
+int aphi_fronts_layout(const aphi_analysis* a, int64_t* panel_offset, int64_t* cb_offset) {
+    return guard([&] {
+        if (!a) throw Error(APHI_ERR_INVALID, "aphi_fronts_layout: null analysis");
+        const Symbolic& S = analysis_symbolic(a);
+        for (int s = 0; s < S.ns; ++s) {
+            if (panel_offset) panel_offset[s] = S.sn_loff[s];
+            if (cb_offset) cb_offset[s] = S.sn_cboff[s];
+        }
+    });
+}
+
 int aphi_analysis_destroy(aphi_analysis* a) {
     return guard([&] { analysis_destroy(a); });
 }

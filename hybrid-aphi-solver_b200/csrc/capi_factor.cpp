@@ -46,6 +46,23 @@ int aphi_solve(aphi_factor* f, int nrhs, const double* b_dev, double* x_dev, voi
     });
 }
 
+int aphi_factorize_fronts(aphi_factor* f, const double* panels_dev, aphi_factor_stats* stats, void* stream) {
+    int rc = APHI_OK;
+    const int g = guard([&] {
+        if (!f || !panels_dev) throw Error(APHI_ERR_INVALID, "aphi_factorize_fronts: null argument");
+        rc = factorize(f, nullptr, 0, 0.0, stats, as_stream(stream), panels_dev);
+    });
+    if (g != APHI_OK) return g;
+    return rc;
+}
+
+int aphi_fronts_read(const aphi_factor* f, int k, double* panels_dev, double* cb_dev, void* stream) {
+    return guard([&] {
+        if (!f) throw Error(APHI_ERR_INVALID, "aphi_fronts_read: null factor");
+        fronts_read(f, k, panels_dev, cb_dev, as_stream(stream));
+    });
+}
+
 int aphi_factor_set_batch(aphi_factor* f, int batch) {
     return guard([&] {
         if (!f) throw Error(APHI_ERR_INVALID, "aphi_factor_set_batch: null factor");

@@ -342,16 +342,40 @@ void set_smem_limits(int small_front) {
     done = true;
 }
 
+// Complex128 -> the factor's precision, and back (dense fronts in and out).
 template <class R>
-void factorize_numeric(aphi_factor* f, const double* values, cudaStream_t st) {
+__global__ void k_narrow(long long len, const double* src, cx<R>* dst) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i < len) dst[i] = cx<R>{static_cast<R>(src[2 * i]), static_cast<R>(src[2 * i + 1])};
+}
+template <class R>
+__global__ void k_widen(long long len, const cx<R>* src, double* dst) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i < len) {
+        dst[2 * i] = static_cast<double>(src[i].re);
+        dst[2 * i + 1] = static_cast<double>(src[i].im);
+    }
+}
+
+// values: upper-CSR entries scattered into the panels; or, when `panels` is
+// given, the panels themselves (complex128, batch x stored).
+template <class R>
+void factorize_numeric(aphi_factor* f, const double* values, const double* panels, cudaStream_t st) {
     const aphi_analysis* A = f->an;
     const int n = A->S.n;
     const dim3 g(ceil_div(std::max(n, 1), 256), f->batch);
     set_smem_limits<R>(A->opt.small_front);
-    APHI_CUDA(cudaMemsetAsync(f->L, 0, static_cast<size_t>(A->S.stored) * f->batch * f->elem, st));
-    k_scatter_a<R><<<g, 256, 0, st>>>(n, A->d.row_ptr, A->d.col_idx, values, A->S.nnz_a, f->dscale, A->d.a_dest,
-                                      reinterpret_cast<cx<R>*>(f->L), A->S.stored);
-    APHI_CHECK_LAUNCH();
+    if (panels) {
+        const long long len = A->S.stored * f->batch;
+        k_narrow<R><<<ceil_div(std::max<long long>(len, 1), 256), 256, 0, st>>>(len, panels,
+                                                                              reinterpret_cast<cx<R>*>(f->L));
+        APHI_CHECK_LAUNCH();
+    } else {
+        APHI_CUDA(cudaMemsetAsync(f->L, 0, static_cast<size_t>(A->S.stored) * f->batch * f->elem, st));
+        k_scatter_a<R><<<g, 256, 0, st>>>(n, A->d.row_ptr, A->d.col_idx, values, A->S.nnz_a, f->dscale,
+                                          A->d.a_dest, reinterpret_cast<cx<R>*>(f->L), A->S.stored);
+        APHI_CHECK_LAUNCH();
+    }
     const bool tc = sizeof(R) == 4 && f->use_tc;
     run_plan<R>(f, tc ? A->plan_factor_tc : A->plan_factor, st, nullptr, nullptr, nullptr, nullptr);
     k_extract_d<R><<<dim3(A->S.ns, f->batch), 128, 0, st>>>(sched_of(A->d), A->S.ns, A->d.ref_of_post,
@@ -426,6 +450,25 @@ aphi_factor* factor_create(aphi_analysis* an, int precision, int batch) {
 
 void factor_destroy(aphi_factor* f) { delete f; }
 
+void fronts_read(const aphi_factor* f, int k, double* panels_out, double* cb_out, cudaStream_t st) {
+    const aphi_analysis* A = f->an;
+    if (!A->fronts) throw Error(APHI_ERR_INVALID, "fronts_read: not a fronts analysis");
+    if (k < 0 || k >= f->batch) throw Error(APHI_ERR_BAD_SHAPE, "fronts_read: batch index out of range");
+    if (!f->factored) throw Error(APHI_ERR_INVALID, "fronts_read: nothing factorized yet");
+    const long long ls = A->S.stored, cs = A->S.cb_pool;
+    auto widen = [&](const void* src, long long len, double* dst) {
+        if (!dst || len == 0) return;
+        if (f->precision == 64)
+            k_widen<double><<<ceil_div(len, 256), 256, 0, st>>>(len, static_cast<const cx<double>*>(src), dst);
+        else
+            k_widen<float><<<ceil_div(len, 256), 256, 0, st>>>(len, static_cast<const cx<float>*>(src), dst);
+        APHI_CHECK_LAUNCH();
+    };
+    widen(static_cast<const char*>(f->L) + static_cast<size_t>(ls) * k * f->elem, ls, panels_out);
+    widen(static_cast<const char*>(A->ws) + static_cast<size_t>(cs) * k * f->elem, cs, cb_out);
+    APHI_CUDA(cudaStreamSynchronize(st));
+}
+
 void factor_set_batch(aphi_factor* f, int batch) {
     if (batch < 1 || batch > f->capacity)
         throw Error(APHI_ERR_BAD_SHAPE, "factor_set_batch: the active batch must be 1.." + std::to_string(f->capacity));
@@ -442,12 +485,14 @@ void factor_profile(aphi_factor* f, bool enable) {
 }
 
 int factorize(aphi_factor* f, const double* values, int equil_iters, double pivot_floor,
-              aphi_factor_stats* stats_out, cudaStream_t st) {
+              aphi_factor_stats* stats_out, cudaStream_t st, const double* panels) {
     const aphi_analysis* A = f->an;
     const Symbolic& S = A->S;
     const int n = S.n;
     const int B = f->batch;
-    if (!values) throw Error(APHI_ERR_INVALID, "factorize: null values");
+    if (!values && !panels) throw Error(APHI_ERR_INVALID, "factorize: null values");
+    if (panels && equil_iters != 0) throw Error(APHI_ERR_BAD_SHAPE, "factorize: dense fronts are not equilibrated");
+    if (!panels && A->fronts) throw Error(APHI_ERR_INVALID, "factorize: a fronts analysis takes panels, not values");
     if (equil_iters < 0) throw Error(APHI_ERR_BAD_SHAPE, "factorize: negative equilibration iterations");
     const auto t0 = std::chrono::steady_clock::now();
     cudaEvent_t e0, e1;
@@ -486,9 +531,9 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
         f->CB = an->ws;
     }
     if (f->precision == 64)
-        factorize_numeric<double>(f, values, st);
+        factorize_numeric<double>(f, values, panels, st);
     else
-        factorize_numeric<float>(f, values, st);
+        factorize_numeric<float>(f, values, panels, st);
     APHI_CUDA(cudaEventRecord(e1, st));
 
     // Stats, computed as the reference computes them: walk the pivots in its
@@ -578,6 +623,7 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
 
 void solve(aphi_factor* f, int nrhs, const double* b, double* x, cudaStream_t st) {
     if (!f->factored) throw Error(APHI_ERR_INVALID, "solve: the factor holds no factorization");
+    if (f->an->fronts) throw Error(APHI_ERR_INVALID, "solve: dense fronts have no system to solve");
     if (nrhs < 1) throw Error(APHI_ERR_BAD_SHAPE, "solve: nrhs must be at least 1");
     for (int k = 0; k < f->batch; ++k)
         if (!f->host_stats[k].ok)

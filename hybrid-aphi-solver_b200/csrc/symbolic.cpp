@@ -376,4 +376,59 @@ Symbolic analyze_supernodal(int n, const int* row_ptr, const int* col_idx, const
     return S;
 }
 
+Symbolic fronts_symbolic(int count, const int* rows, const int* widths) {
+    if (count < 1 || !rows || !widths) throw Error(APHI_ERR_BAD_SHAPE, "fronts: need at least one front");
+    Symbolic S;
+    S.ns = count;
+    S.sn_first.assign(count + 1, 0);
+    for (int s = 0; s < count; ++s) {
+        if (widths[s] < 1 || rows[s] < widths[s])
+            throw Error(APHI_ERR_BAD_SHAPE, "fronts: each front needs 1 <= width <= rows");
+        S.sn_first[s + 1] = S.sn_first[s] + widths[s];
+    }
+    const int n = S.sn_first[count];
+    S.n = n;
+    S.nnz_a = 0;
+    S.perm.resize(n);
+    for (int j = 0; j < n; ++j) S.perm[j] = j;
+    S.post_of_ref = S.ref_of_post = S.new_of_orig = S.orig_of_new = S.perm;
+    S.ref_parent.assign(n, -1);
+    S.ref_colcount.assign(n, 1);
+    S.col_snode.assign(n, 0);
+    S.sn_rows.assign(rows, rows + count);
+    S.sn_parent.assign(count, -1);
+    S.sn_level.assign(count, 0);
+    S.sn_struct_off.assign(count + 1, 0);
+    S.sn_loff.assign(count + 1, 0);
+    for (int s = 0; s < count; ++s) {
+        const int w = widths[s], m = rows[s], f = S.sn_first[s];
+        S.sn_struct_off[s + 1] = S.sn_struct_off[s] + m;
+        // Rows past the pivots belong to no column of this system; they are
+        // never used as indices by the factorization.
+        for (int i = 0; i < m; ++i) S.structs.push_back(i < w ? f + i : 0);
+        S.sn_loff[s + 1] = S.sn_loff[s] + (static_cast<long long>(m) * w + 31) / 32 * 32;
+        for (int j = 0; j < w; ++j) {
+            S.col_snode[f + j] = s;
+            // one column of a front: m - j - 1 entries below its diagonal
+            S.ref_colcount[f + j] = m - j;
+            const double c = m - j - 1;
+            S.flops += 8.0 * c * (c + 1) / 2;
+            S.nnz_l += m - j;
+            if (j + 1 < w) S.ref_parent[f + j] = f + j + 1;
+        }
+        S.max_rows = std::max(S.max_rows, m);
+        S.max_width = std::max(S.max_width, w);
+    }
+    S.stored = S.sn_loff[count];
+    S.num_roots = count;
+    S.child_ptr.assign(count + 1, 0);
+    S.rel_off.assign(count + 1, 0);
+    S.num_levels = 1;
+    S.level_ptr = {0, count};
+    S.level_list.resize(count);
+    for (int s = 0; s < count; ++s) S.level_list[s] = s;
+    S.cb_pool = place_blocks(S, S.sn_cboff);
+    return S;
+}
+
 }  // namespace aphi_b200

@@ -69,6 +69,12 @@ struct Symbolic {
     int max_rows = 0, max_width = 0, num_roots = 0;
 };
 
+// Independent dense fronts (no tree): front s has rows[s] rows, of which the
+// first widths[s] are its pivot columns. Its contribution block starts at zero
+// and is left in the pool (the multifrontal update of the front, without a
+// parent to add it to): the shape of the supernode-update microbenchmark.
+Symbolic fronts_symbolic(int count, const int* rows, const int* widths);
+
 // perm may be null (identity). parent/col_count, when non-null, are checked.
 Symbolic analyze_supernodal(int n, const int* row_ptr, const int* col_idx, const int* perm,
                             const int* parent, const int* col_count, const aphi_analysis_options& opt);

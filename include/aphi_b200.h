@@ -299,6 +299,27 @@ int aphi_residuals_host(const aphi_analysis* an, int batch, int nrhs, const doub
 int aphi_solve_symmetric_host(const aphi_analysis* an, const double* values, const double* b,
                               int equil_iters, double pivot_floor, double* x, double* report);
 
+/* ---- Dense fronts (the supernode-update microbenchmark) -----------------
+ * A schedule of `count` independent dense fronts: front s has rows[s] rows,
+ * of which the first widths[s] are pivot columns. A factor made from it
+ * (aphi_factor_create) factorizes the fronts' panels -- diagonal blocks,
+ * panel rows, and the Schur update of the trailing block -- with the same
+ * kernels and plans as a sparse factorization. The trailing block (the
+ * contribution block) starts at zero, as in the multifrontal method, and ends
+ * as -L21 D L21^T.
+ *   panels_dev: batch x stored complex128, front s's panel at panel_offset[s]
+ *     (column-major, rows[s] x widths[s], leading dimension rows[s]; only
+ *     entries on or below the diagonal are read).
+ *   aphi_fronts_read: entry k's factored panels (D on the diagonal, L below)
+ *     and contribution blocks (front s's (rows - widths)^2 block, column-major,
+ *     lower triangle, at cb_offset[s]), widened to complex128, into device
+ *     buffers of stored and cb_pool entries (analysis info[3], info[9]). */
+int aphi_fronts_create(int count, const int* rows, const int* widths, const aphi_analysis_options* opt,
+                       aphi_analysis** out);
+int aphi_fronts_layout(const aphi_analysis* a, int64_t* panel_offset, int64_t* cb_offset);
+int aphi_factorize_fronts(aphi_factor* f, const double* panels_dev, aphi_factor_stats* stats, void* stream);
+int aphi_fronts_read(const aphi_factor* f, int k, double* panels_dev, double* cb_dev, void* stream);
+
 /* ---- Diagnostics ---------------------------------------------------------
  * Launch plans of an analysis: plan 0 the FP64 / SIMT factorization, 1 the
  * FP32 tensor-core factorization, 2 the forward solve, 3 the backward solve.
