@@ -6,27 +6,34 @@
 // complex product is four real products,
 //     Cr += Ar Br^T - Ai Bi^T        Ci += Ar Bi^T + Ai Br^T,
 // the minus sign carried by the instruction's A-negate bit. Each real operand
-// is split three ways into TF32 numbers, x = hi + mid + lo (exactly), and the
-// six significant cross products are kept,
+// is split exactly into three TF32 numbers, x = hi + mid + lo, and the six
+// significant cross products are kept,
 //     a b ~ hh + (hm + mh + hl + lh + mm),
 // so every product is more accurate than an FP32 multiply (the dropped terms
-// are below 2^-32 relative). The tensor core's FP32 accumulation does not
-// round to nearest, and its error grows with the number of MMAs chained into
-// one accumulator, so the hh products and the small correction terms go to
-// separate TMEM accumulators (Cr, Ci main; Cr, Ci corrections: 4 x 64
-// columns), summed with a rounded FP32 add in the epilogue: 2 MMAs per 8
-// columns of K reach the main accumulator instead of 12.
+// are below 2^-32 relative): 24 tcgen05.mma (kind::tf32, M = 128, N = 64,
+// K = 8) per 8 columns of K.
 //
-// Pipeline: K advances 8 columns per stage, 3 shared-memory stages. All 128
-// threads load the next stage's operands into registers (coalesced column
-// reads of the column-major panel) while earlier stages' MMAs run, split them
-// and store them in the canonical K-major no-swizzle layout (8-row x 16-byte
-// core matrices: LBO = 128 B between the two K-adjacent cores, SBO = 256 B
-// between 8-row groups), 16 bytes per store. Thread 0 issues the stage's 24
-// tcgen05.mma (kind::tf32, M = 128, N = 64, K = 8) and commits them to the
-// stage's mbarrier; a stage is rewritten once that barrier shows its MMAs
-// done. Every wait is bounded: on expiry the CTA stops issuing, waits (again
-// bounded) for what it issued, frees its TMEM and reports failure.
+// Accumulation. The tensor core's FP32 accumulation truncates instead of
+// rounding to nearest, and the error of a long chain of MMAs into one
+// accumulator is biased. So the hh products of each group of kTcGroup stages
+// go to a fresh TMEM accumulator (Cr, Ci main: 2 x 64 columns), which the
+// threads then read and add to a running sum in registers with rounded FP32
+// adds (thread r holds row r: 64 complex); no truncating chain is longer
+// than 2 kTcGroup MMAs. The correction terms, 2^-11 of the main ones and
+// below, accumulate over the whole K in their own TMEM accumulator (Cr, Ci:
+// 2 x 64 columns), where their truncation is negligible.
+//
+// Pipeline: K advances 8 columns per stage. Raw operands (A rows, B rows and
+// the stage's pivots, complex64) are fetched by cp.async into a ring of
+// kTcRawStages buffers, two stages ahead, so no registers hold them in
+// flight. Each stage, the threads split the raw stage into the canonical
+// K-major no-swizzle layout (8-row x 16-byte core matrices: LBO = 128 B
+// between the two K-adjacent cores, SBO = 256 B between 8-row groups; 16-byte
+// stores) in one of kTcPlaneStages plane buffers; thread 0 issues the stage's
+// 24 MMAs and commits them to the buffer's mbarrier, which the threads wait
+// on before rewriting it. Every wait is bounded: on expiry the CTA stops
+// issuing, waits (again bounded) for what it issued, frees its TMEM and
+// reports failure.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -109,6 +116,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
         : "r"(taddr));
 }
 
+// 8-byte global -> shared copy without a register round trip; bytes < 8
+// (here 0) fills the rest of the destination with zeros.
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Four values -> hi, mid, lo (each exactly a TF32 number, hi + mid + lo == v)
 // stored as one 16-byte row of a core matrix in each of three planes.
 __device__ __forceinline__ void split_store4(unsigned char* plane0, int plane_bytes, uint32_t off, const float (&v)[4]) {
@@ -130,39 +148,44 @@ __device__ __forceinline__ void split_store4(unsigned char* plane0, int plane_by
     *reinterpret_cast<float4*>(plane0 + 2 * plane_bytes + off) = l;
 }
 
-// Operands of one stage held in registers between load and store: A row tid
-// (8 columns of K, scaled later by d), B row tid % 64 (4 columns: the half of
-// the stage selected by tid / 64), and the stage's 8 pivots.
-struct TcRegs {
-    float2 a[kTcK];
-    float2 b[4];
-    float2 d[kTcK];
-};
-
-__device__ __forceinline__ void tc_load(TcRegs& R, const float2* P, long long ldp, int rows, int K, int i0, int j0,
-                                        const float2* dk, long long dstride, int kbase) {
+// Raw stage: A rows [k][128], B rows [k][64], pivots [k] (complex64). Thread
+// tid fetches A row tid for the 8 columns, B row tid % 64 for columns
+// 4 (tid / 64) .. +3, and (tid < 8) pivot tid; entries past the panel or the
+// front read as zero.
+__device__ __forceinline__ void tc_fetch(unsigned char* raw, const float2* P, long long ldp, int rows, int K,
+                                         int i0, int j0, const float2* dk, long long dstride, int kbase) {
     const int tid = threadIdx.x;
-    const int rb = tid & (kTcN - 1), qb = tid >> 6;
+    const uint32_t ra = smem_u32(raw), rb = ra + kTcRawA, rd = rb + kTcRawB;
 #pragma unroll
     for (int k = 0; k < kTcK; ++k) {
         const int kk = kbase + k;
-        R.a[k] = make_float2(0.f, 0.f);
-        R.d[k] = make_float2(0.f, 0.f);
-        if (kk < K) {
-            if (i0 + tid < rows) R.a[k] = P[static_cast<long long>(kk) * ldp + i0 + tid];
-            R.d[k] = dk ? dk[static_cast<long long>(kk) * dstride] : make_float2(1.f, 0.f);
-        }
+        const bool in = kk < K && i0 + tid < rows;
+        cp_async8(ra + (k * kTcM + tid) * 8, in ? P + static_cast<long long>(kk) * ldp + i0 + tid : P, in ? 8u : 0u);
     }
+    const int rowb = tid & (kTcN - 1), qb = tid >> 6;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        const int kk = kbase + qb * 4 + q;
-        R.b[q] = make_float2(0.f, 0.f);
-        if (kk < K && j0 + rb < rows) R.b[q] = P[static_cast<long long>(kk) * ldp + j0 + rb];
+        const int k = qb * 4 + q, kk = kbase + k;
+        const bool in = kk < K && j0 + rowb < rows;
+        cp_async8(rb + (k * kTcN + rowb) * 8, in ? P + static_cast<long long>(kk) * ldp + j0 + rowb : P,
+                  in ? 8u : 0u);
+    }
+    if (tid < kTcK) {
+        const int kk = kbase + tid;
+        if (dk) {
+            cp_async8(rd + tid * 8, kk < K ? dk + static_cast<long long>(kk) * dstride : dk, kk < K ? 8u : 0u);
+        } else {
+            *reinterpret_cast<float2*>(raw + kTcRawA + kTcRawB + tid * 8) = make_float2(kk < K ? 1.f : 0.f, 0.f);
+        }
     }
 }
 
-__device__ __forceinline__ void tc_store(const TcRegs& R, unsigned char* stage) {
+// Raw stage -> split planes (A scaled by the pivots).
+__device__ __forceinline__ void tc_split(const unsigned char* raw, unsigned char* stage) {
     const int tid = threadIdx.x;
+    const float2* rA = reinterpret_cast<const float2*>(raw);
+    const float2* rB = reinterpret_cast<const float2*>(raw + kTcRawA);
+    const float2* rD = reinterpret_cast<const float2*>(raw + kTcRawA + kTcRawB);
     unsigned char* A = stage;                                   // Ar hi/mid/lo, Ai hi/mid/lo
     unsigned char* B = stage + 2 * kTcSplit * kTcPlaneA;        // Br hi/mid/lo, Bi hi/mid/lo
 #pragma unroll
@@ -170,7 +193,7 @@ __device__ __forceinline__ void tc_store(const TcRegs& R, unsigned char* stage) 
         float re[4], im[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const float2 v = R.a[4 * g + q], d = R.d[4 * g + q];
+            const float2 v = rA[(4 * g + q) * kTcM + tid], d = rD[4 * g + q];
             re[q] = v.x * d.x - v.y * d.y;
             im[q] = v.x * d.y + v.y * d.x;
         }
@@ -178,22 +201,24 @@ __device__ __forceinline__ void tc_store(const TcRegs& R, unsigned char* stage) 
         split_store4(A, kTcPlaneA, o, re);
         split_store4(A + kTcSplit * kTcPlaneA, kTcPlaneA, o, im);
     }
-    const int rb = tid & (kTcN - 1), qb = tid >> 6;
+    const int rowb = tid & (kTcN - 1), qb = tid >> 6;
     float re[4], im[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        re[q] = R.b[q].x;
-        im[q] = R.b[q].y;
+        const float2 v = rB[(qb * 4 + q) * kTcN + rowb];
+        re[q] = v.x;
+        im[q] = v.y;
     }
-    const uint32_t o = plane_off(rb, 4 * qb);
+    const uint32_t o = plane_off(rowb, 4 * qb);
     split_store4(B, kTcPlaneB, o, re);
     split_store4(B + kTcSplit * kTcPlaneB, kTcPlaneB, o, im);
 }
 
 // The 24 MMAs of one stage: for each kept split pair (pa, pb), the four real
-// products into Cr, Ci; pair 0 (hi, hi) into the main accumulators, the rest
-// into the correction accumulators.
-__device__ __forceinline__ void tc_issue(uint32_t stage_addr, uint32_t tmem, bool first) {
+// products into Cr, Ci; pair 0 (hi, hi) into the main accumulators (restarted
+// when fresh_main), the rest into the correction accumulators (restarted when
+// fresh_corr).
+__device__ __forceinline__ void tc_issue(uint32_t stage_addr, uint32_t tmem, bool fresh_main, bool fresh_corr) {
     const uint32_t A0 = stage_addr, B0 = stage_addr + 2 * kTcSplit * kTcPlaneA;
     const uint32_t id_pos = instr_desc(0), id_neg = instr_desc(1);
     const int pa[6] = {0, 0, 1, 0, 2, 1}, pb[6] = {0, 1, 0, 2, 0, 1};
@@ -205,11 +230,30 @@ __device__ __forceinline__ void tc_issue(uint32_t stage_addr, uint32_t tmem, boo
         const uint64_t bi = smem_desc(B0 + (kTcSplit + pb[t]) * kTcPlaneB);
         const uint32_t d_re = tmem + (t == 0 ? 0 : 2 * kTcN);
         const uint32_t d_im = d_re + kTcN;
-        const uint32_t acc = (first && (t == 0 || t == 1)) ? 0u : 1u;
+        const bool fresh = t == 0 ? fresh_main : (t == 1 && fresh_corr);
+        const uint32_t acc = fresh ? 0u : 1u;
         mma_tf32(d_re, ar, br, id_pos, acc);   // Cr += Ar Br^T
         mma_tf32(d_re, ai, bi, id_neg, 1);     // Cr -= Ai Bi^T
         mma_tf32(d_im, ar, bi, id_pos, acc);   // Ci += Ar Bi^T
         mma_tf32(d_im, ai, br, id_pos, 1);     // Ci += Ai Br^T
+    }
+}
+
+// Adds the main accumulators (this warp's 32 lanes, 64 columns) to the
+// running sums, rounding to nearest.
+__device__ __forceinline__ void tc_drain(uint32_t tmem, float (&sr)[kTcN], float (&si)[kTcN]) {
+    const uint32_t lane_base = static_cast<uint32_t>((threadIdx.x >> 5) * 32) << 16;
+#pragma unroll
+    for (int c0 = 0; c0 < kTcN; c0 += 16) {
+        uint32_t vr[16], vi[16];
+        tmem_ld16(tmem + lane_base + c0, vr);
+        tmem_ld16(tmem + lane_base + kTcN + c0, vi);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+            sr[c0 + c] += __uint_as_float(vr[c]);
+            si[c0 + c] += __uint_as_float(vi[c]);
+        }
     }
 }
 
@@ -218,16 +262,18 @@ __device__ __forceinline__ void tc_issue(uint32_t stage_addr, uint32_t tmem, boo
 // (the front's pivots; all ones when dk is null). Rows at or beyond `rows`
 // read as zero. The result is handed to `store(r, c0, re[16], im[16])`, 16
 // consecutive columns c0.. of row r at a time, by the thread that owns row r
-// (warp r / 32, lane r % 32).
-// Requires kTcSmem bytes of dynamic shared memory (16-byte aligned). Returns
-// false if a bounded wait expired (the caller records the error).
+// (warp r / 32, lane r % 32). Requires kTcSmem bytes of dynamic shared
+// memory (16-byte aligned). Returns false if a bounded wait expired (the
+// caller records the error).
 template <class Store>
 __device__ bool tc_tile(unsigned char* smem, const float2* P, long long ldp, int rows, int K, int i0, int j0,
                         const float2* dk, long long dstride, Store store) {
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kTcStages * kTcStage);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + kTcStages);
+    unsigned char* planes = smem;
+    unsigned char* raws = smem + kTcPlaneStages * kTcStage;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(raws + kTcRawStages * kTcRawStage);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + kTcPlaneStages);
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -235,60 +281,85 @@ __device__ bool tc_tile(unsigned char* smem, const float2* P, long long ldp, int
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        for (int s = 0; s < kTcStages; ++s) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + s)));
+        for (int s = 0; s < kTcPlaneStages; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + s)));
         asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    const int nst = (K + kTcK - 1) / kTcK;
+    // Two raw stages in flight before the loop.
+    for (int c = 0; c < 2; ++c) {
+        if (c < nst) tc_fetch(raws + c * kTcRawStage, P, ldp, rows, K, i0, j0, dk, dstride, c * kTcK);
+        cp_async_commit();
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = *tmem_slot;
 
-    const int nst = (K + kTcK - 1) / kTcK;
+    float sr[kTcN], si[kTcN];
+#pragma unroll
+    for (int c = 0; c < kTcN; ++c) sr[c] = si[c] = 0.f;
     bool ok = true;
     int issued = 0;  // stages whose MMAs were issued and committed
-    TcRegs cur, nxt;
-    tc_load(cur, P, ldp, rows, K, i0, j0, dk, dstride, 0);
     for (int c = 0; c < nst; ++c) {
-        const int s = c % kTcStages;
-        if (c + 1 < nst) tc_load(nxt, P, ldp, rows, K, i0, j0, dk, dstride, (c + 1) * kTcK);
-        // The stage's previous MMAs (stage c - 3) must be done before it is rewritten.
+        const int buf = c % kTcPlaneStages;
+        if (c + 2 < nst)
+            tc_fetch(raws + ((c + 2) % kTcRawStages) * kTcRawStage, P, ldp, rows, K, i0, j0, dk, dstride,
+                     (c + 2) * kTcK);
+        cp_async_commit();
+        cp_async_wait<2>();  // this thread's copies of stage c have landed
         bool mine = true;
-        if (c >= kTcStages) mine = mbar_wait(smem_u32(mbar + s), ((c - kTcStages) / kTcStages) & 1);
-        if (mine) tc_store(cur, smem + s * kTcStage);
+        // The plane buffer's previous MMAs (stage c - 2) must be done.
+        if (c >= kTcPlaneStages)
+            mine = mbar_wait(smem_u32(mbar + buf), ((c - kTcPlaneStages) / kTcPlaneStages) & 1);
+        ok = __syncthreads_and(mine) != 0;  // also: every thread's raw copies of stage c are visible
+        if (!ok) break;
+        tc_split(raws + (c % kTcRawStages) * kTcRawStage, planes + buf * kTcStage);
+        // Generic-proxy stores -> visible to the tensor core's async proxy.
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        // A new group starts: the previous group's main products, complete
+        // once stage c - 1's commit has arrived, go to the running sums
+        // (after the split, so the split overlaps those MMAs).
+        const bool group_start = c % kTcGroup == 0;
+        if (group_start && c > 0) {
+            const int p = c - 1;
+            mine = mbar_wait(smem_u32(mbar + p % kTcPlaneStages), (p / kTcPlaneStages) & 1);
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            if (mine) tc_drain(tmem, sr, si);
+        }
         asm volatile("tcgen05.fence::before_thread_sync;");
         ok = __syncthreads_and(mine) != 0;
         asm volatile("tcgen05.fence::after_thread_sync;");
         if (!ok) break;
         if (tid == 0) {
-            tc_issue(smem_u32(smem + s * kTcStage), tmem, c == 0);
-            mma_commit(smem_u32(mbar + s));
+            tc_issue(smem_u32(planes + buf * kTcStage), tmem, group_start, c == 0);
+            mma_commit(smem_u32(mbar + buf));
         }
         ++issued;
-        cur = nxt;
     }
+    cp_async_wait<0>();
     // Drain: every committed stage not yet waited for, oldest first.
     bool drained = true;
-    for (int c = (issued > kTcStages ? issued - kTcStages : 0); c < issued; ++c)
-        drained = mbar_wait(smem_u32(mbar + c % kTcStages), (c / kTcStages) & 1) && drained;
+    for (int c = (issued > kTcPlaneStages ? issued - kTcPlaneStages : 0); c < issued; ++c)
+        drained = mbar_wait(smem_u32(mbar + c % kTcPlaneStages), (c / kTcPlaneStages) & 1) && drained;
     drained = __syncthreads_and(drained) != 0;
     asm volatile("tcgen05.fence::after_thread_sync;");
     ok = ok && drained;
     if (ok) {
+        tc_drain(tmem, sr, si);  // the last group
         const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
         const int r = warp * 32 + lane;
+#pragma unroll
         for (int c0 = 0; c0 < kTcN; c0 += 16) {
-            uint32_t mr[16], cr[16], mi[16], ci[16];
-            tmem_ld16(tmem + lane_base + c0, mr);
+            uint32_t cr[16], ci[16];
             tmem_ld16(tmem + lane_base + 2 * kTcN + c0, cr);
-            tmem_ld16(tmem + lane_base + kTcN + c0, mi);
             tmem_ld16(tmem + lane_base + 3 * kTcN + c0, ci);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             float re[16], im[16];
 #pragma unroll
             for (int c = 0; c < 16; ++c) {
-                re[c] = __uint_as_float(mr[c]) + __uint_as_float(cr[c]);
-                im[c] = __uint_as_float(mi[c]) + __uint_as_float(ci[c]);
+                re[c] = sr[c0 + c] + __uint_as_float(cr[c]);
+                im[c] = si[c0 + c] + __uint_as_float(ci[c]);
             }
             store(r, c0, re, im);
         }

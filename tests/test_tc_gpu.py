@@ -6,13 +6,15 @@ each entry must be within 1e-5 of the sum of magnitudes |P d||P| -- the
 accuracy of an FP32 dot product of that length -- against the same product
 in FP64 on the host.
 
-The tensor core's FP32 accumulation truncates instead of rounding to nearest,
-so a tile's error has a bias (measured: -6e-7 relative at K = 128 for
-all-positive products, none for a rounded FP32 sum) that accumulates over the
-panels of a large front. The factorization built on it is therefore up to
-~11x less accurate than the SIMT FP32 factorization (measured 4.9x on the
-10^3 and 11x on the 14^3 cylinder, after the main products were given their
-own accumulator); the test bounds the ratio at 15 and requires the refined
+The tensor core's FP32 accumulation truncates instead of rounding to nearest.
+The tile therefore gives the hi*hi products a fresh accumulator every 16
+columns of K and sums those partial results in registers, rounding to
+nearest; that brings the bias of a K = 128 all-positive product down to
+-5e-8 relative (from -1.2e-6 with one chained accumulator). What remains
+comes from the alignment of the products inside each MMA. The factorization
+built on the tile is measured at 2.3-4.7x the forward error of the SIMT
+FP32 factorization on the 10^3 and 14^3 cylinders (16x at 50 Hz on 20^3);
+the test bounds the ratio at 8 on 10^3 and 14^3 and requires the refined
 solve to reach relative residual 1e-13 with it as the preconditioner."""
 import os
 
@@ -93,7 +95,7 @@ def test_tc_factor_as_accurate_as_simt(cells, cuda):
     for k in range(2):
         e_simt = (torch.linalg.norm(xs[k] - x64[k]) / torch.linalg.norm(x64[k])).item()
         e_tc = (torch.linalg.norm(xt[k] - x64[k]) / torch.linalg.norm(x64[k])).item()
-        assert e_tc <= 15.0 * e_simt + 1e-6, (k, e_tc, e_simt)
+        assert e_tc <= 8.0 * e_simt + 1e-6, (k, e_tc, e_simt)
     x, iters, berr, ok = ftc.solve_refined(vals, rhs, tol=1e-16, rtol=1e-13, max_iters=40, krylov=True)
     res = ab.residuals(an, vals, x, rhs)
     assert ok and (res[:, 0, 0] <= 1e-13).all(), (iters, res)
