@@ -1,11 +1,14 @@
 """The drop-in boundary, exercised by the reference's own tests.
 
 oracle/Makefile (`make -C oracle dropin`) builds the reference's
-tests/test_factorization.cpp, tests/test_equilibration.cpp and
-tests/test_symbolic.cpp against its kept sources with src/factorization.cpp
-replaced by hybrid-aphi-solver_b200/dropin/factorization_b200.cpp, which
-defines every function of include/aphi_solver/factorization.hpp over the
-aphi_b200 C ABI. Each program prints "<passed>/<checks> checks passed" and
+tests/test_factorization.cpp, tests/test_equilibration.cpp,
+tests/test_symbolic.cpp and tests/test_assembly.cpp against its kept sources
+with src/factorization.cpp and src/assembly.cpp replaced by
+hybrid-aphi-solver_b200/dropin/factorization_b200.cpp and
+hybrid-aphi-solver_b200/dropin/assembly_b200.cpp, which define every function
+of include/aphi_solver/factorization.hpp and include/aphi_solver/assembly.hpp
+over the aphi_b200 C ABI (the element fill and scatter of refill and the
+factorization, solves and refinement run on the device). Each program prints "<passed>/<checks> checks passed" and
 exits 0 only if every check passed; here they run on the B200."""
 import re
 import subprocess
@@ -19,7 +22,7 @@ ROOT = Path(__file__).resolve().parents[1]
 DROPIN = ROOT / "oracle" / "_ref" / "dropin"
 
 
-@pytest.mark.parametrize("name", ["test_factorization", "test_equilibration", "test_symbolic"])
+@pytest.mark.parametrize("name", ["test_factorization", "test_equilibration", "test_symbolic", "test_assembly"])
 def test_reference_tests_pass_through_the_dropin(name, cuda):
     exe = DROPIN / name
     if not exe.exists():
