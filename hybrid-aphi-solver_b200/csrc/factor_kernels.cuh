@@ -452,12 +452,27 @@ __global__ void __launch_bounds__(256) k_update_wide(Sched S, long long item0, c
 // mma.sync m8n8k4). Same items, tile and K as k_update_wide. 8 warps in a 4 x 2
 // grid, each a 32 x 32 complex block of the tile: 4 x 4 blocks of 8 x 8, each
 // four real products (Cr += Ar Br - Ai Bi, Ci += Ar Bi + Ai Br; the minus by
-// a negated copy of Ai's fragment). Operands are staged as complex pairs
-// (k-major rows, 130 / 66 entries apart so that one quarter-warp's 16-byte
-// fragment loads touch distinct banks), 8 columns of K per double-buffered
-// chunk; a k-step of 4 costs a warp 8 shared loads for 64 DMMA.
+// a negated copy of Ai's fragment).
+//
+// Operands stream global -> shared by cp.async, without a register round
+// trip, through a ring of 3 chunks of 16 panel columns (2 in flight while one
+// is consumed; one barrier a chunk). They are staged as complex pairs, k-major
+// rows 130 / 66 entries apart, so that one quarter-warp's 16-byte fragment
+// loads touch distinct banks. The panel's pivots sit beside the ring and scale
+// the A fragments as they are read (L[i,k] * D[k], the same product, in the
+// same order, as the other trailing updates). A k-step of 4 costs a warp 9
+// shared loads for 64 DMMA.
+//
+// The result is subtracted with red.global.add.f64 (old + (-acc) rounds as
+// old - acc does): every destination entry has exactly one writer in a launch,
+// so the fire-and-forget reduction leaves the same bits as a read-modify-write
+// and, like it, costs the destination's traffic once after the last MMA.
+constexpr int kDmmaKC = 16, kDmmaStages = 3;
 constexpr int kDmmaLdA = kWideM + 2, kDmmaLdB = kWideN + 2;
-constexpr int kDmmaSmem = 2 * kWideKC * (kDmmaLdA + kDmmaLdB) * 16;
+constexpr int kDmmaStage = kDmmaKC * (kDmmaLdA + kDmmaLdB);  // complex entries
+constexpr int kDmmaSmem = (kTcPanel + kDmmaStages * kDmmaStage) * 16;
+static_assert(kDmmaSmem <= 227 * 1024, "DMMA ring exceeds shared memory");
+static_assert(kTcPanel % kDmmaKC == 0 && kDmmaKC % 4 == 0, "chunks must tile the panel in k-steps of 4");
 
 __device__ __forceinline__ void dmma884(double (&c)[2], double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
@@ -465,11 +480,20 @@ __device__ __forceinline__ void dmma884(double (&c)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
+// 16-byte global -> shared copy; bytes = 0 fills the destination with zeros.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void red_sub(double* p, double v) {
+    asm volatile("red.global.add.f64 [%0], %1;" ::"l"(p), "d"(-v) : "memory");
+}
+
 __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long item0, cx<double>* Lb,
                                                           cx<double>* CBb, long long lstride, long long cbstride) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cx<double>* As = reinterpret_cast<cx<double>*>(smem_raw);   // [2][KC][kDmmaLdA], scaled by D
-    cx<double>* Bs = As + 2 * kWideKC * kDmmaLdA;                // [2][KC][kDmmaLdB]
+    cx<double>* Ds = reinterpret_cast<cx<double>*>(smem_raw);  // [kTcPanel] pivots of the panel
+    cx<double>* Ring = Ds + kTcPanel;                            // [stage][A: KC x ldA | B: KC x ldB]
     const Item it = S.items[item0 + blockIdx.x];
     const int s = it.s, p0 = it.a, i0 = it.b, j0 = it.c;
     cx<double>* L = Lb + lstride * blockIdx.y;
@@ -483,34 +507,26 @@ __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long ite
     const cx<double>* P = Ls + static_cast<long long>(p0) * m;
     const cx<double>* dg = Ls + p0 + static_cast<long long>(p0) * m;
     const int tid = threadIdx.x;
-    // Raw values stay in registers until the stash, so the loads' latency is
-    // covered by the chunk being computed.
-    cx<double> pa[4], pd[4], pb[2];
-    auto load = [&](int kbase) {
+    const uint32_t ring = smem_u32(Ring);
+    // Chunk c: panel columns 16c.. of rows i0.. (A, 128 rows) and j0.. (B, 64).
+    auto fetch = [&](int c) {
+        const int kbase = c * kDmmaKC;
+        const uint32_t sa = ring + (c % kDmmaStages) * kDmmaStage * 16;
+        const uint32_t sb = sa + kDmmaKC * kDmmaLdA * 16;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int k = kbase + (tid >> 7) + 2 * q, r = tid & 127;
-            pa[q] = cx<double>{0, 0};
-            pd[q] = cx<double>{0, 0};
-            if (k < K && i0 + r < m) {
-                pa[q] = P[static_cast<long long>(k) * m + i0 + r];
-                pd[q] = dg[static_cast<long long>(k) * (m + 1)];
-            }
+        for (int q = 0; q < kDmmaKC * kWideM / 256; ++q) {
+            const int e = tid + 256 * q, k = e / kWideM, r = e % kWideM;
+            const bool in = kbase + k < K && i0 + r < m;
+            cp_async16(sa + (k * kDmmaLdA + r) * 16, in ? P + static_cast<long long>(kbase + k) * m + i0 + r : P,
+                       in ? 16u : 0u);
         }
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int k = kbase + (tid >> 6) + 4 * q, r = tid & 63;
-            pb[q] = cx<double>{0, 0};
-            if (k < K && j0 + r < m) pb[q] = P[static_cast<long long>(k) * m + j0 + r];
+        for (int q = 0; q < kDmmaKC * kWideN / 256; ++q) {
+            const int e = tid + 256 * q, k = e / kWideN, r = e % kWideN;
+            const bool in = kbase + k < K && j0 + r < m;
+            cp_async16(sb + (k * kDmmaLdB + r) * 16, in ? P + static_cast<long long>(kbase + k) * m + j0 + r : P,
+                       in ? 16u : 0u);
         }
-    };
-    auto stash = [&](int buf) {
-        cx<double>* A = As + buf * kWideKC * kDmmaLdA;
-        cx<double>* B = Bs + buf * kWideKC * kDmmaLdB;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) A[((tid >> 7) + 2 * q) * kDmmaLdA + (tid & 127)] = pa[q] * pd[q];
-#pragma unroll
-        for (int q = 0; q < 2; ++q) B[((tid >> 6) + 4 * q) * kDmmaLdB + (tid & 63)] = pb[q];
     };
     const int warp = tid >> 5, lane = tid & 31;
     const int wm = warp & 3, wn = warp >> 2;
@@ -520,19 +536,25 @@ __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long ite
     for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) cr[a][b][0] = cr[a][b][1] = ci[a][b][0] = ci[a][b][1] = 0.0;
-    const int nc = (K + kWideKC - 1) / kWideKC;
-    load(0);
-    stash(0);
-    __syncthreads();
+    const int nc = (K + kDmmaKC - 1) / kDmmaKC;
+    fetch(0);
+    cp_async_commit();
+    if (nc > 1) fetch(1);
+    cp_async_commit();
+    if (tid < kTcPanel) Ds[tid] = tid < K ? dg[static_cast<long long>(tid) * (m + 1)] : cx<double>{0, 0};
     for (int c = 0; c < nc; ++c) {
-        if (c + 1 < nc) load((c + 1) * kWideKC);
-        const cx<double>* A = As + (c & 1) * kWideKC * kDmmaLdA;
-        const cx<double>* B = Bs + (c & 1) * kWideKC * kDmmaLdB;
+        cp_async_wait<1>();  // this thread's copies of chunk c have landed
+        __syncthreads();     // everyone's have; everyone is done with chunk c - 1
+        if (c + 2 < nc) fetch(c + 2);
+        cp_async_commit();
+        const cx<double>* A = Ring + (c % kDmmaStages) * kDmmaStage;
+        const cx<double>* B = A + kDmmaKC * kDmmaLdA;
 #pragma unroll
-        for (int ks = 0; ks < kWideKC; ks += 4) {
+        for (int ks = 0; ks < kDmmaKC; ks += 4) {
+            const cx<double> d = Ds[c * kDmmaKC + ks + t4];
             cx<double> af[4], bf[4];
 #pragma unroll
-            for (int a = 0; a < 4; ++a) af[a] = A[(ks + t4) * kDmmaLdA + 32 * wm + 8 * a + g];
+            for (int a = 0; a < 4; ++a) af[a] = A[(ks + t4) * kDmmaLdA + 32 * wm + 8 * a + g] * d;
 #pragma unroll
             for (int b = 0; b < 4; ++b) bf[b] = B[(ks + t4) * kDmmaLdB + 32 * wn + 8 * b + g];
             // One real product over all 16 blocks before the next, so that
@@ -554,28 +576,22 @@ __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long ite
 #pragma unroll
                 for (int b = 0; b < 4; ++b) dmma884(ci[a][b], af[a].im, bf[b].re);
         }
-        if (c + 1 < nc) stash((c + 1) & 1);
-        __syncthreads();
     }
     // Thread holds C[g][2 t4 + e] of each 8 x 8 block: rows i0 + 32 wm + 8a + g,
-    // columns j0 + 32 wn + 8b + 2 t4 + e. Read-modify-write per block row.
+    // columns j0 + 32 wn + 8b + 2 t4 + e.
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
         const int i = i0 + 32 * wm + 8 * a + g;
-        cx<double>* dst[8];
-        cx<double> old[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const int j = j0 + 32 * wn + 8 * (q >> 1) + 2 * t4 + (q & 1);
-            dst[q] = nullptr;
-            if (j < m && i < m && i >= j)
-                dst[q] = (j < w) ? Ls + i + static_cast<long long>(j) * m
-                                 : CBs + (i - w) + static_cast<long long>(j - w) * cs;
-            if (dst[q]) old[q] = *dst[q];
+            if (j < m && i < m && i >= j) {
+                cx<double>* dst = (j < w) ? Ls + i + static_cast<long long>(j) * m
+                                          : CBs + (i - w) + static_cast<long long>(j - w) * cs;
+                red_sub(&dst->re, cr[a][q >> 1][q & 1]);
+                red_sub(&dst->im, ci[a][q >> 1][q & 1]);
+            }
         }
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-            if (dst[q]) *dst[q] = cx<double>{old[q].re - cr[a][q >> 1][q & 1], old[q].im - ci[a][q >> 1][q & 1]};
     }
 }
 
