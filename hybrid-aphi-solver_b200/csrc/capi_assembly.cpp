@@ -74,6 +74,20 @@ int aphi_workload_cylinder(int cells, double v_top, int full_wave, aphi_workload
     });
 }
 
+int aphi_workload_torus(int cells, double current, aphi_workload** out) {
+    return guard([&] {
+        if (!out) throw Error(APHI_ERR_INVALID, "aphi_workload_torus: null output");
+        auto* w = new aphi_workload;
+        try {
+            build_torus(w->w, cells, current);
+        } catch (...) {
+            delete w;
+            throw;
+        }
+        *out = w;
+    });
+}
+
 void aphi_workload_free(aphi_workload* w) { delete w; }
 
 int aphi_workload_sizes(const aphi_workload* h, int64_t* s) {

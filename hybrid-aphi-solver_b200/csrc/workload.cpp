@@ -243,82 +243,30 @@ void gauge_tree(Workload& w) {
         }
 }
 
-}  // namespace
-
-void build_cylinder(Workload& w, int n, double v_top, int full_wave) {
-    if (n < 1) throw std::invalid_argument("build_cylinder: need at least one cell per side");
-    w = Workload{};
-    build_mesh(w, n);
+// The unknowns, per-tet tables, positions and pattern, once the bodies, the
+// gauge and the ports are known (src/dof_map.cpp:8-194, src/sparsity.cpp:19-136).
+//   phi_port   P2 node -> the port claiming it (later ports win), -1 if none
+//   port_cut   per port: 1 for an internal cut (two-sided), 0 for a terminal
+//   tet_side   per tet: +1 on a cut's plus side, -1 on its minus side, 0 when
+//              it touches no cut (empty when there are no cuts)
+//   pinned     P2 nodes fixed at 0 V (floating conductors), unless a port claims them
+//   port_xyz   3 per port: where its unknown sits for a geometric ordering
+void finish(Workload& w, std::vector<int>& phi_port, const std::vector<uint8_t>& port_cut,
+            const std::vector<int8_t>& tet_side, const std::vector<uint8_t>& pinned, int full_wave,
+            const std::vector<double>& port_xyz) {
     const size_t nt = static_cast<size_t>(w.num_tets);
-
-    // Bodies: 0 = wire (sigma 5.8e7), 1 = air, by tet centroid distance to the axis.
-    w.material = {5.8e7, 1.0, 1.0, 0.0, 1.0, 1.0};
-    w.body_of_tet.assign(nt, 1);
-    for (size_t t = 0; t < nt; ++t) {
-        double cx = 0, cy = 0;
-        for (int q = 0; q < 4; ++q) {
-            cx += w.xyz[3 * w.tets[4 * t + q]];
-            cy += w.xyz[3 * w.tets[4 * t + q] + 1];
-        }
-        // The same arithmetic order as a centroid summed vertex by vertex then scaled.
-        cx *= 0.25;
-        cy *= 0.25;
-        if (std::hypot(cx - 0.5, cy - 0.5) < 0.2) w.body_of_tet[t] = 0;
-    }
-    w.body_ptr.assign(3, 0);
-    for (size_t t = 0; t < nt; ++t) ++w.body_ptr[w.body_of_tet[t] + 1];
-    if (w.body_ptr[1] == 0)
-        throw std::invalid_argument("build_cylinder: no tet centroid lies inside the conductor at " +
-                                    std::to_string(n) + " cells per side, so its ports have no faces");
-    w.body_ptr[2] += w.body_ptr[1];
-    w.body_tets.resize(nt);
-    {
-        std::vector<int> cur(w.body_ptr.begin(), w.body_ptr.end() - 1);
-        for (size_t t = 0; t < nt; ++t) w.body_tets[cur[w.body_of_tet[t]]++] = static_cast<int>(t);
-    }
-
-    boundary_edges(w);
-    gauge_tree(w);
-
-    // Port terminals: faces of conductor tets with all three nodes on z = 1
-    // (port 0, v_top) or z = 0 (port 1, 0 V).
     const int num_p2 = w.num_nodes + w.num_edges;
-    std::vector<int> phi_port(num_p2, -1);
-    int port_faces[2] = {0, 0};
-    for (size_t t = 0; t < nt; ++t) {
-        if (w.body_of_tet[t] != 0) continue;
-        for (int f = 0; f < 4; ++f) {
-            int v[3];
-            bool z0 = true, z1 = true;
-            for (int q = 0; q < 3; ++q) {
-                v[q] = w.tets[4 * t + kFaceVerts[f][q]];
-                const double z = w.xyz[3 * v[q] + 2];
-                if (z != 0.0) z0 = false;
-                if (z != 1.0) z1 = false;
-            }
-            if (!z0 && !z1) continue;
-            const int port = z1 ? 0 : 1;
-            ++port_faces[port];
-            for (int q = 0; q < 3; ++q) phi_port[v[q]] = port;
-            phi_port[w.num_nodes + find_edge(w, v[0], v[1])] = port;
-            phi_port[w.num_nodes + find_edge(w, v[1], v[2])] = port;
-            phi_port[w.num_nodes + find_edge(w, v[0], v[2])] = port;
-        }
-    }
-
-    if (port_faces[0] == 0 || port_faces[1] == 0)
-        throw std::invalid_argument("build_cylinder: a port surface has no triangles in the mesh at " +
-                                    std::to_string(n) + " cells per side");
 
     // A unknowns: edges neither on n x A = 0 nor in the tree, in edge order.
     w.edge_index.assign(w.num_edges, -1);
     for (int e = 0; e < w.num_edges; ++e)
         if (!w.dirichlet_edge[e] && !w.tree_edge[e]) w.edge_index[e] = w.num_a++;
 
-    // Phi unknowns: P2 nodes touched by a Phi tet, minus port terminals.
+    // Phi unknowns: P2 nodes touched by a Phi tet, minus port terminals, cut
+    // nodes and pinned nodes.
     std::vector<uint8_t> present(num_p2, 0);
     for (size_t t = 0; t < nt; ++t) {
-        if (!full_wave && w.body_of_tet[t] != 0) continue;
+        if (!full_wave && w.material[3 * w.body_of_tet[t]] <= 0.0) continue;
         for (int q = 0; q < 4; ++q) present[w.tets[4 * t + q]] = 1;
         for (int le = 0; le < 6; ++le) present[w.num_nodes + w.tet_edges[6 * t + le]] = 1;
     }
@@ -328,15 +276,13 @@ void build_cylinder(Workload& w, int n, double v_top, int full_wave) {
             phi_port[i] = -1;
             continue;
         }
-        if (phi_port[i] < 0) w.phi_index[i] = w.num_a + w.num_phi++;
+        if (phi_port[i] < 0 && !pinned[i]) w.phi_index[i] = w.num_a + w.num_phi++;
     }
 
-    // Ports: both voltage driven, one unknown each after [a | phi].
-    w.num_ports = 2;
-    w.port_current = {0, 0};
-    w.port_row = {w.num_a + w.num_phi, w.num_a + w.num_phi + 1};
-    w.port_amplitude = {v_top, 0.0, 0.0, 0.0};
-    w.port_value = w.port_amplitude;
+    // Ports: one unknown each after [a | phi].
+    w.num_ports = static_cast<int>(w.port_current.size());
+    w.port_row.resize(w.num_ports);
+    for (int k = 0; k < w.num_ports; ++k) w.port_row[k] = w.num_a + w.num_phi + k;
     w.num_total = w.num_a + w.num_phi + w.num_ports;
 
     // Per-tet DOF tables.
@@ -353,15 +299,18 @@ void build_cylinder(Workload& w, int n, double v_top, int full_wave) {
             if (w.phi_index[p2] >= 0) {
                 w.tet_idx[16 * t + 6 + ln] = w.phi_index[p2];
                 w.tet_coeff[16 * t + 6 + ln] = 1.0;
-            } else if (phi_port[p2] >= 0) {
-                const int k = phi_port[p2];
-                if (w.port_current[k]) {
-                    w.tet_idx[16 * t + 6 + ln] = w.port_row[k];
-                    w.tet_coeff[16 * t + 6 + ln] = 1.0;
-                } else {
-                    w.tet_fixed[20 * t + 2 * ln] = w.port_value[2 * k];
-                    w.tet_fixed[20 * t + 2 * ln + 1] = w.port_value[2 * k + 1];
-                }
+                continue;
+            }
+            const int k = phi_port[p2];
+            if (k < 0) continue;
+            // A cut's minus side reads the grounded zero (the defaults).
+            if (port_cut[k] && !(tet_side.size() == nt && tet_side[t] > 0)) continue;
+            if (w.port_current[k]) {
+                w.tet_idx[16 * t + 6 + ln] = w.port_row[k];
+                w.tet_coeff[16 * t + 6 + ln] = 1.0;
+            } else {
+                w.tet_fixed[20 * t + 2 * ln] = w.port_value[2 * k];
+                w.tet_fixed[20 * t + 2 * ln + 1] = w.port_value[2 * k + 1];
             }
         }
     }
@@ -380,11 +329,8 @@ void build_cylinder(Workload& w, int n, double v_top, int full_wave) {
         if (w.edge_index[e] >= 0) p2_xyz(w.num_nodes + e, &w.dof_xyz[3 * w.edge_index[e]]);
     for (int i = 0; i < num_p2; ++i)
         if (w.phi_index[i] >= 0) p2_xyz(i, &w.dof_xyz[3 * w.phi_index[i]]);
-    for (int k = 0; k < w.num_ports; ++k) {
-        w.dof_xyz[3 * w.port_row[k]] = 0.5;
-        w.dof_xyz[3 * w.port_row[k] + 1] = 0.5;
-        w.dof_xyz[3 * w.port_row[k] + 2] = k == 0 ? 1.0 : 0.0;
-    }
+    for (int k = 0; k < w.num_ports; ++k)
+        for (int d = 0; d < 3; ++d) w.dof_xyz[3 * w.port_row[k] + d] = port_xyz[3 * k + d];
 
     // Upper-triangle pattern: each tet's live unknowns, sorted and uniqued,
     // give every pair (i <= j); voltage-port rows get their diagonal.
@@ -411,6 +357,187 @@ void build_cylinder(Workload& w, int n, double v_top, int full_wave) {
     }
     w.col_idx.resize(w.row_ptr[N]);
     for (int r = 0; r < N; ++r) std::copy(rows[r].begin(), rows[r].end(), w.col_idx.begin() + w.row_ptr[r]);
+}
+
+// Bodies 0 = conductor (sigma 5.8e7), 1 = air, mu_r = eps_r = 1; a tet is
+// conductor when inside(centroid), the centroid summed vertex by vertex and
+// then scaled, in the reference's order.
+template <class Inside>
+void assign_bodies(Workload& w, Inside inside) {
+    const size_t nt = static_cast<size_t>(w.num_tets);
+    w.material = {5.8e7, 1.0, 1.0, 0.0, 1.0, 1.0};
+    w.body_of_tet.assign(nt, 1);
+    for (size_t t = 0; t < nt; ++t) {
+        double c[3] = {0, 0, 0};
+        for (int q = 0; q < 4; ++q)
+            for (int d = 0; d < 3; ++d) c[d] += w.xyz[3 * w.tets[4 * t + q] + d];
+        for (int d = 0; d < 3; ++d) c[d] *= 0.25;
+        if (inside(c)) w.body_of_tet[t] = 0;
+    }
+    w.body_ptr.assign(3, 0);
+    for (size_t t = 0; t < nt; ++t) ++w.body_ptr[w.body_of_tet[t] + 1];
+    w.body_ptr[2] += w.body_ptr[1];
+    w.body_tets.resize(nt);
+    std::vector<int> cur(w.body_ptr.begin(), w.body_ptr.end() - 1);
+    for (size_t t = 0; t < nt; ++t) w.body_tets[cur[w.body_of_tet[t]]++] = static_cast<int>(t);
+}
+
+void claim_face(const Workload& w, const int* v, int port, std::vector<int>& phi_port) {
+    for (int q = 0; q < 3; ++q) phi_port[v[q]] = port;
+    phi_port[w.num_nodes + find_edge(w, v[0], v[1])] = port;
+    phi_port[w.num_nodes + find_edge(w, v[1], v[2])] = port;
+    phi_port[w.num_nodes + find_edge(w, v[0], v[2])] = port;
+}
+
+}  // namespace
+
+void build_cylinder(Workload& w, int n, double v_top, int full_wave) {
+    if (n < 1) throw std::invalid_argument("build_cylinder: need at least one cell per side");
+    w = Workload{};
+    build_mesh(w, n);
+    const size_t nt = static_cast<size_t>(w.num_tets);
+    assign_bodies(w, [](const double* c) { return std::hypot(c[0] - 0.5, c[1] - 0.5) < 0.2; });
+    if (w.body_ptr[1] == 0)
+        throw std::invalid_argument("build_cylinder: no tet centroid lies inside the conductor at " +
+                                    std::to_string(n) + " cells per side, so its ports have no faces");
+    boundary_edges(w);
+    gauge_tree(w);
+
+    // Port terminals: faces of conductor tets with all three nodes on z = 1
+    // (port 0, v_top) or z = 0 (port 1, 0 V).
+    std::vector<int> phi_port(w.num_nodes + w.num_edges, -1);
+    int port_faces[2] = {0, 0};
+    for (size_t t = 0; t < nt; ++t) {
+        if (w.body_of_tet[t] != 0) continue;
+        for (int f = 0; f < 4; ++f) {
+            int v[3];
+            bool z0 = true, z1 = true;
+            for (int q = 0; q < 3; ++q) {
+                v[q] = w.tets[4 * t + kFaceVerts[f][q]];
+                const double z = w.xyz[3 * v[q] + 2];
+                if (z != 0.0) z0 = false;
+                if (z != 1.0) z1 = false;
+            }
+            if (!z0 && !z1) continue;
+            const int port = z1 ? 0 : 1;
+            ++port_faces[port];
+            claim_face(w, v, port, phi_port);
+        }
+    }
+    if (port_faces[0] == 0 || port_faces[1] == 0)
+        throw std::invalid_argument("build_cylinder: a port surface has no triangles in the mesh at " +
+                                    std::to_string(n) + " cells per side");
+
+    // Both ports voltage driven.
+    w.port_current = {0, 0};
+    w.port_amplitude = {v_top, 0.0, 0.0, 0.0};
+    w.port_value = w.port_amplitude;
+    finish(w, phi_port, {0, 0}, {}, std::vector<uint8_t>(w.num_nodes + w.num_edges, 0), full_wave,
+           {0.5, 0.5, 1.0, 0.5, 0.5, 0.0});
+}
+
+void build_torus(Workload& w, int n, double current) {
+    if (n < 2 || n % 2) throw std::invalid_argument("build_torus: need an even number of cells per side, so that y = 0.5 is a grid plane");
+    w = Workload{};
+    build_mesh(w, n);
+    const size_t nt = static_cast<size_t>(w.num_tets);
+    assign_bodies(w, [](const double* c) {
+        return std::hypot(std::hypot(c[0] - 0.5, c[1] - 0.5) - 0.25, c[2] - 0.5) < 0.04;
+    });
+    if (w.body_ptr[1] == 0)
+        throw std::invalid_argument("build_torus: no tet centroid lies inside the torus at " + std::to_string(n) +
+                                    " cells per side");
+    boundary_edges(w);
+    gauge_tree(w);
+
+    // Conductor faces, each with its tet: a face listed twice is shared by two
+    // conductor tets (conduction across it), once is on the conductor's surface.
+    struct FaceRec {
+        int a, b, c, tet;
+        bool operator<(const FaceRec& o) const {
+            return a != o.a ? a < o.a : (b != o.b ? b < o.b : (c != o.c ? c < o.c : tet < o.tet));
+        }
+    };
+    std::vector<FaceRec> faces;
+    for (size_t t = 0; t < nt; ++t) {
+        if (w.body_of_tet[t] != 0) continue;
+        for (int f = 0; f < 4; ++f) {
+            int v[3] = {w.tets[4 * t + kFaceVerts[f][0]], w.tets[4 * t + kFaceVerts[f][1]],
+                        w.tets[4 * t + kFaceVerts[f][2]]};
+            std::sort(v, v + 3);
+            faces.push_back({v[0], v[1], v[2], static_cast<int>(t)});
+        }
+    }
+    std::sort(faces.begin(), faces.end());
+
+    // The cut: conductor-conductor faces in the plane y = 0.5 with x > 0.5.
+    // Conduction paths: conductor tets joined across shared faces.
+    std::vector<int> uf(nt);
+    std::iota(uf.begin(), uf.end(), 0);
+    auto find = [&](int x) {
+        while (uf[x] != x) x = uf[x] = uf[uf[x]];
+        return x;
+    };
+    std::vector<int> phi_port(w.num_nodes + w.num_edges, -1);
+    std::vector<uint8_t> cut_node(w.num_nodes, 0), cut_tet(nt, 0);
+    int cut_faces = 0;
+    for (size_t i = 0; i + 1 < faces.size(); ++i) {
+        const FaceRec& f = faces[i];
+        const FaceRec& g = faces[i + 1];
+        if (f.a != g.a || f.b != g.b || f.c != g.c) continue;
+        const int ra = find(f.tet), rb = find(g.tet);
+        if (ra != rb) uf[std::max(ra, rb)] = std::min(ra, rb);
+        const int v[3] = {f.a, f.b, f.c};
+        bool on_cut = true;
+        for (int q = 0; q < 3; ++q)
+            if (w.xyz[3 * v[q] + 1] != 0.5 || !(w.xyz[3 * v[q]] > 0.5)) on_cut = false;
+        if (!on_cut) continue;
+        ++cut_faces;
+        claim_face(w, v, 0, phi_port);
+        for (int q = 0; q < 3; ++q) cut_node[v[q]] = 1;
+        cut_tet[f.tet] = cut_tet[g.tet] = 1;
+    }
+    if (cut_faces == 0)
+        throw std::invalid_argument("build_torus: the cut plane crosses no conductor at " + std::to_string(n) +
+                                    " cells per side");
+
+    // Side of every tet touching the cut (a cut face or a cut node): the sign
+    // of (centroid - origin) . d with d = +y (the current-direction hint) and
+    // origin on the plane, i.e. of centroid.y - 0.5, summed in the reference's
+    // order (src/problem_binding.cpp:702-737).
+    std::vector<int8_t> tet_side(nt, 0);
+    for (size_t t = 0; t < nt; ++t) {
+        bool touches = cut_tet[t] != 0;
+        for (int q = 0; q < 4 && !touches; ++q) touches = cut_node[w.tets[4 * t + q]] != 0;
+        if (!touches) continue;
+        double cy = 0;
+        for (int q = 0; q < 4; ++q) cy += w.xyz[3 * w.tets[4 * t + q] + 1];
+        cy *= 0.25;
+        tet_side[t] = cy - 0.5 > 0.0 ? 1 : -1;
+    }
+
+    // A conduction path the cut does not touch is floating: its lowest node
+    // is pinned at 0 V (src/problem_binding.cpp:581-690).
+    std::vector<uint8_t> pinned(w.num_nodes + w.num_edges, 0);
+    std::vector<int> lowest(nt, -1);
+    std::vector<uint8_t> referenced(nt, 0);
+    for (size_t t = 0; t < nt; ++t) {
+        if (w.body_of_tet[t] != 0) continue;
+        const int r = find(static_cast<int>(t));
+        if (cut_tet[t]) referenced[r] = 1;
+        for (int q = 0; q < 4; ++q) {
+            const int v = w.tets[4 * t + q];
+            if (lowest[r] < 0 || v < lowest[r]) lowest[r] = v;
+        }
+    }
+    for (size_t r = 0; r < nt; ++r)
+        if (lowest[r] >= 0 && !referenced[r] && phi_port[lowest[r]] < 0) pinned[lowest[r]] = 1;
+
+    // One internal current port.
+    w.port_current = {1};
+    w.port_amplitude = {current, 0.0};
+    w.port_value = {0.0, 0.0};
+    finish(w, phi_port, {1}, tet_side, pinned, 0, {0.75, 0.5, 0.5});
 }
 
 }  // namespace aphi_b200

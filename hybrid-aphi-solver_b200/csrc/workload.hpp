@@ -1,4 +1,4 @@
-// Synthetic cylinder-in-box workloads: the host-side inputs of the numeric
+// Synthetic workloads (cylinder-in-box, torus with a cut port): the host-side inputs of the numeric
 // hot path (per-tet geometry, per-tet DOF tables, bodies, ports and the
 // upper-triangle CSR pattern), generated directly in the layouts the device
 // kernels consume.
@@ -73,5 +73,12 @@ struct Workload {
 // in air (mu_r = eps_r = 1), voltage ports v_top on the conductor's z = 1 cap
 // and 0 V on its z = 0 cap. full_wave = 0 puts Phi on conductor tets only.
 void build_cylinder(Workload& w, int n, double v_top, int full_wave);
+
+// The torus: the same box and split, conductor (sigma 5.8e7) where the tet
+// centroid is within 0.04 of the circle of radius 0.25 about (0.5, 0.5, 0.5) in
+// the plane z = 0.5, air elsewhere. One internal current port (`current` A,
+// phase 0) on the cut: the conductor-conductor faces in the plane y = 0.5 with
+// x > 0.5, current direction hint +y. Phi on conductor tets only. n even.
+void build_torus(Workload& w, int n, double current);
 
 }  // namespace aphi_b200

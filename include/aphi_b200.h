@@ -67,6 +67,12 @@ int64_t aphi_launch_count(void);
  * with its mesh, binding, DOF-map and sparsity passes. */
 typedef struct aphi_workload aphi_workload;
 int aphi_workload_cylinder(int cells, double v_top, int full_wave, aphi_workload** out);
+/* The multiply-connected case: the same box and split (cells even), a copper
+ * torus (major radius 0.25, minor 0.04, axis z, centred in the box) and one
+ * internal current port of `current` A on the cut y = 0.5, x > 0.5 (its
+ * conductor-conductor faces), current direction hint +y; Phi on the
+ * conductor only. */
+int aphi_workload_torus(int cells, double current, aphi_workload** out);
 void aphi_workload_free(aphi_workload* w);
 /* sizes[0..9]: nodes, tets, edges, unknowns, nnz_upper, num_a, num_phi,
  * num_ports, num_bodies, num_terms (0 until an assembly is built) */

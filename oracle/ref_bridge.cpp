@@ -114,6 +114,50 @@ void build_cylinder_mesh(Mesh& m, int n) {
     }
 }
 
+// The torus variant of the same box: tag 1 "torus" for tets whose centroid is
+// within 0.04 of the circle of radius 0.25 about (0.5, 0.5, 0.5) in z = 0.5,
+// tag 2 "air" elsewhere; tag 12 "cut" on the faces in the plane y = 0.5 with
+// x > 0.5 that two torus tets share (n even).
+void build_torus_mesh(Mesh& m, int n) {
+    auto id = [&](int i, int j, int k) { return (k * (n + 1) + j) * (n + 1) + i; };
+    for (int k = 0; k <= n; ++k)
+        for (int j = 0; j <= n; ++j)
+            for (int i = 0; i <= n; ++i)
+                m.nodes.push_back(Vec3(double(i) / n, double(j) / n, double(k) / n));
+    for (int k = 0; k < n; ++k)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i)
+                for (int t = 0; t < 6; ++t) {
+                    TetVerts v;
+                    for (int q = 0; q < 4; ++q)
+                        v[q] = id(i + kKuhn[t][q][0], j + kKuhn[t][q][1], k + kKuhn[t][q][2]);
+                    m.tets.push_back(v);
+                }
+    m.build_topology();
+    m.tet_tags.assign(m.tets.size(), 2);
+    for (std::size_t t = 0; t < m.tets.size(); ++t) {
+        Vec3 c(0, 0, 0);
+        for (int q = 0; q < 4; ++q) c = c + m.nodes[m.tets[t][q]];
+        c = c * 0.25;
+        if (std::hypot(std::hypot(c.x - 0.5, c.y - 0.5) - 0.25, c.z - 0.5) < 0.04) m.tet_tags[t] = 1;
+    }
+    m.physical_names = {{3, 1, "torus"}, {3, 2, "air"}, {2, 12, "cut"}};
+    for (int f = 0; f < m.num_faces(); ++f) {
+        const FaceTets& ft = m.face_tets[static_cast<std::size_t>(f)];
+        if (ft.count != 2 || m.tet_tags[ft.tets[0]] != 1 || m.tet_tags[ft.tets[1]] != 1) continue;
+        const std::array<int, 3>& fv = m.faces[static_cast<std::size_t>(f)];
+        bool on_cut = true;
+        for (int q = 0; q < 3; ++q)
+            if (m.nodes[fv[q]].y != 0.5 || !(m.nodes[fv[q]].x > 0.5)) on_cut = false;
+        if (!on_cut) continue;
+        TaggedFace tf;
+        tf.nodes = fv;
+        std::sort(tf.nodes.begin(), tf.nodes.end());
+        tf.tag = 12;
+        m.tagged_boundary_faces.push_back(tf);
+    }
+}
+
 void to_complex(const double* in, std::size_t n, std::vector<Complex>& out) {
     out.resize(n);
     for (std::size_t i = 0; i < n; ++i) out[i] = Complex(in[2 * i], in[2 * i + 1]);
@@ -168,6 +212,47 @@ void* ref_kuhn_cylinder(int n, int full_wave, double v_top, int ordering) {
         p->dofs = build_dof_map(p->bound, p->mesh);
         p->pattern = build_sparsity(p->dofs, p->bound, p->mesh, SparsityStorage::UpperTriangle);
         // ordering < 0 skips the symbolic analysis (assembly-only use).
+        if (ordering >= 0) p->analysis = analyze(p->pattern, static_cast<Ordering>(ordering));
+        p->system = make_symmetric_system(p->pattern, p->dofs.num_total);
+        p->map = std::make_unique<ScatterMap>(
+            ScatterMap::build(p->pattern, p->dofs, p->mesh, p->bound));
+        p->has_mesh = true;
+        return 0;
+    });
+    if (rc != 0) return nullptr;
+    return p.release();
+}
+
+/// The torus with one internal current port (`current` A, hint +y) through
+/// the same pipeline.
+void* ref_kuhn_torus(int n, double current, int ordering) {
+    auto p = std::make_unique<RefProblem>();
+    int rc = guarded([&] {
+        build_torus_mesh(p->mesh, n);
+        Problem pr;
+        pr.type = AnalysisType::Frequency;
+        pr.frequencies = {50.0};
+        pr.formulation = Formulation::Reduced;
+        pr.conditioning = Conditioning::RowScaled;
+        Body w;
+        w.name = "B1";
+        w.volume = "torus";
+        w.sigma = 5.8e7;
+        Body a;
+        a.name = "B2";
+        a.volume = "air";
+        a.sigma = 0.0;
+        pr.bodies = {w, a};
+        Port p1;
+        p1.name = "P1";
+        p1.type = PortType::InternalCurrent;
+        p1.surface = {"cut"};
+        p1.amplitude = current;
+        p1.current_direction = Vec3(0.0, 1.0, 0.0);
+        pr.ports = {p1};
+        p->bound = bind_to_mesh(pr, p->mesh);
+        p->dofs = build_dof_map(p->bound, p->mesh);
+        p->pattern = build_sparsity(p->dofs, p->bound, p->mesh, SparsityStorage::UpperTriangle);
         if (ordering >= 0) p->analysis = analyze(p->pattern, static_cast<Ordering>(ordering));
         p->system = make_symmetric_system(p->pattern, p->dofs.num_total);
         p->map = std::make_unique<ScatterMap>(

@@ -25,6 +25,8 @@ def ref() -> C.CDLL:
         vp = C.c_void_p
         L.ref_kuhn_cylinder.restype = vp
         L.ref_kuhn_cylinder.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int]
+        L.ref_kuhn_torus.restype = vp
+        L.ref_kuhn_torus.argtypes = [C.c_int, C.c_double, C.c_int]
         L.ref_from_pattern.restype = vp
         L.ref_from_pattern.argtypes = [C.c_int, vp, vp, C.c_int]
         L.ref_free.argtypes = [vp]
@@ -65,6 +67,10 @@ class RefProblem:
     @classmethod
     def cylinder(cls, cells: int, v_top: float = 1.0, full_wave: bool = False, ordering: int = 2):
         return cls(ref().ref_kuhn_cylinder(cells, 1 if full_wave else 0, v_top, ordering))
+
+    @classmethod
+    def torus(cls, cells: int, current: float = 1.0, ordering: int = 2):
+        return cls(ref().ref_kuhn_torus(cells, current, ordering))
 
     @classmethod
     def from_pattern(cls, row_ptr, col_idx, ordering: int = 2):

@@ -8,6 +8,7 @@ import pytest
 import torch
 
 import aphi_b200 as ab
+from solvecheck import refined_solution, rel, spmv_extended  # noqa: F401
 
 pytestmark = pytest.mark.gpu
 
@@ -128,34 +129,6 @@ def test_random_patterns_match_reference(small_front, cuda, ref_or_skip):
 
 
 OMEGAS = [2 * np.pi * 50.0, 2 * np.pi * 1e4, 2 * np.pi * 1e6]
-
-
-def spmv_extended(rp, ci, v, x):
-    """A x for the upper-stored A in extended precision (numpy clongdouble)."""
-    n = rp.size - 1
-    vl = v.astype(np.clongdouble)
-    xl = x.astype(np.clongdouble)
-    rows = np.repeat(np.arange(n), np.diff(rp))
-    y = np.zeros(n, np.clongdouble)
-    np.add.at(y, rows, vl * xl[ci])
-    off = ci != rows
-    np.add.at(y, ci[off], vl[off] * xl[rows[off]])
-    return y
-
-
-def refined_solution(factor, rp, ci, v, b, x, steps=6):
-    """x* : x refined with residuals in extended precision and corrections
-    from the FP64 factor -- a reference solution accurate well beyond what a
-    plain FP64 solve of an ill-conditioned system gives."""
-    for _ in range(steps):
-        r = np.array(b.astype(np.clongdouble) - spmv_extended(rp, ci, v, x), np.complex128)
-        dx = factor.solve(torch.from_numpy(r).cuda().unsqueeze(0))[0].cpu().numpy()
-        x = np.array(x.astype(np.clongdouble) + dx.astype(np.clongdouble), np.complex128)
-    return x
-
-
-def rel(a, b):
-    return np.linalg.norm(a - b) / np.linalg.norm(b)
 
 
 @pytest.mark.parametrize("cells,small_front", [(6, 96), (6, 8), (8, 96), (12, 96), (12, 16)])

@@ -1,4 +1,5 @@
-"""The synthetic workload generator against the reference's own host pipeline
+"""The synthetic workload generators (cylinder-in-box, torus with a cut port)
+against the reference's own host pipeline
 (build_topology, bind_to_mesh with the tree-cotree gauge, build_dof_map,
 local_dofs, build_sparsity): bit-exact, so the GPU path is fed the same
 matrices the reference assembles. CPU only."""
@@ -21,6 +22,38 @@ def test_cylinder_matches_reference_pipeline(cells, ref_or_skip):
     np.testing.assert_array_equal(w.tet_idx, idx)
     np.testing.assert_array_equal(w.tet_coeff, co)
     np.testing.assert_array_equal(w.tet_fixed, fx)
+
+
+@pytest.mark.parametrize("cells", [16, 24])
+def test_torus_matches_reference_pipeline(cells, ref_or_skip):
+    """The torus with its internal current port: the cut's nodes read the
+    port unknown from plus-side tets and a grounded zero from minus-side
+    ones (src/dof_map.cpp:160-181), so the per-tet tables are where a wrong
+    side would show."""
+    w = ab.Workload.torus(cells)
+    r = ref_or_skip.RefProblem.torus(cells, ordering=-1)
+    assert (w.num_nodes, w.num_tets, w.num_edges) == (r.num_nodes, r.num_tets, r.num_edges)
+    assert (w.num_a, w.num_phi, w.num_ports, w.num_unknowns) == (r.num_a, r.num_phi, r.num_ports, r.n)
+    assert w.num_ports == 1 and list(w.port_current) == [1]
+    rp, ci = r.pattern()
+    np.testing.assert_array_equal(w.row_ptr, rp)
+    np.testing.assert_array_equal(w.col_idx, ci)
+    idx, co, fx = r.tet_dofs()
+    np.testing.assert_array_equal(w.tet_idx, idx)
+    np.testing.assert_array_equal(w.tet_coeff, co)
+    np.testing.assert_array_equal(w.tet_fixed, fx)
+    # both sides of the cut exist: some tets read the port unknown, and the
+    # port unknown appears only through Phi entries
+    port_row = int(w.port_row[0])
+    assert (w.tet_idx.reshape(-1, 16)[:, 6:] == port_row).any()
+    assert not (w.tet_idx.reshape(-1, 16)[:, :6] == port_row).any()
+
+
+def test_torus_refusals():
+    with pytest.raises(ab.AphiError, match="even number"):
+        ab.Workload.torus(15)   # y = 0.5 is not a grid plane
+    with pytest.raises(ab.AphiError, match="crosses no conductor"):
+        ab.Workload.torus(12)   # the tube is too thin for a conductor face on the cut
 
 
 def test_config1_sizes():
