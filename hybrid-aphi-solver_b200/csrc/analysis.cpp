@@ -30,10 +30,16 @@ T* upload(const std::vector<T>& h, long long& bytes) {
 // reads and writes it a quarter as often.
 void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing, std::vector<Launch>& plan) {
     const Symbolic& S = A.S;
-    auto push = [&](int kind, long long first) {
+    auto push = [&](int kind, long long first, int kcap = kTcPanel) {
         const int count = static_cast<int>(items.size() - first);
-        if (count > 0) plan.push_back({kind, first, count});
+        if (count > 0) plan.push_back({kind, first, count, kcap});
     };
+    // The tensor-core plan updates the trailing matrix after every 128-column
+    // panel. The FP64 / SIMT plan pairs the panels: after an even panel it
+    // updates only the next panel's columns, after the odd one the rest of the
+    // front with both (K up to 256), so every trailing entry is read and
+    // written once per 256 columns instead of once per 128.
+    const bool paired = trailing == K_UPDATE_WIDE;
     for (int L = 0; L < S.num_levels; ++L) {
         const int* lb = S.level_list.data() + S.level_ptr[L];
         const int* le = S.level_list.data() + S.level_ptr[L + 1];
@@ -84,21 +90,29 @@ void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing,
                     for (int i = j; i < m; i += kTile) items.push_back({s, k0, i, j});
             }
             push(K_UPDATE_PANEL, f0);
-            // A panel's trailing update follows its last 32-column step.
+            // A panel's trailing update follows its last 32-column step. Tiles
+            // cover rows and columns [pe, jend) x ..., lower part only.
             f0 = static_cast<long long>(items.size());
+            const bool odd = (k0 / kTcPanel) % 2 == 1;
             for (int s : large) {
                 const int w = width(s);
                 if (k0 >= w) continue;
                 const bool panel_done = (k0 + kStep) % kTcPanel == 0 || k0 + kStep >= w;
                 if (!panel_done) continue;
-                const int p0 = (k0 / kTcPanel) * kTcPanel;
+                int p0 = (k0 / kTcPanel) * kTcPanel;
                 const int pe = std::min(w, p0 + kTcPanel);
                 const int m = S.sn_rows[s];
-                for (int j = pe; j < m; j += kTcN)
+                int jend = m;
+                // Only full pairs are paired: the next panel's tiles then end
+                // exactly at its last column. A partial second panel is updated
+                // on its own (K = w - p0 < 128 under the pair's cap).
+                if (paired && !odd && p0 + kWidePair <= w) jend = p0 + kWidePair;  // the next panel only
+                if (paired && odd && p0 + kTcPanel <= w) p0 -= kTcPanel;          // both panels of the pair
+                for (int j = pe; j < jend; j += kTcN)
                     for (int i = pe; i < m; i += kTcM)
                         if (i + kTcM > j) items.push_back({s, p0, i, j});
             }
-            push(trailing, f0);
+            push(trailing, f0, paired && odd ? kWidePair : kTcPanel);
         }
     }
 }

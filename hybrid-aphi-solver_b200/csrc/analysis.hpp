@@ -3,6 +3,8 @@
 // numeric factorization and the solves replay.
 #pragma once
 
+#include "tc_config.hpp"
+
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -32,6 +34,7 @@ struct Launch {
     int kind;
     long long first;  // offset into the item array
     int count;
+    int kcap = kTcPanel;  // trailing updates: panel columns applied at once (K = min(kcap, w - p0))
 };
 
 struct Item {
@@ -41,6 +44,7 @@ struct Item {
 constexpr int kStep = 32;        // pivot block width of the blocked factorization
 constexpr int kTile = 64;        // update tile
 constexpr int kTrsmRows = 128;   // rows per TRSM block
+constexpr int kWidePair = 2 * kTcPanel;  // FP64 / SIMT trailing updates apply two panels at once
 constexpr int kEaCols = 32;      // front columns per extend-add item
 constexpr int kSolveBlock = 64;  // columns per triangular-solve block
 constexpr int kSolveRows = 256;  // rows per solve update item

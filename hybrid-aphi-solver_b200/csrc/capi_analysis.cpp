@@ -101,7 +101,7 @@ int aphi_analysis_plan_stats(const aphi_analysis* a, int plan, int64_t* launches
                 const int m = S.sn_rows[it.s];
                 double u = 0, e = 0;
                 if (l.kind == K_UPDATE_WIDE || l.kind == K_UPDATE_TC) {
-                    const int K = std::min(kTcPanel, w - it.a);
+                    const int K = std::min(l.kcap, w - it.a);
                     u = 8.0 * K * lower(it.b, std::min(m, it.b + kTcM), it.c, std::min(m, it.c + kTcN));
                     e = 8.0 * K * kTcM * kTcN;
                 } else if (l.kind == K_UPDATE_PANEL) {

@@ -349,7 +349,7 @@ constexpr int wide_smem() {
 
 template <class R>
 __global__ void __launch_bounds__(256) k_update_wide(Sched S, long long item0, cx<R>* Lb, cx<R>* CBb,
-                                                     long long lstride, long long cbstride) {
+                                                     long long lstride, long long cbstride, int kcap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<R>* As = reinterpret_cast<cx<R>*>(smem_raw);   // [2][KC][128], scaled by D
     cx<R>* Bs = As + 2 * kWideKC * kWideM;            // [2][KC][64]
@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(256) k_update_wide(Sched S, long long item0, c
     const int w = S.first[s + 1] - S.first[s];
     const int m = S.rows[s];
     const int cs = m - w;
-    const int K = min(kTcPanel, w - p0);
+    const int K = min(kcap, w - p0);
     cx<R>* Ls = L + S.loff[s];
     cx<R>* CBs = CB + (cs > 0 ? S.cboff[s] : 0);
     const cx<R>* P = Ls + static_cast<long long>(p0) * m;
@@ -448,8 +448,9 @@ __global__ void __launch_bounds__(256) k_update_wide(Sched S, long long item0, c
     }
 }
 
-// FP64 trailing update of a complete panel on the FP64 tensor path (DMMA,
-// mma.sync m8n8k4). Same items, tile and K as k_update_wide. 8 warps in a 4 x 2
+// FP64 trailing update of complete panels on the FP64 tensor path (DMMA,
+// mma.sync m8n8k4). Same items, tile and K (up to kcap = 256: a pair of
+// 128-column panels) as k_update_wide. 8 warps in a 4 x 2
 // grid, each a 32 x 32 complex block of the tile: 4 x 4 blocks of 8 x 8, each
 // four real products (Cr += Ar Br - Ai Bi, Ci += Ar Bi + Ai Br; the minus by
 // a negated copy of Ai's fragment).
@@ -470,7 +471,7 @@ __global__ void __launch_bounds__(256) k_update_wide(Sched S, long long item0, c
 constexpr int kDmmaKC = 16, kDmmaStages = 3;
 constexpr int kDmmaLdA = kWideM + 2, kDmmaLdB = kWideN + 2;
 constexpr int kDmmaStage = kDmmaKC * (kDmmaLdA + kDmmaLdB);  // complex entries
-constexpr int kDmmaSmem = (kTcPanel + kDmmaStages * kDmmaStage) * 16;
+constexpr int kDmmaSmem = (kWidePair + kDmmaStages * kDmmaStage) * 16;
 static_assert(kDmmaSmem <= 227 * 1024, "DMMA ring exceeds shared memory");
 static_assert(kTcPanel % kDmmaKC == 0 && kDmmaKC % 4 == 0, "chunks must tile the panel in k-steps of 4");
 
@@ -490,10 +491,11 @@ __device__ __forceinline__ void red_sub(double* p, double v) {
 }
 
 __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long item0, cx<double>* Lb,
-                                                          cx<double>* CBb, long long lstride, long long cbstride) {
+                                                          cx<double>* CBb, long long lstride, long long cbstride,
+                                                          int kcap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cx<double>* Ds = reinterpret_cast<cx<double>*>(smem_raw);  // [kTcPanel] pivots of the panel
-    cx<double>* Ring = Ds + kTcPanel;                            // [stage][A: KC x ldA | B: KC x ldB]
+    cx<double>* Ds = reinterpret_cast<cx<double>*>(smem_raw);  // [kWidePair] pivots of the panels
+    cx<double>* Ring = Ds + kWidePair;                           // [stage][A: KC x ldA | B: KC x ldB]
     const Item it = S.items[item0 + blockIdx.x];
     const int s = it.s, p0 = it.a, i0 = it.b, j0 = it.c;
     cx<double>* L = Lb + lstride * blockIdx.y;
@@ -501,7 +503,7 @@ __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long ite
     const int w = S.first[s + 1] - S.first[s];
     const int m = S.rows[s];
     const int cs = m - w;
-    const int K = min(kTcPanel, w - p0);
+    const int K = min(kcap, w - p0);
     cx<double>* Ls = L + S.loff[s];
     cx<double>* CBs = CB + (cs > 0 ? S.cboff[s] : 0);
     const cx<double>* P = Ls + static_cast<long long>(p0) * m;
@@ -541,7 +543,7 @@ __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long ite
     cp_async_commit();
     if (nc > 1) fetch(1);
     cp_async_commit();
-    if (tid < kTcPanel) Ds[tid] = tid < K ? dg[static_cast<long long>(tid) * (m + 1)] : cx<double>{0, 0};
+    for (int t = tid; t < kWidePair; t += 256) Ds[t] = t < K ? dg[static_cast<long long>(t) * (m + 1)] : cx<double>{0, 0};
     for (int c = 0; c < nc; ++c) {
         cp_async_wait<1>();  // this thread's copies of chunk c have landed
         __syncthreads();     // everyone's have; everyone is done with chunk c - 1
