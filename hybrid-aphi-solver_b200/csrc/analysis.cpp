@@ -25,7 +25,7 @@ T* upload(const std::vector<T>& h, long long& bytes) {
 // block, solves the panel rows below it and updates the rest of the panel's
 // own columns. Once a panel is complete, its trailing update -- every column
 // to its right, K = panel width -- runs as 128 x 64 tiles: `trailing` is
-// K_UPDATE_WIDE (SIMT, either precision) or K_UPDATE_TC (tensor cores, FP32).
+// K_UPDATE_WIDE (DMMA for FP64, SIMT for FP32) or K_UPDATE_TC (tensor cores, FP32).
 // Updating the trailing front once per 128 columns instead of once per 32
 // reads and writes it a quarter as often.
 void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing, std::vector<Launch>& plan) {
@@ -34,12 +34,11 @@ void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing,
         const int count = static_cast<int>(items.size() - first);
         if (count > 0) plan.push_back({kind, first, count, kcap});
     };
-    // The tensor-core plan updates the trailing matrix after every 128-column
-    // panel. The FP64 / SIMT plan pairs the panels: after an even panel it
-    // updates only the next panel's columns, after the odd one the rest of the
+    // Panels are paired for the trailing update: after an even panel only the
+    // next panel's columns are updated, after the odd one the rest of the
     // front with both (K up to 256), so every trailing entry is read and
     // written once per 256 columns instead of once per 128.
-    const bool paired = trailing == K_UPDATE_WIDE;
+    const bool paired = true;
     for (int L = 0; L < S.num_levels; ++L) {
         const int* lb = S.level_list.data() + S.level_ptr[L];
         const int* le = S.level_list.data() + S.level_ptr[L + 1];

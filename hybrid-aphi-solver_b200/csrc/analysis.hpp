@@ -44,7 +44,7 @@ struct Item {
 constexpr int kStep = 32;        // pivot block width of the blocked factorization
 constexpr int kTile = 64;        // update tile
 constexpr int kTrsmRows = 128;   // rows per TRSM block
-constexpr int kWidePair = 2 * kTcPanel;  // FP64 / SIMT trailing updates apply two panels at once
+constexpr int kWidePair = 2 * kTcPanel;  // trailing updates apply a pair of panels at once
 constexpr int kEaCols = 32;      // front columns per extend-add item
 constexpr int kSolveBlock = 64;  // columns per triangular-solve block
 constexpr int kSolveRows = 256;  // rows per solve update item

@@ -284,7 +284,7 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
                 break;
             case K_UPDATE_TC:
                 if constexpr (sizeof(R) == 4)
-                    k_update_tc<<<grid, kTcThreads, kTcSmem, st>>>(S, l.first, L, CB, ls, cs, f->err);
+                    k_update_tc<<<grid, kTcThreads, kTcSmem, st>>>(S, l.first, L, CB, ls, cs, l.kcap, f->err);
                 else
                     throw Error(APHI_ERR_INVALID, "tensor-core update planned for an FP64 factor");
                 break;

@@ -597,13 +597,13 @@ __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long ite
     }
 }
 
-// Tensor-core trailing update of a complete panel (FP32 factors). Item
-// (s, p0, i0, j0): F[i, j] -= sum_{t in panel} L[i,t] D[t] L[j,t] over the
-// 128 x 64 tile at rows i0.., columns j0.. (i >= j). K is the panel width
-// (<= 128). A bounded wait that expires sets err[0] and leaves the tile
+// Tensor-core trailing update of complete panels (FP32 factors). Item
+// (s, p0, i0, j0): F[i, j] -= sum_{t in panels} L[i,t] D[t] L[j,t] over the
+// 128 x 64 tile at rows i0.., columns j0.. (i >= j). K = min(kcap, w - p0):
+// one panel (128) or a pair (256). A bounded wait that expires sets err[0] and leaves the tile
 // unchanged; the host reports it.
 __global__ void __launch_bounds__(kTcThreads) k_update_tc(Sched S, long long item0, cx<float>* Lb, cx<float>* CBb,
-                                                          long long lstride, long long cbstride, int* err) {
+                                                          long long lstride, long long cbstride, int kcap, int* err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Item it = S.items[item0 + blockIdx.x];
     const int s = it.s, p0 = it.a, i0 = it.b, j0 = it.c;
@@ -612,7 +612,7 @@ __global__ void __launch_bounds__(kTcThreads) k_update_tc(Sched S, long long ite
     const int w = S.first[s + 1] - S.first[s];
     const int m = S.rows[s];
     const int cs = m - w;
-    const int K = min(kTcPanel, w - p0);
+    const int K = min(kcap, w - p0);
     cx<float>* Ls = L + S.loff[s];
     cx<float>* CBs = CB + (cs > 0 ? S.cboff[s] : 0);
     const float2* P = reinterpret_cast<const float2*>(Ls + static_cast<long long>(p0) * m);
