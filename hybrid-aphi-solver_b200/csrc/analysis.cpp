@@ -34,11 +34,16 @@ void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing,
         const int count = static_cast<int>(items.size() - first);
         if (count > 0) plan.push_back({kind, first, count, kcap});
     };
-    // Panels are paired for the trailing update: after an even panel only the
-    // next panel's columns are updated, after the odd one the rest of the
-    // front with both (K up to 256), so every trailing entry is read and
-    // written once per 256 columns instead of once per 128.
-    const bool paired = true;
+    // Panels are grouped for the trailing update: after each panel but a
+    // group's last only the group's remaining columns are updated; after its
+    // last, the rest of the front with all of the group's panels, so every
+    // trailing entry is read and written once per group instead of once per
+    // 128 columns. Groups are 4 panels (K up to 512) in fronts of at least
+    // kGroup4Rows rows, where the trailing matrix dwarfs the group's columns,
+    // and 2 panels (K up to 256) elsewhere, where the in-group updates would
+    // cost more than the traffic they save. Only full groups are grouped: the
+    // narrow tiles then end exactly at the group's last column, and a front's
+    // incomplete last group is updated panel by panel.
     for (int L = 0; L < S.num_levels; ++L) {
         const int* lb = S.level_list.data() + S.level_ptr[L];
         const int* le = S.level_list.data() + S.level_ptr[L + 1];
@@ -91,27 +96,32 @@ void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing,
             push(K_UPDATE_PANEL, f0);
             // A panel's trailing update follows its last 32-column step. Tiles
             // cover rows and columns [pe, jend) x ..., lower part only.
-            f0 = static_cast<long long>(items.size());
-            const bool odd = (k0 / kTcPanel) % 2 == 1;
-            for (int s : large) {
-                const int w = width(s);
-                if (k0 >= w) continue;
-                const bool panel_done = (k0 + kStep) % kTcPanel == 0 || k0 + kStep >= w;
-                if (!panel_done) continue;
-                int p0 = (k0 / kTcPanel) * kTcPanel;
-                const int pe = std::min(w, p0 + kTcPanel);
-                const int m = S.sn_rows[s];
-                int jend = m;
-                // Only full pairs are paired: the next panel's tiles then end
-                // exactly at its last column. A partial second panel is updated
-                // on its own (K = w - p0 < 128 under the pair's cap).
-                if (paired && !odd && p0 + kWidePair <= w) jend = p0 + kWidePair;  // the next panel only
-                if (paired && odd && p0 + kTcPanel <= w) p0 -= kTcPanel;          // both panels of the pair
-                for (int j = pe; j < jend; j += kTcN)
-                    for (int i = pe; i < m; i += kTcM)
-                        if (i + kTcM > j) items.push_back({s, p0, i, j});
+            // One launch per K cap: a group's last panel applies the whole group.
+            for (int cap_group : {1, 2, 4}) {
+                f0 = static_cast<long long>(items.size());
+                for (int s : large) {
+                    const int w = width(s);
+                    if (k0 >= w) continue;
+                    const bool panel_done = (k0 + kStep) % kTcPanel == 0 || k0 + kStep >= w;
+                    if (!panel_done) continue;
+                    const int m = S.sn_rows[s];
+                    const int G = m >= kGroup4Rows ? 4 : 2;
+                    const int q = (k0 / kTcPanel) % G;        // the panel's place in its group
+                    int p0 = (k0 / kTcPanel) * kTcPanel;
+                    const int pe = std::min(w, p0 + kTcPanel);
+                    const int g0 = p0 - q * kTcPanel;         // the group's first column
+                    const bool full = g0 + G * kTcPanel <= w;
+                    const bool last = full && q == G - 1;
+                    if ((last ? G : 1) != cap_group) continue;
+                    int jend = m;
+                    if (full && !last) jend = g0 + G * kTcPanel;  // the group's remaining columns
+                    if (last) p0 = g0;                            // all of the group's panels
+                    for (int j = pe; j < jend; j += kTcN)
+                        for (int i = pe; i < m; i += kTcM)
+                            if (i + kTcM > j) items.push_back({s, p0, i, j});
+                }
+                push(trailing, f0, cap_group * kTcPanel);
             }
-            push(trailing, f0, paired && odd ? kWidePair : kTcPanel);
         }
     }
 }

@@ -44,7 +44,9 @@ struct Item {
 constexpr int kStep = 32;        // pivot block width of the blocked factorization
 constexpr int kTile = 64;        // update tile
 constexpr int kTrsmRows = 128;   // rows per TRSM block
-constexpr int kWidePair = 2 * kTcPanel;  // trailing updates apply a pair of panels at once
+constexpr int kPanelGroup = 4;                 // most panels per trailing update of the rest of a front
+constexpr int kWidePair = kPanelGroup * kTcPanel;  // the most panel columns one trailing update applies
+constexpr int kGroup4Rows = 8192;              // fronts this tall group 4 panels, smaller ones 2
 constexpr int kEaCols = 32;      // front columns per extend-add item
 constexpr int kSolveBlock = 64;  // columns per triangular-solve block
 constexpr int kSolveRows = 256;  // rows per solve update item

@@ -449,8 +449,8 @@ __global__ void __launch_bounds__(256) k_update_wide(Sched S, long long item0, c
 }
 
 // FP64 trailing update of complete panels on the FP64 tensor path (DMMA,
-// mma.sync m8n8k4). Same items, tile and K (up to kcap = 256: a pair of
-// 128-column panels) as k_update_wide. 8 warps in a 4 x 2
+// mma.sync m8n8k4). Same items, tile and K (up to kcap = kWidePair: a group
+// of 128-column panels) as k_update_wide. 8 warps in a 4 x 2
 // grid, each a 32 x 32 complex block of the tile: 4 x 4 blocks of 8 x 8, each
 // four real products (Cr += Ar Br - Ai Bi, Ci += Ar Bi + Ai Br; the minus by
 // a negated copy of Ai's fragment).
@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long ite
                                                           cx<double>* CBb, long long lstride, long long cbstride,
                                                           int kcap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cx<double>* Ds = reinterpret_cast<cx<double>*>(smem_raw);  // [kWidePair] pivots of the panels
+    cx<double>* Ds = reinterpret_cast<cx<double>*>(smem_raw);  // [kWidePair] pivots of the group's panels
     cx<double>* Ring = Ds + kWidePair;                           // [stage][A: KC x ldA | B: KC x ldB]
     const Item it = S.items[item0 + blockIdx.x];
     const int s = it.s, p0 = it.a, i0 = it.b, j0 = it.c;
@@ -600,7 +600,7 @@ __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long ite
 // Tensor-core trailing update of complete panels (FP32 factors). Item
 // (s, p0, i0, j0): F[i, j] -= sum_{t in panels} L[i,t] D[t] L[j,t] over the
 // 128 x 64 tile at rows i0.., columns j0.. (i >= j). K = min(kcap, w - p0):
-// one panel (128) or a pair (256). A bounded wait that expires sets err[0] and leaves the tile
+// one panel (128) or a group of them (up to kWidePair). A bounded wait that expires sets err[0] and leaves the tile
 // unchanged; the host reports it.
 __global__ void __launch_bounds__(kTcThreads) k_update_tc(Sched S, long long item0, cx<float>* Lb, cx<float>* CBb,
                                                           long long lstride, long long cbstride, int kcap, int* err) {

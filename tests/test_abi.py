@@ -53,16 +53,16 @@ def test_analysis_matches_reference_etree_on_host():
 
 def test_plan_stats_account_for_the_same_update_work():
     """Both factorization plans (DMMA / SIMT trailing tiles, tensor-core
-    trailing tiles) do the same Schur-complement work, with the trailing
-    matrix updated after every pair of 128-column panels (the next panel's
-    columns after the first, the rest with both after the second): equal
+    trailing tiles) do the same Schur-complement work, with the rest of a
+    front updated once per group of 128-column panels (each panel before the
+    group's last updates only the group's remaining columns): equal
     tiles and useful flops per kind, and as many useful flops as one update
     per panel would apply (the in-panel and trailing updates together carry
     the factorization's flops). Never more useful than executed; each plan
     uses only its own tile kind."""
-    w = ab.Workload.cylinder(10)
+    w = ab.Workload.cylinder(12)
     an = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx))
-    assert an.info["max_width"] > 256   # fronts with several panel pairs
+    assert an.info["max_width"] > 512   # fronts with several panel groups
     simt = an.plan_stats(0, flops=True)
     tc = an.plan_stats(1, flops=True)
     assert "update_tc" not in simt and "update_wide" not in tc
