@@ -532,6 +532,18 @@ def _stats_dict(s: FactorStats) -> dict:
     return {k: getattr(s, k) for k in STATS_KEYS}
 
 
+def _expect_device(t, shape, what: str, contiguous: bool = True) -> None:
+    """The device entry points take raw pointers, so a tensor of the wrong
+    shape, type or placement would be read past its end: refuse it here."""
+    import torch
+    ok = (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.complex128
+          and tuple(t.shape) == tuple(shape) and (t.is_contiguous() or not contiguous))
+    if not ok:
+        got = (f"{tuple(t.shape)} {t.dtype} on {t.device}" if isinstance(t, torch.Tensor) else type(t).__name__)
+        raise InvalidArgument(ERR_BAD_SHAPE, f"{what}: expected a {'contiguous ' if contiguous else ''}complex128 "
+                                             f"CUDA tensor of shape {tuple(shape)}, got {got}")
+
+
 class Factor:
     """`batch` numeric factorizations sharing one Analysis, resident on the
     device (factorize_ldlt, src/factorization.cpp:109-218, run as a
@@ -551,6 +563,7 @@ class Factor:
                   stream=None) -> bool:
         """values: complex128 device tensor [batch, nnz]. Returns False (with
         self.stats[k]['ok'] == 0) if any entry met the pivot floor."""
+        _expect_device(values, (self.batch, self.analysis.nnz), "factorize: values")
         st = (FactorStats * self.batch)()
         rc = lib().aphi_factorize(self._h, dptr(values), equilibration_iterations, pivot_floor, st,
                                   stream_ptr(stream))
@@ -566,9 +579,12 @@ class Factor:
         squeeze = b.dim() == 2
         bb = b.unsqueeze(1) if squeeze else b
         nrhs = bb.shape[1]
+        _expect_device(bb, (self.batch, nrhs, self.n), "solve: b", contiguous=False)
         bb = bb.contiguous()
         if x is None:
             x = torch.empty_like(bb)
+        else:
+            _expect_device(x.unsqueeze(1) if x.dim() == 2 else x, (self.batch, nrhs, self.n), "solve: x")
         check(lib().aphi_solve(self._h, nrhs, dptr(bb), dptr(x), stream_ptr(stream)))
         return x.squeeze(1) if squeeze else x
 
@@ -581,6 +597,8 @@ class Factor:
         squeeze = b.dim() == 2
         bb = (b.unsqueeze(1) if squeeze else b).contiguous()
         nrhs = bb.shape[1]
+        _expect_device(values, (self.batch, self.analysis.nnz), "solve_refined: values")
+        _expect_device(bb, (self.batch, nrhs, self.n), "solve_refined: b")
         x = torch.empty_like(bb)
         it = (C.c_int * (self.batch * nrhs))()
         be = (C.c_double * (self.batch * nrhs))()
@@ -662,6 +680,9 @@ def residuals(analysis: Analysis, values, x, b, stream=None) -> np.ndarray:
     bb = b.unsqueeze(1) if b.dim() == 2 else b
     xx = x.unsqueeze(1) if x.dim() == 2 else x
     batch, nrhs = bb.shape[0], bb.shape[1]
+    _expect_device(values, (batch, analysis.nnz), "residuals: values")
+    _expect_device(bb, (batch, nrhs, analysis.n), "residuals: b", contiguous=False)
+    _expect_device(xx, (batch, nrhs, analysis.n), "residuals: x", contiguous=False)
     out = np.zeros((batch, nrhs, 2))
     check(lib().aphi_residuals(analysis._h, batch, nrhs, dptr(values), dptr(xx.contiguous()),
                                dptr(bb.contiguous()), out.ctypes.data_as(PD), stream_ptr(stream)))
@@ -763,8 +784,10 @@ class SweepSolver:
         self.factorized = {PREC_FP32: 0, PREC_FP64: 0}   # entries factorized since profile(True)
 
     def _factor(self, precision: int, size: int) -> Factor:
+        """The resident factor of this precision holding `size` entries: kept
+        across calls and chunks, reallocated only when it must grow."""
         f = self._factors.get(precision)
-        if f is None or f.batch != size:
+        if f is None or f.capacity < size:
             if f is not None:
                 self._fold_profile(precision, f)
                 f.close()
@@ -773,6 +796,8 @@ class SweepSolver:
             if self._profile:
                 f.profile(True)
             self._factors[precision] = f
+        if f.batch != size:
+            f.set_batch(size)
         return f
 
     def _fold_profile(self, precision, f):
