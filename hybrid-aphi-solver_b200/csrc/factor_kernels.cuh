@@ -709,6 +709,7 @@ __global__ void __launch_bounds__(256) k_fwd_diag(Sched S, long long item0, Solv
     const int f = S.first[s];
     const int jb = min(kSolveBlock, w - j0);
     const cx<R>* P = Lb + lstride * blockIdx.y + S.loff[s] + j0 + static_cast<long long>(j0) * m;
+#pragma unroll 4
     for (int e = threadIdx.x; e < jb * jb; e += blockDim.x) {
         const int i = e % jb, j = e / jb;
         T[i + j * kSolveBlock] = P[i + static_cast<long long>(j) * m];
@@ -749,11 +750,19 @@ __global__ void __launch_bounds__(256) k_fwd_update(Sched S, long long item0, So
     cx<R> acc[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) acc[k] = cx<R>{0, 0};
-    for (int j = 0; j < jb; ++j) {
-        const cx<R> l = P[static_cast<long long>(j) * m];
+    // Eight columns' loads in flight before they are used (one round trip per
+    // eight columns, not per column); the sums keep their column order.
+    for (int j = 0; j < jb; j += 8) {
+        cx<R> l[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k)
-            if (k < a.nr) acc[k] = acc[k] + l * ys[k][j];
+        for (int u = 0; u < 8; ++u) l[u] = j + u < jb ? P[static_cast<long long>(j + u) * m] : cx<R>{0, 0};
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (j + u >= jb) break;
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (k < a.nr) acc[k] = acc[k] + l[u] * ys[k][j + u];
+        }
     }
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
@@ -794,11 +803,19 @@ __global__ void __launch_bounds__(256) k_bwd_update(Sched S, long long item0, So
         cx<R> acc[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) acc[k] = cx<R>{0, 0};
-        for (int t = lane; t < nrows; t += 32) {
-            const cx<R> l = col[t];
+        // All of a lane's rows (at most 8: kSolveRows = 256) loaded before
+        // use; the sums keep their row order.
+        static_assert(kSolveRows <= 32 * 8, "one pass of 8 loads per lane covers the chunk");
+        cx<R> l[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) l[u] = lane + 32 * u < nrows ? col[lane + 32 * u] : cx<R>{0, 0};
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int t = lane + 32 * u;
+            if (t >= nrows) break;
 #pragma unroll
             for (int k = 0; k < 8; ++k)
-                if (k < a.nr) acc[k] = acc[k] + l * xs[k][t];
+                if (k < a.nr) acc[k] = acc[k] + l[u] * xs[k][t];
         }
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
@@ -828,6 +845,7 @@ __global__ void __launch_bounds__(256) k_bwd_diag(Sched S, long long item0, Solv
     const int f = S.first[s];
     const int jb = min(kSolveBlock, w - j0);
     const cx<R>* P = Lb + lstride * blockIdx.y + S.loff[s] + j0 + static_cast<long long>(j0) * m;
+#pragma unroll 4
     for (int e = threadIdx.x; e < jb * jb; e += blockDim.x) {
         const int i = e % jb, j = e / jb;
         T[i + j * kSolveBlock] = P[i + static_cast<long long>(j) * m];
