@@ -258,7 +258,7 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
     aphi_factor* fm = const_cast<aphi_factor*>(f);
     const bool prof = f->profile && !sa;
     for (const Launch& l : plan) {
-        dim3 grid(l.count, f->batch);
+        dim3 grid(l.count, sa && sa->ny > 0 ? sa->ny : f->batch);
         if (prof) {
             cudaEvent_t e[2];
             APHI_CUDA(cudaEventCreate(&e[0]));
@@ -385,7 +385,8 @@ void factorize_numeric(aphi_factor* f, const double* values, const double* panel
 }
 
 template <class R>
-void solve_numeric(aphi_factor* f, int nrhs, const double* b, double* x, cudaStream_t st) {
+void solve_numeric(aphi_factor* f, int nrhs, const double* b, double* x, cudaStream_t st, const int* entries,
+                   int nentries) {
     const aphi_analysis* A = f->an;
     const int n = A->S.n;
     if (f->nrhs_cap < nrhs) {
@@ -407,7 +408,8 @@ void solve_numeric(aphi_factor* f, int nrhs, const double* b, double* x, cudaStr
     k_permute_in<R><<<g, 256, 0, st>>>(n, nrhs, A->d.orig_of_new, f->dscale, b, y);
     APHI_CHECK_LAUNCH();
     for (int k0 = 0; k0 < nrhs; k0 += 8) {
-        const SolveArgs sa{n, nrhs, k0, std::min(8, nrhs - k0), A->upool, A->max_parts};
+        const SolveArgs sa{n, nrhs, k0, std::min(8, nrhs - k0), A->upool, A->max_parts, entries,
+                           entries ? nentries : 0};
         run_plan<R>(f, A->plan_fwd, st, &sa, y, U, part);
         run_plan<R>(f, A->plan_bwd, st, &sa, y, U, part);
     }
@@ -621,7 +623,10 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
     return any_fail ? APHI_ERR_PIVOT_FLOOR : APHI_OK;
 }
 
-void solve(aphi_factor* f, int nrhs, const double* b, double* x, cudaStream_t st) {
+// entries (device, nentries of them): solve only these batch entries; the
+// others' x is left holding their permuted, scaled b. Null: every entry.
+void solve(aphi_factor* f, int nrhs, const double* b, double* x, cudaStream_t st, const int* entries,
+           int nentries) {
     if (!f->factored) throw Error(APHI_ERR_INVALID, "solve: the factor holds no factorization");
     if (f->an->fronts) throw Error(APHI_ERR_INVALID, "solve: dense fronts have no system to solve");
     if (nrhs < 1) throw Error(APHI_ERR_BAD_SHAPE, "solve: nrhs must be at least 1");
@@ -631,9 +636,9 @@ void solve(aphi_factor* f, int nrhs, const double* b, double* x, cudaStream_t st
                         "solve_in_place: the factorization stopped at a pivot at or below the floor, so "
                         "this factor cannot be used.");
     if (f->precision == 64)
-        solve_numeric<double>(f, nrhs, b, x, st);
+        solve_numeric<double>(f, nrhs, b, x, st, entries, nentries);
     else
-        solve_numeric<float>(f, nrhs, b, x, st);
+        solve_numeric<float>(f, nrhs, b, x, st, entries, nentries);
 }
 
 // Per-thread device scratch that only grows: freeing device memory
@@ -1007,7 +1012,7 @@ int solve_krylov(aphi_factor* f, int nrhs, const double* values, const double* b
         // r, z, p, Ap; partials (3 per block per system); norms, rho, alpha,
         // beta; max|A| words; active flags -- sized for the capacity.
         const long long qc = static_cast<long long>(f->capacity) * nrhs;
-        f->kr = dalloc<double>(static_cast<size_t>(4 * 2LL * n * qc + 3LL * nb * qc + 11LL * qc + f->capacity + 16));
+        f->kr = dalloc<double>(static_cast<size_t>(4 * 2LL * n * qc + 3LL * nb * qc + 11LL * qc + 2LL * f->capacity + 16));
         f->kr_cap = nrhs;
     }
     double* r = f->kr;
@@ -1021,12 +1026,13 @@ int solve_krylov(aphi_factor* f, int nrhs, const double* values, const double* b
     double* beta = alpha + 2LL * q;             // 2 * q
     unsigned long long* amax = reinterpret_cast<unsigned long long*>(beta + 2LL * q);  // B
     int* active = reinterpret_cast<int*>(amax + B);                                   // q ints
+    int* entries = active + q;                                                        // B ints
     const dim3 gv(nb, q);
 
     APHI_CUDA(cudaMemsetAsync(amax, 0, sizeof(unsigned long long) * B, st));
     k_amax<<<dim3(ceil_div(std::max<long long>(A->S.nnz_a, 1), 256), B), 256, 0, st>>>(values, A->S.nnz_a, amax);
     APHI_CHECK_LAUNCH();
-    std::vector<int> act(q, 1), it(q, 0), since(q, 0);
+    std::vector<int> act(q, 1), it(q, 0), since(q, 0), ent;
     std::vector<double> h(4 * static_cast<size_t>(q)), best(q, INFINITY);
     APHI_CUDA(cudaMemcpyAsync(active, act.data(), sizeof(int) * q, cudaMemcpyHostToDevice, st));
 
@@ -1080,7 +1086,20 @@ int solve_krylov(aphi_factor* f, int nrhs, const double* values, const double* b
         }
         if (!any) break;
         APHI_CUDA(cudaMemcpyAsync(active, act.data(), sizeof(int) * q, cudaMemcpyHostToDevice, st));
-        solve(f, nrhs, r, z, st);  // z = M^-1 r
+        // The preconditioner solve runs over the entries with a system still
+        // iterating; a frozen system's z is never read again (its alpha and
+        // beta are zero and its updates are masked).
+        ent.clear();
+        for (int e = 0; e < B; ++e)
+            for (int k = 0; k < nrhs; ++k)
+                if (act[e * nrhs + k]) {
+                    ent.push_back(e);
+                    break;
+                }
+        const bool all = static_cast<int>(ent.size()) == B;
+        if (!all)
+            APHI_CUDA(cudaMemcpyAsync(entries, ent.data(), sizeof(int) * ent.size(), cudaMemcpyHostToDevice, st));
+        solve(f, nrhs, r, z, st, all ? nullptr : entries, static_cast<int>(ent.size()));  // z = M^-1 r
         if (!started) {
             APHI_CUDA(cudaMemcpyAsync(p, z, sizeof(double) * len, cudaMemcpyDeviceToDevice, st));
             dot(r, z, 0);

@@ -62,7 +62,8 @@ void factor_set_batch(aphi_factor* f, int batch);
 int factorize(aphi_factor* f, const double* values_dev, int equil_iters, double pivot_floor,
               aphi_factor_stats* stats, cudaStream_t stream, const double* panels_dev = nullptr);
 void fronts_read(const aphi_factor* f, int k, double* panels_out, double* cb_out, cudaStream_t stream);
-void solve(aphi_factor* f, int nrhs, const double* b_dev, double* x_dev, cudaStream_t stream);
+void solve(aphi_factor* f, int nrhs, const double* b_dev, double* x_dev, cudaStream_t stream,
+           const int* entries = nullptr, int nentries = 0);
 void factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, double* value,
                    double* diagonal, double* d_scale);
 void residuals(const aphi_analysis* an, int batch, int nrhs, const double* values_dev, const double* x_dev,

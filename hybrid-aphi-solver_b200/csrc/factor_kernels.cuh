@@ -661,7 +661,13 @@ struct SolveArgs {
     int k0, nr;    // the rhs handled by this pass
     long long upool;
     int max_parts;
+    const int* entries;  // grid.y -> batch entry (the entries still being solved); null: grid.y is the entry
+    int ny;              // grid.y of the solve launches (0: the factor's batch)
 };
+
+__device__ __forceinline__ int solve_entry(const SolveArgs& a) {
+    return a.entries ? a.entries[blockIdx.y] : static_cast<int>(blockIdx.y);
+}
 
 __device__ __forceinline__ long long vec_at(const SolveArgs& a, int b, int k) {
     return static_cast<long long>(b) * a.nrhs + (a.k0 + k);
@@ -669,14 +675,15 @@ __device__ __forceinline__ long long vec_at(const SolveArgs& a, int b, int k) {
 
 template <class R>
 __global__ void __launch_bounds__(256) k_fwd_gather(Sched S, long long item0, SolveArgs a, cx<R>* yb, cx<R>* Ub) {
+    const int eb = solve_entry(a);
     const int s = S.items[item0 + blockIdx.x].s;
     const int w = S.first[s + 1] - S.first[s];
     const int m = S.rows[s];
     const int cs = m - w;
     const int f = S.first[s];
     for (int k = 0; k < a.nr; ++k) {
-        cx<R>* y = yb + vec_at(a, blockIdx.y, k) * a.n;
-        cx<R>* U = Ub + vec_at(a, blockIdx.y, k) * a.upool;
+        cx<R>* y = yb + vec_at(a, eb, k) * a.n;
+        cx<R>* U = Ub + vec_at(a, eb, k) * a.upool;
         cx<R>* Us = U + S.uoff[s];
         for (int i = threadIdx.x; i < cs; i += blockDim.x) Us[i] = cx<R>{0, 0};
         __syncthreads();
@@ -699,6 +706,7 @@ __global__ void __launch_bounds__(256) k_fwd_gather(Sched S, long long item0, So
 template <class R>
 __global__ void __launch_bounds__(256) k_fwd_diag(Sched S, long long item0, SolveArgs a, const cx<R>* Lb,
                                                   long long lstride, cx<R>* yb) {
+    const int eb = solve_entry(a);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<R>* T = reinterpret_cast<cx<R>*>(smem_raw);
     cx<R>(*ys)[kSolveBlock] = reinterpret_cast<cx<R>(*)[kSolveBlock]>(T + kSolveBlock * kSolveBlock);
@@ -708,14 +716,14 @@ __global__ void __launch_bounds__(256) k_fwd_diag(Sched S, long long item0, Solv
     const int m = S.rows[s];
     const int f = S.first[s];
     const int jb = min(kSolveBlock, w - j0);
-    const cx<R>* P = Lb + lstride * blockIdx.y + S.loff[s] + j0 + static_cast<long long>(j0) * m;
+    const cx<R>* P = Lb + lstride * eb + S.loff[s] + j0 + static_cast<long long>(j0) * m;
 #pragma unroll 4
     for (int e = threadIdx.x; e < jb * jb; e += blockDim.x) {
         const int i = e % jb, j = e / jb;
         T[i + j * kSolveBlock] = P[i + static_cast<long long>(j) * m];
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    cx<R>* y = yb + vec_at(a, blockIdx.y, warp) * a.n + f + j0;
+    cx<R>* y = yb + vec_at(a, eb, warp) * a.n + f + j0;
     if (warp < a.nr)
         for (int i = lane; i < jb; i += 32) ys[warp][i] = y[i];
     __syncthreads();
@@ -732,6 +740,7 @@ __global__ void __launch_bounds__(256) k_fwd_diag(Sched S, long long item0, Solv
 template <class R>
 __global__ void __launch_bounds__(256) k_fwd_update(Sched S, long long item0, SolveArgs a, const cx<R>* Lb,
                                                     long long lstride, cx<R>* yb, cx<R>* Ub) {
+    const int eb = solve_entry(a);
     __shared__ cx<R> ys[8][kSolveBlock];
     const Item it = S.items[item0 + blockIdx.x];
     const int s = it.s, j0 = it.a * kSolveBlock, row0 = it.b;
@@ -741,12 +750,12 @@ __global__ void __launch_bounds__(256) k_fwd_update(Sched S, long long item0, So
     const int jb = min(kSolveBlock, w - j0);
     for (int e = threadIdx.x; e < jb * a.nr; e += blockDim.x) {
         const int j = e % jb, k = e / jb;
-        ys[k][j] = yb[vec_at(a, blockIdx.y, k) * a.n + f + j0 + j];
+        ys[k][j] = yb[vec_at(a, eb, k) * a.n + f + j0 + j];
     }
     __syncthreads();
     const int r = row0 + threadIdx.x;
     if (r >= m) return;
-    const cx<R>* P = Lb + lstride * blockIdx.y + S.loff[s] + r + static_cast<long long>(j0) * m;
+    const cx<R>* P = Lb + lstride * eb + S.loff[s] + r + static_cast<long long>(j0) * m;
     cx<R> acc[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) acc[k] = cx<R>{0, 0};
@@ -767,8 +776,8 @@ __global__ void __launch_bounds__(256) k_fwd_update(Sched S, long long item0, So
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         if (k >= a.nr) break;
-        cx<R>* dst = r < w ? yb + vec_at(a, blockIdx.y, k) * a.n + f + r
-                           : Ub + vec_at(a, blockIdx.y, k) * a.upool + S.uoff[s] + (r - w);
+        cx<R>* dst = r < w ? yb + vec_at(a, eb, k) * a.n + f + r
+                           : Ub + vec_at(a, eb, k) * a.upool + S.uoff[s] + (r - w);
         *dst = *dst - acc[k];
     }
 }
@@ -778,6 +787,7 @@ __global__ void __launch_bounds__(256) k_fwd_update(Sched S, long long item0, So
 template <class R>
 __global__ void __launch_bounds__(256) k_bwd_update(Sched S, long long item0, SolveArgs a, const cx<R>* Lb,
                                                     long long lstride, const cx<R>* yb, cx<R>* partb) {
+    const int eb = solve_entry(a);
     __shared__ cx<R> xs[8][kSolveRows];
     const Item it = S.items[item0 + blockIdx.x];
     const int s = it.s, j0 = it.a * kSolveBlock, row0 = it.b, slot = it.c;
@@ -791,12 +801,12 @@ __global__ void __launch_bounds__(256) k_bwd_update(Sched S, long long item0, So
         const int t = e % nrows, k = e / nrows;
         const int r = row0 + t;
         const int g = r < w ? f + r : st[r];
-        xs[k][t] = yb[vec_at(a, blockIdx.y, k) * a.n + g];
+        xs[k][t] = yb[vec_at(a, eb, k) * a.n + g];
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const cx<R>* P = Lb + lstride * blockIdx.y + S.loff[s] + row0 + static_cast<long long>(j0) * m;
-    cx<R>* part = partb + static_cast<long long>(blockIdx.y) * a.max_parts * kSolveBlock * 8 +
+    const cx<R>* P = Lb + lstride * eb + S.loff[s] + row0 + static_cast<long long>(j0) * m;
+    cx<R>* part = partb + static_cast<long long>(eb) * a.max_parts * kSolveBlock * 8 +
                   static_cast<long long>(slot) * kSolveBlock * 8;
     for (int j = warp; j < jb; j += 8) {
         const cx<R>* col = P + static_cast<long long>(j) * m;
@@ -835,6 +845,7 @@ __global__ void __launch_bounds__(256) k_bwd_update(Sched S, long long item0, So
 template <class R>
 __global__ void __launch_bounds__(256) k_bwd_diag(Sched S, long long item0, SolveArgs a, const cx<R>* Lb,
                                                   long long lstride, cx<R>* yb, const cx<R>* partb) {
+    const int eb = solve_entry(a);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<R>* T = reinterpret_cast<cx<R>*>(smem_raw);
     cx<R>(*zs)[kSolveBlock] = reinterpret_cast<cx<R>(*)[kSolveBlock]>(T + kSolveBlock * kSolveBlock);
@@ -844,19 +855,19 @@ __global__ void __launch_bounds__(256) k_bwd_diag(Sched S, long long item0, Solv
     const int m = S.rows[s];
     const int f = S.first[s];
     const int jb = min(kSolveBlock, w - j0);
-    const cx<R>* P = Lb + lstride * blockIdx.y + S.loff[s] + j0 + static_cast<long long>(j0) * m;
+    const cx<R>* P = Lb + lstride * eb + S.loff[s] + j0 + static_cast<long long>(j0) * m;
 #pragma unroll 4
     for (int e = threadIdx.x; e < jb * jb; e += blockDim.x) {
         const int i = e % jb, j = e / jb;
         T[i + j * kSolveBlock] = P[i + static_cast<long long>(j) * m];
     }
     __syncthreads();
-    const cx<R>* part = partb + static_cast<long long>(blockIdx.y) * a.max_parts * kSolveBlock * 8;
+    const cx<R>* part = partb + static_cast<long long>(eb) * a.max_parts * kSolveBlock * 8;
     for (int e = threadIdx.x; e < jb * a.nr; e += blockDim.x) {
         const int j = e % jb, k = e / jb;
         cx<R> sum{0, 0};
         for (int q = 0; q < np; ++q) sum = sum + part[(static_cast<long long>(p0 + q) * kSolveBlock + j) * 8 + k];
-        const cx<R> yv = yb[vec_at(a, blockIdx.y, k) * a.n + f + j0 + j];
+        const cx<R> yv = yb[vec_at(a, eb, k) * a.n + f + j0 + j];
         zs[k][j] = yv * crecip(T[j * (kSolveBlock + 1)]) - sum;
     }
     __syncthreads();
@@ -867,7 +878,7 @@ __global__ void __launch_bounds__(256) k_bwd_diag(Sched S, long long item0, Solv
         for (int t = lane; t < j; t += 32) zs[warp][t] = fms(zs[warp][t], T[j + t * kSolveBlock], xj);
         __syncwarp();
     }
-    cx<R>* y = yb + vec_at(a, blockIdx.y, warp) * a.n + f + j0;
+    cx<R>* y = yb + vec_at(a, eb, warp) * a.n + f + j0;
     for (int i = lane; i < jb; i += 32) y[i] = zs[warp][i];
 }
 
