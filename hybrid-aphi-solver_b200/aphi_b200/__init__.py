@@ -104,6 +104,11 @@ class IROptions(C.Structure):
     _fields_ = [("max_iters", I), ("tol", D), ("stall_ratio", D), ("krylov", I), ("rtol", D)]
 
 
+class FieldsOut(C.Structure):
+    _fields_ = [(name, P) for name in ("phi_node", "a_tet", "b_tet", "e_tet", "j_tet", "sigma_tet", "a_node",
+                                       "b_node", "h_node", "e_node", "j_node", "vertex_weight", "on_interface")]
+
+
 _SIGS = {
     "aphi_status_string": (C.c_char_p, [I]),
     "aphi_last_error": (C.c_char_p, []),
@@ -124,6 +129,10 @@ _SIGS = {
     "aphi_refill_host": (I, [P, D, I, PD, PD]),
     "aphi_element_blocks": (I, [I, PD, D, PD, PD, PD, PD, PD]),
     "aphi_element_coefficients": (None, [D, D, D, D, PD]),
+    "aphi_fields_create": (I, [P, I, I, PI, C.POINTER(P)]),
+    "aphi_fields_destroy": (I, [P]),
+    "aphi_fields_sizes": (I, [P, PI64]),
+    "aphi_fields_compute": (I, [P, D, I, P, C.POINTER(FieldsOut), P]),
     "aphi_analysis_default_options": (None, [C.POINTER(AnalysisOptions)]),
     "aphi_analysis_create": (I, [I, PI, PI, PI, PI, PI, C.POINTER(AnalysisOptions), C.POINTER(P)]),
     "aphi_analysis_destroy": (I, [P]),
@@ -264,6 +273,58 @@ class Workload:
             pass
 
 
+class Fields:
+    """Post-solve fields over an Assembly's mesh (compute_fields and
+    potential_at_nodes' values, src/postprocess.cpp:42-126, 223-486): per tet
+    A and E at the centroid, B = curl A, J = sigma E; per P2 node (vertices,
+    then edge midpoints) Phi and volume-weighted A, B, H, E, J. The Assembly
+    must stay alive as long as this object."""
+
+    def __init__(self, assembly, num_nodes: int, num_edges: int, tet_edges):
+        te = np.ascontiguousarray(tet_edges, np.int32)
+        if te.size != 6 * assembly.num_tets:
+            raise InvalidArgument(ERR_BAD_SHAPE, f"Fields: {te.size} tet edges for {assembly.num_tets} tets")
+        self.assembly = assembly
+        self._h = P()
+        check(lib().aphi_fields_create(assembly._h, num_nodes, num_edges, _ptr(te, C.c_int), C.byref(self._h)))
+        s = (C.c_int64 * 6)()
+        check(lib().aphi_fields_sizes(self._h, s))
+        self.num_tets, self.num_p2, self.num_vertices, self.num_edges, self.num_interface_nodes, \
+            self.num_orphans = list(s)
+
+    @classmethod
+    def of_workload(cls, assembly, w: "Workload") -> "Fields":
+        return cls(assembly, w.num_nodes, w.num_edges, w.tet_edges)
+
+    def compute(self, x, omega: float, conditioning: int = COND_ROW_SCALED, stream=None) -> dict:
+        """x: the solution, complex128 device tensor [N]. Returns device tensors."""
+        import torch
+        _expect_device(x, (self.assembly.num_unknowns,), "Fields.compute: x")
+        T, Pn = self.num_tets, self.num_p2
+        c = dict(dtype=torch.complex128, device="cuda")
+        out = {"phi_node": torch.empty(Pn, **c), "sigma_tet": torch.empty(T, dtype=torch.float64, device="cuda"),
+               "vertex_weight": torch.empty(Pn, dtype=torch.float64, device="cuda"),
+               "on_interface": torch.empty(Pn, dtype=torch.uint8, device="cuda")}
+        for k in ("a_tet", "b_tet", "e_tet", "j_tet"):
+            out[k] = torch.empty((T, 3), **c)
+        for k in ("a_node", "b_node", "h_node", "e_node", "j_node"):
+            out[k] = torch.empty((Pn, 3), **c)
+        fo = FieldsOut(**{k: dptr(v) for k, v in out.items()})
+        check(lib().aphi_fields_compute(self._h, omega, conditioning, dptr(x), C.byref(fo), stream_ptr(stream)))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().aphi_fields_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def assembly_desc_from(arrays: dict, upper_only: bool = True):
     """An AssemblyDesc over numpy arrays (kept alive by the returned tuple)."""
     keep = {}
@@ -366,6 +427,7 @@ class Assembly:
 
     def __init__(self, arrays: dict, upper_only: bool = True):
         desc, keep = assembly_desc_from(arrays, upper_only)
+        self.num_tets = int(desc.num_tets)
         self._h = P()
         check(lib().aphi_assembly_create(C.byref(desc), C.byref(self._h)))
         info = (C.c_int64 * 4)()

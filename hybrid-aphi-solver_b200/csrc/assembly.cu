@@ -25,6 +25,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #include "assembly.hpp"
@@ -714,6 +715,344 @@ void element_blocks_host(int ntets, const double* xyz, double nu, const double* 
     cudaFree(d_pp);
     cudaFree(d_err);
     if (err) throw Error(APHI_ERR_DEGENERATE_TET, "compute_tet_geometry: degenerate (zero-volume) tet");
+}
+
+// ---------------------------------------------------------------- post-solve fields
+// compute_fields and the potential of potential_at_nodes (src/postprocess.cpp:
+// 42-126, 223-486) on the device.
+//   k_field_tets: one thread per tet. Geometry, A's and Phi's coefficients
+//     for this tet (a cut's side already resolved by the tet's DOF table),
+//     B = curl A (constant), A and E = -j w A - grad Phi at the centroid and
+//     at each of the ten P2 nodes, J = sigma E. The node values go, with the
+//     tet's volume, to a contribution array.
+//   k_field_nodes: one thread per P2 node sums its contributions in
+//     increasing tet order -- the reference's accumulation order -- with the
+//     reference's side selection (E over the most conducting tets, B over the
+//     most permeable), normalises each by its own weight, and forms J and H.
+// Every operation is the reference's, in its order, rounded explicitly.
+namespace {
+
+constexpr int kFieldContrib = 13;  // volume, A (3 complex), E (3 complex)
+
+struct FieldArgs {
+    int T, P, nv;
+    const double* xyz;
+    const int* tets;
+    const int* tet_edges;
+    const int* body_of_tet;
+    const double* material;
+    const int* tet_idx;
+    const double* tet_coeff;
+    const double* tet_fixed;
+    const cplx* x;
+    cplx scale, mjw;
+    double* contrib;
+    const int* inc_ptr;
+    const int* inc;
+    const double* sig_max;
+    const double* mu_max;
+    const unsigned char* sig_uniform;
+    const unsigned char* mu_uniform;
+    int* err;
+};
+
+__device__ __forceinline__ void cross_rn(const double* a, const double* b, double* out) {
+    out[0] = __dsub_rn(__dmul_rn(a[1], b[2]), __dmul_rn(a[2], b[1]));
+    out[1] = __dsub_rn(__dmul_rn(a[2], b[0]), __dmul_rn(a[0], b[2]));
+    out[2] = __dsub_rn(__dmul_rn(a[0], b[1]), __dmul_rn(a[1], b[0]));
+}
+
+// A and E of one tet at barycentric point L.
+__device__ void field_at(const Geometry& g, const cplx (&a)[6], const double (&sgn)[6], const cplx (&ph)[10],
+                         cplx mjw, const double* L, cplx (&av)[3], cplx (&ev)[3]) {
+    cplx gp[3];
+    for (int i = 0; i < 3; ++i) av[i] = gp[i] = cplx{0.0, 0.0};
+    for (int k = 0; k < 6; ++k) {
+        double w[3];
+        whitney(g, k, L, w);
+        for (int i = 0; i < 3; ++i) av[i] = cadd_exact(av[i], cscale_exact(a[k], __dmul_rn(w[i], sgn[k])));
+    }
+    for (int n = 0; n < 10; ++n) {
+        double gr[3];
+        p2_grad(g, n, L, gr);
+        for (int i = 0; i < 3; ++i) gp[i] = cadd_exact(gp[i], cscale_exact(ph[n], gr[i]));
+    }
+    for (int i = 0; i < 3; ++i) {
+        const cplx t = cmul_exact(mjw, av[i]);
+        ev[i] = cplx{__dsub_rn(t.re, gp[i].re), __dsub_rn(t.im, gp[i].im)};
+    }
+}
+
+__global__ void __launch_bounds__(128) k_field_tets(FieldArgs A, cplx* a_tet, cplx* b_tet, cplx* e_tet, cplx* j_tet,
+                                                    double* sigma_tet) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= A.T) return;
+    double p[4][3];
+    for (int q = 0; q < 4; ++q) {
+        const int node = A.tets[4LL * t + q];
+        for (int k = 0; k < 3; ++k) p[q][k] = A.xyz[3LL * node + k];
+    }
+    Geometry g;
+    if (!tet_geometry(p, g)) {
+        atomicExch(A.err, 1);
+        return;
+    }
+    // A: the raw global unknown of each live edge; the edge sign goes with the
+    // basis function (whitney_edge_value_global).
+    cplx a[6];
+    double sgn[6];
+    for (int k = 0; k < 6; ++k) {
+        const int idx = A.tet_idx[16LL * t + k];
+        sgn[k] = A.tet_coeff[16LL * t + k];
+        a[k] = idx >= 0 ? A.x[idx] : cplx{0.0, 0.0};
+    }
+    // Phi: (scale * coeff) * x for an unknown, the prescribed value otherwise.
+    cplx ph[10];
+    for (int n = 0; n < 10; ++n) {
+        const int idx = A.tet_idx[16LL * t + 6 + n];
+        if (idx >= 0)
+            ph[n] = cmul_exact(cscale_exact(A.scale, A.tet_coeff[16LL * t + 6 + n]), A.x[idx]);
+        else
+            ph[n] = cplx{A.tet_fixed[20LL * t + 2 * n], A.tet_fixed[20LL * t + 2 * n + 1]};
+    }
+    // B = curl A = sum_e a_e * 2 (grad L_i x grad L_j) * sign_e.
+    cplx b[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    for (int k = 0; k < 6; ++k) {
+        double c[3];
+        cross_rn(g.grad[c_edge_verts[k][0]], g.grad[c_edge_verts[k][1]], c);
+        for (int i = 0; i < 3; ++i) b[i] = cadd_exact(b[i], cscale_exact(a[k], __dmul_rn(__dmul_rn(c[i], 2.0), sgn[k])));
+    }
+    const int body = A.body_of_tet[t];
+    const double sigma = A.material[3 * body];
+    sigma_tet[t] = sigma;
+    cplx av[3], ev[3];
+    const double Lc[4] = {0.25, 0.25, 0.25, 0.25};
+    field_at(g, a, sgn, ph, A.mjw, Lc, av, ev);
+    for (int i = 0; i < 3; ++i) {
+        a_tet[3LL * t + i] = av[i];
+        b_tet[3LL * t + i] = b[i];
+        e_tet[3LL * t + i] = ev[i];
+        j_tet[3LL * t + i] = cscale_exact(ev[i], sigma);
+    }
+    const double vol = g.volume;
+    for (int k = 0; k < 10; ++k) {
+        double L[4] = {0.0, 0.0, 0.0, 0.0};
+        if (k < 4) {
+            L[k] = 1.0;
+        } else {
+            L[c_edge_verts[k - 4][0]] = 0.5;
+            L[c_edge_verts[k - 4][1]] = 0.5;
+        }
+        field_at(g, a, sgn, ph, A.mjw, L, av, ev);
+        double* o = A.contrib + (10LL * t + k) * kFieldContrib;
+        o[0] = vol;
+        for (int i = 0; i < 3; ++i) {
+            o[1 + 2 * i] = av[i].re;
+            o[2 + 2 * i] = av[i].im;
+            o[7 + 2 * i] = ev[i].re;
+            o[8 + 2 * i] = ev[i].im;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_field_nodes(FieldArgs A, const cplx* b_tet, const double* sigma_tet,
+                                                     cplx* phi_node, cplx* a_node, cplx* b_node, cplx* h_node,
+                                                     cplx* e_node, cplx* j_node, double* vertex_weight,
+                                                     unsigned char* on_interface) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= A.P) return;
+    const bool sig_u = A.sig_uniform[u] != 0, mu_u = A.mu_uniform[u] != 0;
+    double vw = 0.0, ew = 0.0, bw = 0.0;
+    cplx an[3], en[3], bn[3];
+    for (int i = 0; i < 3; ++i) an[i] = en[i] = bn[i] = cplx{0.0, 0.0};
+    cplx phi{0.0, 0.0};
+    bool phi_unknown = false, phi_fixed = false;
+    for (int q = A.inc_ptr[u]; q < A.inc_ptr[u + 1]; ++q) {
+        const int e = A.inc[q];
+        const int t = e / 10, k = e % 10;
+        const double* c = A.contrib + static_cast<long long>(e) * kFieldContrib;
+        const double vol = c[0];
+        vw = __dadd_rn(vw, vol);
+        for (int i = 0; i < 3; ++i) an[i] = cadd_exact(an[i], cscale_exact(cplx{c[1 + 2 * i], c[2 + 2 * i]}, vol));
+        if (sig_u || sigma_tet[t] == A.sig_max[u]) {
+            ew = __dadd_rn(ew, vol);
+            for (int i = 0; i < 3; ++i) en[i] = cadd_exact(en[i], cscale_exact(cplx{c[7 + 2 * i], c[8 + 2 * i]}, vol));
+        }
+        const double mu = __dmul_rn(kMu0, A.material[3 * A.body_of_tet[t] + 2]);
+        if (mu_u || mu == A.mu_max[u]) {
+            bw = __dadd_rn(bw, vol);
+            for (int i = 0; i < 3; ++i) bn[i] = cadd_exact(bn[i], cscale_exact(b_tet[3LL * t + i], vol));
+        }
+        // Phi at the node: the unknown any incident tet reads (a cut's plus
+        // side), else the first nonzero prescribed value.
+        {
+            const int idx = A.tet_idx[16LL * t + 6 + k];
+            if (idx >= 0 && !phi_unknown) {
+                phi = cmul_exact(A.scale, A.x[idx]);
+                phi_unknown = true;
+            } else if (idx < 0 && !phi_unknown && !phi_fixed) {
+                const cplx f{A.tet_fixed[20LL * t + 2 * k], A.tet_fixed[20LL * t + 2 * k + 1]};
+                if (f.re != 0.0 || f.im != 0.0) {
+                    phi = f;
+                    phi_fixed = true;
+                }
+            }
+        }
+    }
+    phi_node[u] = phi;
+    vertex_weight[u] = vw;
+    on_interface[u] = (A.inc_ptr[u + 1] > A.inc_ptr[u]) && (!sig_u || !mu_u) ? 1 : 0;
+    if (vw > 0.0) {
+        for (int i = 0; i < 3; ++i) an[i] = cplx{__ddiv_rn(an[i].re, vw), __ddiv_rn(an[i].im, vw)};
+        if (ew > 0.0)
+            for (int i = 0; i < 3; ++i) en[i] = cplx{__ddiv_rn(en[i].re, ew), __ddiv_rn(en[i].im, ew)};
+        if (bw > 0.0)
+            for (int i = 0; i < 3; ++i) bn[i] = cplx{__ddiv_rn(bn[i].re, bw), __ddiv_rn(bn[i].im, bw)};
+    }
+    const double nu_node = vw > 0.0 ? __ddiv_rn(1.0, A.mu_max[u]) : 0.0;
+    const double smax = vw > 0.0 ? A.sig_max[u] : 0.0;
+    for (int i = 0; i < 3; ++i) {
+        a_node[3LL * u + i] = an[i];
+        e_node[3LL * u + i] = en[i];
+        b_node[3LL * u + i] = bn[i];
+        j_node[3LL * u + i] = vw > 0.0 ? cscale_exact(en[i], smax) : cplx{0.0, 0.0};
+        h_node[3LL * u + i] = vw > 0.0 ? cscale_exact(bn[i], nu_node) : cplx{0.0, 0.0};
+    }
+}
+
+}  // namespace
+
+Fields::~Fields() {
+    for (void* p : {(void*)d_tet_edges, (void*)d_body_of_tet, (void*)d_inc_ptr, (void*)d_inc, (void*)d_sig_max,
+                    (void*)d_mu_max, (void*)d_sig_uniform, (void*)d_mu_uniform, (void*)d_contrib, (void*)d_err})
+        if (p) cudaFree(p);
+}
+
+std::unique_ptr<Fields> fields_create(const Assembly& A, int num_nodes, int num_edges, const int* tet_edges) {
+    if (num_nodes < 1 || num_edges < 0 || (A.T > 0 && !tet_edges))
+        throw Error(APHI_ERR_BAD_SHAPE, "fields: need the mesh's node and edge counts and 6 edges per tet");
+    auto F = std::make_unique<Fields>();
+    F->A = &A;
+    F->T = A.T;
+    F->nv = num_nodes;
+    F->ne = num_edges;
+    F->P = num_nodes + num_edges;
+    const int T = A.T, P = F->P;
+    std::vector<int> tets(4LL * T), visit_tet(T), visit_body(T);
+    std::vector<double> material(3LL * A.num_bodies);
+    APHI_CUDA(cudaMemcpy(tets.data(), A.d_tets, tets.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    APHI_CUDA(cudaMemcpy(visit_tet.data(), A.d_visit_tet, visit_tet.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    APHI_CUDA(cudaMemcpy(visit_body.data(), A.d_visit_body, visit_body.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    APHI_CUDA(cudaMemcpy(material.data(), A.d_material, material.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<int> body_of_tet(T, -1);
+    for (int v = 0; v < T; ++v) body_of_tet[visit_tet[v]] = visit_body[v];
+    for (int t = 0; t < T; ++t) {
+        if (body_of_tet[t] < 0) throw Error(APHI_ERR_BAD_SHAPE, "fields: a tet belongs to no body");
+        for (int q = 0; q < 4; ++q)
+            if (tets[4LL * t + q] < 0 || tets[4LL * t + q] >= num_nodes)
+                throw Error(APHI_ERR_BAD_SHAPE, "fields: a tet names a node past num_nodes");
+        for (int q = 0; q < 6; ++q)
+            if (tet_edges[6LL * t + q] < 0 || tet_edges[6LL * t + q] >= num_edges)
+                throw Error(APHI_ERR_BAD_SHAPE, "fields: a tet names an edge past num_edges");
+    }
+    // P2 node -> (tet, local node) in increasing tet order, and each node's
+    // extreme conductivity and permeability over its tets.
+    auto node_of = [&](int t, int k) { return k < 4 ? tets[4LL * t + k] : num_nodes + tet_edges[6LL * t + k - 4]; };
+    std::vector<int> ptr(P + 1, 0);
+    constexpr double kInf = std::numeric_limits<double>::infinity();
+    std::vector<double> smin(P, kInf), smax(P, -kInf), mmin(P, kInf), mmax(P, -kInf);
+    for (int t = 0; t < T; ++t) {
+        const double s = material[3 * body_of_tet[t]], m = kMu0 * material[3 * body_of_tet[t] + 2];
+        for (int k = 0; k < 10; ++k) {
+            const int u = node_of(t, k);
+            ++ptr[u + 1];
+            smin[u] = std::min(smin[u], s);
+            smax[u] = std::max(smax[u], s);
+            mmin[u] = std::min(mmin[u], m);
+            mmax[u] = std::max(mmax[u], m);
+        }
+    }
+    for (int u = 0; u < P; ++u) ptr[u + 1] += ptr[u];
+    std::vector<int> inc(ptr[P]), cur(ptr.begin(), ptr.end() - 1);
+    for (int t = 0; t < T; ++t)
+        for (int k = 0; k < 10; ++k) inc[cur[node_of(t, k)]++] = 10 * t + k;
+    std::vector<unsigned char> su(P), mu(P);
+    for (int u = 0; u < P; ++u) {
+        su[u] = smin[u] == smax[u];
+        mu[u] = mmin[u] == mmax[u];
+        if (ptr[u + 1] == ptr[u]) {
+            ++F->orphans;
+            smax[u] = mmax[u] = 1.0;  // no tet: never read
+        } else if (!su[u] || !mu[u]) {
+            ++F->interface_nodes;
+        }
+    }
+    F->d_tet_edges = upload(tet_edges, 6LL * T);
+    F->d_body_of_tet = upload(body_of_tet.data(), body_of_tet.size());
+    F->d_inc_ptr = upload(ptr.data(), ptr.size());
+    F->d_inc = upload(inc.data(), inc.size());
+    F->d_sig_max = upload(smax.data(), smax.size());
+    F->d_mu_max = upload(mmax.data(), mmax.size());
+    F->d_sig_uniform = upload(su.data(), su.size());
+    F->d_mu_uniform = upload(mu.data(), mu.size());
+    APHI_CUDA(cudaMalloc(&F->d_contrib, std::max<size_t>(1, 10ULL * T * kFieldContrib) * sizeof(double)));
+    APHI_CUDA(cudaMalloc(&F->d_err, sizeof(int)));
+    APHI_CUDA(cudaMemset(F->d_err, 0, sizeof(int)));
+    return F;
+}
+
+void fields_compute(Fields& F, double omega, int conditioning, const double* x, const FieldsOut& o, cudaStream_t st) {
+    const Assembly& A = *F.A;
+    if (!x || !o.phi_node || !o.a_tet || !o.b_tet || !o.e_tet || !o.j_tet || !o.sigma_tet || !o.a_node ||
+        !o.b_node || !o.h_node || !o.e_node || !o.j_node || !o.vertex_weight || !o.on_interface)
+        throw Error(APHI_ERR_INVALID, "fields: null solution or output array");
+    if (conditioning != APHI_COND_NATURAL && conditioning != APHI_COND_ROW_SCALED && conditioning != APHI_COND_SCALED_PHI)
+        throw Error(APHI_ERR_BAD_SHAPE, "fields: unknown conditioning");
+    // Member by member: a braced initializer here (with the conditional
+    // complex scale) crashed the device front end of CUDA 12.9.
+    FieldArgs fa;
+    fa.T = F.T;
+    fa.P = F.P;
+    fa.nv = F.nv;
+    fa.xyz = A.d_xyz;
+    fa.tets = A.d_tets;
+    fa.tet_edges = F.d_tet_edges;
+    fa.body_of_tet = F.d_body_of_tet;
+    fa.material = A.d_material;
+    fa.tet_idx = A.d_tet_idx;
+    fa.tet_coeff = A.d_tet_coeff;
+    fa.tet_fixed = A.d_tet_fixed;
+    fa.x = reinterpret_cast<const cplx*>(x);
+    fa.scale.re = conditioning == APHI_COND_SCALED_PHI ? 0.0 : 1.0;  // j omega under ScaledPhi
+    fa.scale.im = conditioning == APHI_COND_SCALED_PHI ? omega : 0.0;
+    fa.mjw.re = -0.0;                                                 // -(j omega)
+    fa.mjw.im = -omega;
+    fa.contrib = F.d_contrib;
+    fa.inc_ptr = F.d_inc_ptr;
+    fa.inc = F.d_inc;
+    fa.sig_max = F.d_sig_max;
+    fa.mu_max = F.d_mu_max;
+    fa.sig_uniform = F.d_sig_uniform;
+    fa.mu_uniform = F.d_mu_uniform;
+    fa.err = F.d_err;
+    if (F.T > 0) {
+        k_field_tets<<<ceil_div(F.T, 128), 128, 0, st>>>(fa, reinterpret_cast<cplx*>(o.a_tet),
+                                                        reinterpret_cast<cplx*>(o.b_tet), reinterpret_cast<cplx*>(o.e_tet),
+                                                        reinterpret_cast<cplx*>(o.j_tet), o.sigma_tet);
+        APHI_CHECK_LAUNCH();
+    }
+    k_field_nodes<<<ceil_div(std::max(F.P, 1), 256), 256, 0, st>>>(
+        fa, reinterpret_cast<const cplx*>(o.b_tet), o.sigma_tet, reinterpret_cast<cplx*>(o.phi_node),
+        reinterpret_cast<cplx*>(o.a_node), reinterpret_cast<cplx*>(o.b_node), reinterpret_cast<cplx*>(o.h_node),
+        reinterpret_cast<cplx*>(o.e_node), reinterpret_cast<cplx*>(o.j_node), o.vertex_weight, o.on_interface);
+    APHI_CHECK_LAUNCH();
+    int err = 0;
+    APHI_CUDA(cudaMemcpyAsync(&err, F.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    APHI_CUDA(cudaStreamSynchronize(st));
+    if (err) {
+        APHI_CUDA(cudaMemsetAsync(F.d_err, 0, sizeof(int), st));
+        throw Error(APHI_ERR_DEGENERATE_TET, "compute_fields: degenerate (zero-volume) tet");
+    }
 }
 
 }  // namespace aphi_b200

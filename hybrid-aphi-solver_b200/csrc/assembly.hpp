@@ -41,6 +41,28 @@ struct Assembly {
     ~Assembly();
 };
 
+// Post-solve fields over an assembly's mesh (compute_fields, src/postprocess.cpp:223-486).
+struct Fields {
+    const Assembly* A = nullptr;  // must outlive the Fields
+    int T = 0, P = 0, nv = 0, ne = 0;
+    int interface_nodes = 0, orphans = 0;
+    int* d_tet_edges = nullptr;
+    int* d_body_of_tet = nullptr;
+    int* d_inc_ptr = nullptr;  // P2 node -> 10 * tet + local node, increasing tet
+    int* d_inc = nullptr;
+    double* d_sig_max = nullptr;
+    double* d_mu_max = nullptr;
+    unsigned char* d_sig_uniform = nullptr;
+    unsigned char* d_mu_uniform = nullptr;
+    double* d_contrib = nullptr;
+    int* d_err = nullptr;
+    ~Fields();
+};
+using FieldsOut = aphi_fields_out;
+std::unique_ptr<Fields> fields_create(const Assembly& A, int num_nodes, int num_edges, const int* tet_edges);
+void fields_compute(Fields& F, double omega, int conditioning, const double* x_dev, const FieldsOut& out,
+                    cudaStream_t stream);
+
 std::unique_ptr<Assembly> assembly_create(const aphi_assembly_desc& d);
 void assembly_refill(Assembly& A, int nfreq, const double* omegas, int cond, double* values_dev,
                      double* rhs_dev, cudaStream_t stream);

@@ -19,6 +19,10 @@ struct aphi_assembly {
     std::unique_ptr<Assembly> a;
 };
 
+struct aphi_fields {
+    std::unique_ptr<Fields> f;
+};
+
 #include <atomic>
 
 namespace aphi_b200 {
@@ -228,6 +232,46 @@ int aphi_refill_host(aphi_assembly* h, double omega, int conditioning, double* v
         }
         cudaFree(dv);
         cudaFree(dr);
+    });
+}
+
+int aphi_fields_create(const aphi_assembly* a, int num_nodes, int num_edges, const int* tet_edges,
+                       aphi_fields** out) {
+    return guard([&] {
+        if (!a || !out) throw Error(APHI_ERR_INVALID, "aphi_fields_create: null argument");
+        auto* h = new aphi_fields;
+        try {
+            h->f = fields_create(*a->a, num_nodes, num_edges, tet_edges);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int aphi_fields_destroy(aphi_fields* f) {
+    return guard([&] { delete f; });
+}
+
+int aphi_fields_sizes(const aphi_fields* h, int64_t* s) {
+    return guard([&] {
+        if (!h || !s) throw Error(APHI_ERR_INVALID, "aphi_fields_sizes: null argument");
+        const Fields& F = *h->f;
+        s[0] = F.T;
+        s[1] = F.P;
+        s[2] = F.nv;
+        s[3] = F.ne;
+        s[4] = F.interface_nodes;
+        s[5] = F.orphans;
+    });
+}
+
+int aphi_fields_compute(aphi_fields* h, double omega, int conditioning, const double* x_dev,
+                        const aphi_fields_out* out, void* stream) {
+    return guard([&] {
+        if (!h || !out) throw Error(APHI_ERR_INVALID, "aphi_fields_compute: null argument");
+        fields_compute(*h->f, omega, conditioning, x_dev, *out, static_cast<cudaStream_t>(stream));
     });
 }
 

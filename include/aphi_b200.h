@@ -157,6 +157,45 @@ int aphi_element_blocks(int ntets, const double* xyz, double nu, const double* a
 /* Element coefficients nu, alpha, beta (5 doubles) -- src/element_matrix.cpp:10-25. */
 void aphi_element_coefficients(double sigma, double eps_r, double mu_r, double omega, double* out5);
 
+/* ---- post-solve fields ----------------------------------------------------
+ * compute_fields (src/postprocess.cpp:223-486, include/aphi_solver/
+ * postprocess.hpp:298) and potential_at_nodes' values (:42-126) on the device,
+ * over an assembly's mesh and DOF tables. P2 nodes are numbered as DofMap
+ * numbers them: the mesh's vertices, then one per edge. Per tet: A and E at
+ * the centroid, B = curl A (constant), J = sigma E, sigma. Per P2 node: Phi
+ * (the plus side on a cut), and A, B, H, E, J averaged over the node's tets
+ * with their volumes as weights -- E and J over the most conducting tets, B
+ * and H over the most permeable -- in the reference's tet order. Complex
+ * arrays are interleaved (re, im); vector fields are 3 complex per entry.
+ * All outputs are device arrays the caller owns. */
+typedef struct aphi_fields aphi_fields;
+typedef struct {
+    double* phi_node;              /* P complex */
+    double* a_tet;                 /* T x 3 complex */
+    double* b_tet;
+    double* e_tet;
+    double* j_tet;
+    double* sigma_tet;             /* T */
+    double* a_node;                /* P x 3 complex */
+    double* b_node;
+    double* h_node;
+    double* e_node;
+    double* j_node;
+    double* vertex_weight;         /* P: summed volume of each node's tets */
+    unsigned char* on_interface;   /* P: 1 where the node's tets are not all one material */
+} aphi_fields_out;
+/* tet_edges: 6 global edge numbers per tet (host, the mesh's tet_edges);
+ * num_nodes / num_edges: the mesh's. The assembly must outlive the fields. */
+int aphi_fields_create(const aphi_assembly* a, int num_nodes, int num_edges, const int* tet_edges,
+                       aphi_fields** out);
+int aphi_fields_destroy(aphi_fields* f);
+/* sizes[0..5]: tets T, P2 nodes P, vertices, edges, interface nodes, nodes without a tet */
+int aphi_fields_sizes(const aphi_fields* f, int64_t* sizes);
+/* x_dev: the solution, N complex, laid out [a | phi | V]; conditioning as in
+ * the solve (ScaledPhi's unknown is Phi / (j omega)). */
+int aphi_fields_compute(aphi_fields* f, double omega, int conditioning, const double* x_dev,
+                        const aphi_fields_out* out, void* stream);
+
 /* ---- analysis: supernodal schedule from the reference's symbolic pass -----
  * Consumes the pattern and the reference's permutation (SolverAnalysis::
  * permutation, include/aphi_solver/symbolic.hpp:69-92), recomputes the

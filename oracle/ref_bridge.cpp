@@ -25,6 +25,7 @@
 #include "aphi_solver/assembly.hpp"
 #include "aphi_solver/equilibration.hpp"
 #include "aphi_solver/factorization.hpp"
+#include "aphi_solver/postprocess.hpp"
 #include "aphi_solver/symbolic.hpp"
 
 using namespace aphi_solver;
@@ -547,6 +548,47 @@ int ref_element_blocks(const double* xyz, double sigma, double eps_r, double mu_
         for (int i = 0; i < 36; ++i) { aa[2 * i] = a1[i].real(); aa[2 * i + 1] = a1[i].imag(); }
         for (int i = 0; i < 60; ++i) { ap[2 * i] = a2[i].real(); ap[2 * i + 1] = a2[i].imag(); }
         for (int i = 0; i < 100; ++i) { pp[2 * i] = a3[i].real(); pp[2 * i + 1] = a3[i].imag(); }
+        return 0;
+    });
+}
+
+/// The reference's compute_fields on solution x (complex, n), copied out:
+/// per tet a/b/e/j (3 complex each) and sigma; per P2 node phi (complex),
+/// a/b/h/e/j (3 complex each), vertex_weight and on_material_interface;
+/// counts[0..1] = num_interface_nodes, num_orphan_vertices.
+int ref_compute_fields(void* h, const double* x, double omega, int conditioning, double* phi_node, double* a_tet,
+                       double* b_tet, double* e_tet, double* j_tet, double* sigma_tet, double* a_node,
+                       double* b_node, double* h_node, double* e_node, double* j_node, double* vertex_weight,
+                       unsigned char* on_interface, int* counts) {
+    return guarded([&] {
+        auto* p = static_cast<RefProblem*>(h);
+        Solution sol;
+        to_complex(x, static_cast<std::size_t>(p->dofs.num_total), sol.x);
+        sol.omega = omega;
+        sol.conditioning = static_cast<Conditioning>(conditioning);
+        const FieldOutput f = compute_fields(p->mesh, p->bound, p->dofs, sol);
+        auto put3 = [](const std::vector<Vec3C>& v, double* out) {
+            for (std::size_t i = 0; i < v.size(); ++i)
+                for (int k = 0; k < 3; ++k) {
+                    out[6 * i + 2 * k] = v[i][static_cast<std::size_t>(k)].real();
+                    out[6 * i + 2 * k + 1] = v[i][static_cast<std::size_t>(k)].imag();
+                }
+        };
+        from_complex(f.phi_node, phi_node);
+        put3(f.a_tet, a_tet);
+        put3(f.b_tet, b_tet);
+        put3(f.e_tet, e_tet);
+        put3(f.j_tet, j_tet);
+        std::copy(f.sigma_tet.begin(), f.sigma_tet.end(), sigma_tet);
+        put3(f.a_node, a_node);
+        put3(f.b_node, b_node);
+        put3(f.h_node, h_node);
+        put3(f.e_node, e_node);
+        put3(f.j_node, j_node);
+        std::copy(f.vertex_weight.begin(), f.vertex_weight.end(), vertex_weight);
+        std::copy(f.on_material_interface.begin(), f.on_material_interface.end(), on_interface);
+        counts[0] = f.num_interface_nodes;
+        counts[1] = f.num_orphan_vertices;
         return 0;
     });
 }

@@ -42,6 +42,7 @@ def ref() -> C.CDLL:
         L.ref_factorize.argtypes = [vp, C.c_double, vp, vp, vp, vp, vp]
         L.ref_element_blocks.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double, vp, vp, vp]
         L.ref_body_tets.argtypes = [vp, C.c_int, vp]
+        L.ref_compute_fields.argtypes = [vp, vp, C.c_double, C.c_int] + [vp] * 14
         _ref = L
     return _ref
 
@@ -94,6 +95,25 @@ class RefProblem:
         a = [np.zeros(self.n, np.int32) for _ in range(4)]
         ref().ref_analysis(self.h, *map(_p, a))
         return dict(perm=a[0], iperm=a[1], parent=a[2], col_count=a[3])
+
+    def compute_fields(self, x: np.ndarray, omega: float, conditioning: int = 1) -> dict:
+        """The reference's compute_fields on solution x (complex128, n)."""
+        x = np.ascontiguousarray(x, np.complex128)
+        T, P = self.num_tets, self.num_nodes + self.num_edges
+        out = {"phi_node": np.zeros(P, np.complex128), "sigma_tet": np.zeros(T),
+               "vertex_weight": np.zeros(P), "on_interface": np.zeros(P, np.uint8)}
+        for k in ("a_tet", "b_tet", "e_tet", "j_tet"):
+            out[k] = np.zeros((T, 3), np.complex128)
+        for k in ("a_node", "b_node", "h_node", "e_node", "j_node"):
+            out[k] = np.zeros((P, 3), np.complex128)
+        counts = np.zeros(2, np.int32)
+        order = ["phi_node", "a_tet", "b_tet", "e_tet", "j_tet", "sigma_tet", "a_node", "b_node", "h_node",
+                 "e_node", "j_node", "vertex_weight", "on_interface"]
+        rc = ref().ref_compute_fields(self.h, _p(x), omega, conditioning, *[_p(out[k]) for k in order], _p(counts))
+        if rc != 0:
+            raise RuntimeError("reference: " + ref().ref_last_error().decode())
+        out["num_interface_nodes"], out["num_orphan_vertices"] = int(counts[0]), int(counts[1])
+        return out
 
     def tet_dofs(self):
         t = self.num_tets
