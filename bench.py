@@ -99,10 +99,8 @@ class Clocks:
 
 
 def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    from aphi_b200.replicas import dist_env as env
+    return env()
 
 
 # ---------------------------------------------------------------- CPU arm
@@ -194,10 +192,8 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
 
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
+    from aphi_b200 import replicas
+    barrier = replicas.barrier
 
     # Host-side per-mesh setup (untimed, once): workload, ordering, analysis.
     w = ab.Workload.cylinder(args.cells)
@@ -210,7 +206,7 @@ def run_ours(args):
     asm = ab.Assembly(ab.workload_arrays(w))
     n = an.n
     # Each rank solves its own sweep: the frequencies shifted per rank.
-    omegas = 2 * np.pi * np.geomspace(F_LO, F_HI, args.nfreq) * (1.0 + 1e-3 * rank)
+    omegas = replicas.rank_omegas(rank, args.nfreq, F_LO, F_HI)
     stream = torch.cuda.current_stream()
 
     solver = ab.SweepSolver(an, asm, args.nfreq, "mixed", fp64_batch=args.fp64_batch, rtol=args.rtol,
@@ -244,19 +240,14 @@ def run_ours(args):
             step_ms.append(s0.elapsed_time(s1))
         t1.record(stream)
         torch.cuda.synchronize()
+        barrier()
     torch.cuda.nvtx.range_pop()
     launches = (ab.launch_count() - launches0) // max(args.steps, 1)
     kind_ms = solver.profile_read()
     entries = {"fp32": solver.factorized[ab.PREC_FP32], "fp64": solver.factorized[ab.PREC_FP64]}
     solver.profile(False)
-    elapsed = t0.elapsed_time(t1)
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = t0.elapsed_time(t1)   # this rank's; the job's is the slowest rank's (below)
     res = ab.residuals(an, vals, x, rhs)
-    value = world * args.nfreq * args.steps / (elapsed / 1000.0)
 
     # The dominant kernel of the timed steps and its roofline: useful
     # Schur-update flops (lower-triangle entries of the fronts, 8 real flops
@@ -300,14 +291,15 @@ def run_ours(args):
 
     e2e_step()
     torch.cuda.synchronize()
+    barrier()
     a, b = ev(), ev()
     a.record(stream)
     for _ in range(args.steps):
         e2e_step()
     b.record(stream)
     torch.cuda.synchronize()
+    barrier()
     e2e_ms = a.elapsed_time(b) / args.steps
-    e2e_value = world * args.nfreq / (e2e_ms / 1000.0)
     h2d = 2 * (host_vals.numel() + host_rhs.numel()) * 8
     d2h = 2 * (host_vals.numel() + host_rhs.numel() + host_x.numel()) * 8
 
@@ -319,15 +311,22 @@ def run_ours(args):
     fp64 = ab.SweepSolver(an, asm, args.nfreq, "fp64", fp64_batch=args.fp64_batch)
     fp64.solve(omegas, stream=stream)
     torch.cuda.synchronize()
+    barrier()
     a, b = ev(), ev()
     a.record(stream)
     for _ in range(args.fp64_steps):
         x64, vals64, rhs64, _ = fp64.solve(omegas, stream=stream)
     b.record(stream)
     torch.cuda.synchronize()
+    barrier()
     fp64_ms = a.elapsed_time(b) / args.fp64_steps
     res64 = ab.residuals(an, vals64, x64, rhs64)
-    fp64_value = world * args.nfreq / (fp64_ms / 1000.0)
+
+    # The job's figures are the slowest rank's: one max-over-ranks reduction.
+    elapsed, e2e_ms, fp64_ms = replicas.max_over_ranks([elapsed, e2e_ms, fp64_ms], device=dev)
+    value = replicas.job_rate(world, args.nfreq * args.steps, elapsed)
+    e2e_value = replicas.job_rate(world, args.nfreq, e2e_ms)
+    fp64_value = replicas.job_rate(world, args.nfreq, fp64_ms)
     fp64.close()
     del fp64
 
