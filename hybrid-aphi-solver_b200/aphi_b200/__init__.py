@@ -129,6 +129,7 @@ _SIGS = {
     "aphi_refill_host": (I, [P, D, I, PD, PD]),
     "aphi_element_blocks": (I, [I, PD, D, PD, PD, PD, PD, PD]),
     "aphi_element_coefficients": (None, [D, D, D, D, PD]),
+    "aphi_selftest_bounded_wait": (I, [C.c_longlong]),
     "aphi_fields_create": (I, [P, I, I, PI, C.POINTER(P)]),
     "aphi_fields_destroy": (I, [P]),
     "aphi_fields_sizes": (I, [P, PI64]),
@@ -756,6 +757,12 @@ def measure_peaks() -> dict:
     out = np.zeros(5)
     check(lib().aphi_measure_peaks(out.ctypes.data_as(PD)))
     return dict(zip(["fp64_dmma", "fp64_dfma", "fp32_ffma", "tf32_tc_n64", "tf32_tc_n256"], out.tolist()))
+
+
+def bounded_wait_selftest(spin_limit: int = 1 << 12) -> int:
+    """Status of aphi_selftest_bounded_wait: a device wait that nothing ends,
+    bounded like the tensor-core tile's. ERR_TIMEOUT is the expected answer."""
+    return int(lib().aphi_selftest_bounded_wait(spin_limit))
 
 
 def tc_tile_selftest(P: np.ndarray, i0: int, j0: int, d: np.ndarray | None = None) -> np.ndarray:

@@ -23,8 +23,45 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_selftest(const float2* P, int
     if (!ok && threadIdx.x == 0) atomicExch(err, 1);
 }
 
+// A wait nothing will end: an mbarrier expecting one arrival that never
+// comes, waited on by every thread with the same bounded wait the tensor-core
+// tile uses. Each thread gives up after `limit` tries and the kernel returns
+// normally with the error word set.
+__global__ void k_wait_selftest(long long limit, int* err) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    __syncthreads();
+    const bool done = mbar_wait(smem_u32(&bar), 0, limit);
+    if (!done && threadIdx.x == 0) atomicExch(err, 1);
+}
+
 }  // namespace
 }  // namespace aphi_b200
+
+extern "C" int aphi_selftest_bounded_wait(long long spin_limit) {
+    using namespace aphi_b200;
+    return guard([&] {
+        if (spin_limit < 1 || spin_limit > kTcSpinLimit)
+            throw Error(APHI_ERR_BAD_SHAPE, "selftest: the spin limit is 1 .. the tile's own limit");
+        int* derr = nullptr;
+        APHI_CUDA(cudaMalloc(&derr, sizeof(int)));
+        int e = 0;
+        try {
+            APHI_CUDA(cudaMemset(derr, 0, sizeof(int)));
+            k_wait_selftest<<<1, 128>>>(spin_limit, derr);
+            APHI_CHECK_LAUNCH();
+            APHI_CUDA(cudaMemcpy(&e, derr, sizeof(int), cudaMemcpyDeviceToHost));
+        } catch (...) {
+            cudaFree(derr);
+            throw;
+        }
+        cudaFree(derr);
+        if (e) throw Error(APHI_ERR_TIMEOUT, "selftest: the bounded wait expired, as it must");
+    });
+}
 
 extern "C" int aphi_selftest_tc_tile(int rows, int K, int i0, int j0, const float* P, const float* d, float* out) {
     using namespace aphi_b200;

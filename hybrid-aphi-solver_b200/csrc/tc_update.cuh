@@ -90,8 +90,8 @@ __device__ __forceinline__ void mma_commit(uint32_t mbar) {
                  : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
-    for (long long i = 0; i < kTcSpinLimit; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase, long long limit = kTcSpinLimit) {
+    for (long long i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

@@ -401,6 +401,11 @@ int aphi_measure_peaks(double* tflops);
  * NULL for ones). Rows of P at or beyond `rows` read as zero. K <= 128. The
  * kernel the FP32 factorization uses for its trailing updates. */
 int aphi_selftest_tc_tile(int rows, int K, int i0, int j0, const float* P, const float* d, float* out);
+/* The bounded device wait, exercised: one CTA waits on an mbarrier that
+ * nothing will complete, with the tensor-core tile's own wait, giving up
+ * after spin_limit tries (1 .. the tile's limit). Returns APHI_ERR_TIMEOUT,
+ * with the context still usable; anything else is a failure of the wait. */
+int aphi_selftest_bounded_wait(long long spin_limit);
 
 #ifdef __cplusplus
 }

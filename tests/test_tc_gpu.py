@@ -99,3 +99,15 @@ def test_tc_factor_as_accurate_as_simt(cells, cuda):
     x, iters, berr, ok = ftc.solve_refined(vals, rhs, tol=1e-16, rtol=1e-13, max_iters=40, krylov=True)
     res = ab.residuals(an, vals, x, rhs)
     assert ok and (res[:, 0, 0] <= 1e-13).all(), (iters, res)
+
+
+def test_bounded_wait_gives_up_and_the_context_survives(cuda):
+    """A device wait that nothing ends -- an mbarrier whose one arrival never
+    comes -- waited on with the tensor-core tile's own bounded wait: the
+    kernel gives up, returns normally and reports TIMEOUT, and the device
+    keeps working (a tile computed right after is still exact)."""
+    assert ab.bounded_wait_selftest(1 << 12) == ab.ERR_TIMEOUT
+    rng = np.random.default_rng(5)
+    P = (rng.integers(-4, 5, (160, 16)) + 1j * rng.integers(-4, 5, (160, 16))).astype(np.complex64)
+    out = ab.tc_tile_selftest(P, 0, 0)
+    np.testing.assert_array_equal(out, (P[:128] @ P[:64].T).astype(np.complex64))
