@@ -24,7 +24,7 @@ def test_cylinder_matches_reference_pipeline(cells, ref_or_skip):
     np.testing.assert_array_equal(w.tet_fixed, fx)
 
 
-@pytest.mark.parametrize("cells", [16, 24])
+@pytest.mark.parametrize("cells", [16, 24, 32])
 def test_torus_matches_reference_pipeline(cells, ref_or_skip):
     """The torus with its internal current port: the cut's nodes read the
     port unknown from plus-side tets and a grounded zero from minus-side
