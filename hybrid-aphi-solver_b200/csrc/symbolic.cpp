@@ -21,6 +21,9 @@ long long place_blocks(const Symbolic& S, std::vector<long long>& off) {
         long long begin, end;
         int until;  // last level at which the block is read
     };
+    // `live` stays sorted by begin (blocks never overlap, so begins are
+    // distinct): erasing keeps the order, and each new block is inserted at
+    // its place.
     std::vector<Live> live;
     long long top = 0;
     off.assign(S.ns, -1);
@@ -35,7 +38,6 @@ long long place_blocks(const Symbolic& S, std::vector<long long>& off) {
             if (c <= 0) continue;
             const long long need = c * c;
             const int until = S.sn_parent[s] >= 0 ? S.sn_level[S.sn_parent[s]] : L;
-            std::sort(live.begin(), live.end(), [](const Live& a, const Live& b) { return a.begin < b.begin; });
             long long at = 0;
             for (const Live& b : live) {
                 if (b.begin - at >= need) break;
@@ -46,7 +48,10 @@ long long place_blocks(const Symbolic& S, std::vector<long long>& off) {
             for (const Live& b : live)
                 if (at < b.end && b.begin < at + need) at = (std::max(at, b.end) + 31) / 32 * 32;
             off[s] = at;
-            live.push_back({at, at + need, until});
+            const Live blk{at, at + need, until};
+            live.insert(std::lower_bound(live.begin(), live.end(), blk,
+                                         [](const Live& a, const Live& b) { return a.begin < b.begin; }),
+                        blk);
             top = std::max(top, at + need);
         }
     }
