@@ -120,32 +120,6 @@ Symbolic analyze_supernodal(int n, const int* row_ptr, const int* col_idx, const
                 }
             }
     }
-    // Column counts from the row subtrees: row k of L is every node met
-    // walking up from each earlier neighbour until a node already marked.
-    std::vector<int>& cc = S.ref_colcount;
-    cc.assign(n, 1);
-    {
-        std::vector<int> mark(n, -1);
-        for (int k = 0; k < n; ++k) {
-            mark[k] = k;
-            for (int t = lo_ptr[k]; t < lo_ptr[k + 1]; ++t)
-                for (int i = lo_idx[t]; i != -1 && mark[i] != k; i = parent[i]) {
-                    mark[i] = k;
-                    ++cc[i];
-                }
-        }
-    }
-    if (parent_in)
-        for (int j = 0; j < n; ++j)
-            if (parent_in[j] != parent[j])
-                mismatch("analysis: the elimination tree handed in differs from this pattern's at column " +
-                         std::to_string(j));
-    if (col_count_in)
-        for (int j = 0; j < n; ++j)
-            if (col_count_in[j] != cc[j])
-                mismatch("analysis: the column counts handed in differ from this pattern's at column " +
-                         std::to_string(j));
-
     // Post order (children in ascending order, roots ascending).
     std::vector<int> head(n, -1), next(n, -1);
     for (int j = n - 1; j >= 0; --j)
@@ -177,6 +151,80 @@ Symbolic analyze_supernodal(int n, const int* row_ptr, const int* col_idx, const
         }
         if (k != n) mismatch("analysis: the elimination tree is not a forest");
     }
+    // Column counts (Gilbert, Ng and Peyton 1994): cc[j] is the number of
+    // row subtrees through j. In postorder, a neighbour k of row i is a leaf
+    // of row i's subtree when k's subtree holds no earlier neighbour of row i
+    // (first[k] > the last neighbour's postorder index). Each leaf adds one at
+    // itself, each pair of consecutive leaves subtracts one at their least
+    // common ancestor (the root of the union-find over finished nodes), and
+    // row i subtracts one at its parent, so summing over a node's subtree
+    // counts the rows through it exactly once; a row with no leaf adds its
+    // own diagonal. O(nnz(A) alpha), equal to walking every row subtree.
+    std::vector<int>& cc = S.ref_colcount;
+    cc.assign(n, 0);
+    {
+        const std::vector<int>& post = S.post_of_ref;
+        const std::vector<int>& ref = S.ref_of_post;
+        std::vector<int> first(n, -1);  // smallest postorder index in each subtree, by postorder index
+        for (int q = 0; q < n; ++q) {
+            for (int v = ref[q]; v != -1 && first[post[v]] == -1; v = parent[v]) first[post[v]] = q;
+        }
+        // Rows below each column: the transpose of the earlier-neighbour lists.
+        std::vector<int> up_ptr(n + 1, 0), up_idx(lo_ptr[n]);
+        for (int t = 0; t < lo_ptr[n]; ++t) ++up_ptr[lo_idx[t] + 1];
+        for (int j = 0; j < n; ++j) up_ptr[j + 1] += up_ptr[j];
+        {
+            std::vector<int> at(up_ptr.begin(), up_ptr.end() - 1);
+            for (int i = 0; i < n; ++i)
+                for (int t = lo_ptr[i]; t < lo_ptr[i + 1]; ++t) up_idx[at[lo_idx[t]]++] = i;
+        }
+        std::vector<long long> delta(n, 0);
+        std::vector<int> prevleaf(n, -1), maxfirst(n, -1), uf(n);
+        std::iota(uf.begin(), uf.end(), 0);
+        auto find = [&](int x) {
+            int r = x;
+            while (uf[r] != r) r = uf[r];
+            while (uf[x] != r) {
+                const int nx = uf[x];
+                uf[x] = r;
+                x = nx;
+            }
+            return r;
+        };
+        for (int q = 0; q < n; ++q) {
+            const int j = ref[q];
+            for (int t = up_ptr[j]; t < up_ptr[j + 1]; ++t) {
+                const int i = up_idx[t];
+                if (first[q] <= maxfirst[i]) continue;  // not a leaf of row i's subtree
+                maxfirst[i] = first[q];
+                ++delta[j];
+                if (prevleaf[i] != -1) --delta[find(prevleaf[i])];
+                prevleaf[i] = j;
+            }
+            if (prevleaf[j] == -1) ++delta[j];  // row j has no earlier neighbour: its diagonal
+            if (parent[j] != -1) {
+                --delta[parent[j]];
+                uf[j] = parent[j];
+            }
+        }
+        for (int q = 0; q < n; ++q) {
+            const int j = ref[q];
+            const long long c = delta[j] + cc[j];
+            cc[j] = static_cast<int>(c);
+            if (parent[j] != -1) cc[parent[j]] += cc[j];
+        }
+    }
+    if (parent_in)
+        for (int j = 0; j < n; ++j)
+            if (parent_in[j] != parent[j])
+                mismatch("analysis: the elimination tree handed in differs from this pattern's at column " +
+                         std::to_string(j));
+    if (col_count_in)
+        for (int j = 0; j < n; ++j)
+            if (col_count_in[j] != cc[j])
+                mismatch("analysis: the column counts handed in differ from this pattern's at column " +
+                         std::to_string(j));
+
     S.new_of_orig.resize(n);
     S.orig_of_new.resize(n);
     for (int r = 0; r < n; ++r) {
