@@ -19,18 +19,41 @@ namespace {
 long long place_blocks(const Symbolic& S, std::vector<long long>& off) {
     struct Live {
         long long begin, end;
-        int until;  // last level at which the block is read
+        long long gap;  // free entries between the previous live block's end (or 0) and begin
+        int until;      // last level at which the block is read
     };
-    // `live` stays sorted by begin (blocks never overlap, so begins are
-    // distinct): erasing keeps the order, and each new block is inserted at
-    // its place.
-    std::vector<Live> live;
+    // The live blocks, sorted by begin (they never overlap, so ends are sorted
+    // too), in runs of at most 2 * kRun; each run keeps its largest gap, so the
+    // first-fit search skips the runs with no room. The rule: the first gap
+    // of at least `need` entries, or the end of the last block; rounded up to
+    // 32 entries (512 B for complex128) and, where the rounding reaches the
+    // next block, moved past it, as often as that happens.
+    constexpr size_t kRun = 256;
+    struct Run {
+        std::vector<Live> b;
+        long long max_gap = 0;
+    };
+    auto regap = [](Run& r) {
+        r.max_gap = 0;
+        for (const Live& x : r.b) r.max_gap = std::max(r.max_gap, x.gap);
+    };
+    std::vector<Run> runs;
+    std::vector<Live> flat;
     long long top = 0;
     off.assign(S.ns, -1);
     for (int L = 0; L < S.num_levels; ++L) {
         // Blocks read for the last time at an earlier level are free now.
-        live.erase(std::remove_if(live.begin(), live.end(), [&](const Live& b) { return b.until < L; }),
-                   live.end());
+        flat.clear();
+        for (const Run& r : runs)
+            for (const Live& x : r.b)
+                if (x.until >= L) flat.push_back(x);
+        runs.clear();
+        for (size_t i = 0; i < flat.size(); ++i) {
+            flat[i].gap = flat[i].begin - (i ? flat[i - 1].end : 0);
+            if (i % kRun == 0) runs.emplace_back();
+            runs.back().b.push_back(flat[i]);
+        }
+        for (Run& r : runs) regap(r);
         for (int k = S.level_ptr[L]; k < S.level_ptr[L + 1]; ++k) {
             const int s = S.level_list[k];
             const long long w = S.sn_first[s + 1] - S.sn_first[s];
@@ -38,21 +61,42 @@ long long place_blocks(const Symbolic& S, std::vector<long long>& off) {
             if (c <= 0) continue;
             const long long need = c * c;
             const int until = S.sn_parent[s] >= 0 ? S.sn_level[S.sn_parent[s]] : L;
-            long long at = 0;
-            for (const Live& b : live) {
-                if (b.begin - at >= need) break;
-                at = std::max(at, b.end);
+            // (ri, bi): the first block after the chosen gap (ri == runs.size(): none).
+            size_t ri = 0, bi = 0;
+            while (ri < runs.size() && runs[ri].max_gap < need) ++ri;
+            if (ri < runs.size())
+                while (runs[ri].b[bi].gap < need) ++bi;
+            auto end_before = [&](size_t r, size_t i) -> long long {
+                if (i > 0) return runs[r].b[i - 1].end;
+                return r > 0 ? runs[r - 1].b.back().end : 0;
+            };
+            long long at = (end_before(ri, bi) + 31) / 32 * 32;
+            while (ri < runs.size() && runs[ri].b[bi].begin < at + need) {
+                at = (std::max(at, runs[ri].b[bi].end) + 31) / 32 * 32;
+                if (++bi == runs[ri].b.size()) ++ri, bi = 0;
             }
-            // Keep every block 32-entry aligned (512 B for complex128).
-            at = (at + 31) / 32 * 32;
-            for (const Live& b : live)
-                if (at < b.end && b.begin < at + need) at = (std::max(at, b.end) + 31) / 32 * 32;
             off[s] = at;
-            const Live blk{at, at + need, until};
-            live.insert(std::lower_bound(live.begin(), live.end(), blk,
-                                         [](const Live& a, const Live& b) { return a.begin < b.begin; }),
-                        blk);
             top = std::max(top, at + need);
+            const Live blk{at, at + need, at - end_before(ri, bi), until};
+            if (ri == runs.size()) {
+                if (runs.empty() || runs.back().b.size() >= 2 * kRun) runs.emplace_back();
+                runs.back().b.push_back(blk);
+                runs.back().max_gap = std::max(runs.back().max_gap, blk.gap);
+                continue;
+            }
+            Run& r = runs[ri];
+            r.b[bi].gap = r.b[bi].begin - blk.end;
+            r.b.insert(r.b.begin() + bi, blk);
+            if (r.b.size() > 2 * kRun) {
+                Run tail;
+                tail.b.assign(r.b.begin() + kRun, r.b.end());
+                r.b.resize(kRun);
+                regap(tail);
+                regap(r);
+                runs.insert(runs.begin() + ri + 1, std::move(tail));
+            } else {
+                regap(r);
+            }
         }
     }
     return top;
@@ -304,13 +348,16 @@ Symbolic analyze_supernodal(int n, const int* row_ptr, const int* col_idx, const
             if (a != b) ++acol_ptr[std::min(a, b) + 1];
         }
     for (int j = 0; j < n; ++j) acol_ptr[j + 1] += acol_ptr[j];
-    std::vector<int> acol(acol_ptr[n]);
+    std::vector<int> acol(acol_ptr[n]), acol_k(acol_ptr[n]);  // row, and the entry's index in A
     {
         std::vector<int> c2(acol_ptr.begin(), acol_ptr.end() - 1);
         for (int r = 0; r < n; ++r)
             for (int k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
                 const int a = S.new_of_orig[r], b = S.new_of_orig[col_idx[k]];
-                if (a != b) acol[c2[std::min(a, b)]++] = std::max(a, b);
+                if (a == b) continue;
+                const int t = c2[std::min(a, b)]++;
+                acol[t] = std::max(a, b);
+                acol_k[t] = k;
             }
     }
 
@@ -375,40 +422,52 @@ Symbolic analyze_supernodal(int n, const int* row_ptr, const int* col_idx, const
     }
     S.stored = S.sn_loff[ns];
 
-    // Extend-add maps: each CB row of child c -> its position in the parent's structure.
+    // Extend-add maps (each CB row of child c -> its position in the parent's
+    // structure) and A entries -> panel positions. Both look rows up in one
+    // numbering of a supernode's structure: its children's CB rows, and the
+    // rows of the entries of A in its columns. The diagonal entry of column j
+    // sits at row j - first of its panel, since a structure opens with its own
+    // columns.
     S.rel_off.assign(ns + 1, 0);
     for (int s = 0; s < ns; ++s) {
         const int w = S.sn_first[s + 1] - S.sn_first[s];
         S.rel_off[s + 1] = S.rel_off[s] + (S.sn_parent[s] >= 0 ? S.sn_rows[s] - w : 0);
     }
     S.rel.assign(S.rel_off[ns], 0);
-    for (int s = 0; s < ns; ++s) {
-        const int p = S.sn_parent[s];
-        if (p < 0) continue;
-        const int w = S.sn_first[s + 1] - S.sn_first[s];
-        const int* pb = S.structs.data() + S.sn_struct_off[p];
-        const int* pe = S.structs.data() + S.sn_struct_off[p + 1];
-        for (int i = w; i < S.sn_rows[s]; ++i) {
-            const int row = S.structs[S.sn_struct_off[s] + i];
-            const int* it = std::lower_bound(pb, pe, row);
-            if (it == pe || *it != row) mismatch("analysis: a child's row is missing from its parent's structure");
-            S.rel[S.rel_off[s] + (i - w)] = static_cast<int>(it - pb);
+    S.a_dest.assign(S.nnz_a, -1);
+    {
+        std::vector<int> at_row(n), owner(n, -1);
+        for (int s = 0; s < ns; ++s) {
+            const int f = S.sn_first[s], l = S.sn_first[s + 1] - 1, m = S.sn_rows[s];
+            const int* st = S.structs.data() + S.sn_struct_off[s];
+            for (int q = 0; q < m; ++q) {
+                at_row[st[q]] = q;
+                owner[st[q]] = s;
+            }
+            for (int t = S.child_ptr[s]; t < S.child_ptr[s + 1]; ++t) {
+                const int c = S.child_list[t];
+                const int wc = S.sn_first[c + 1] - S.sn_first[c];
+                const int* sc = S.structs.data() + S.sn_struct_off[c];
+                for (int i = wc; i < S.sn_rows[c]; ++i) {
+                    if (owner[sc[i]] != s) mismatch("analysis: a child's row is missing from its parent's structure");
+                    S.rel[S.rel_off[c] + (i - wc)] = at_row[sc[i]];
+                }
+            }
+            for (int j = f; j <= l; ++j) {
+                const long long col0 = S.sn_loff[s] + static_cast<long long>(j - f) * m;
+                for (int t = acol_ptr[j]; t < acol_ptr[j + 1]; ++t) {
+                    if (owner[acol[t]] != s) mismatch("analysis: an entry of A has no place in L's structure");
+                    S.a_dest[acol_k[t]] = col0 + at_row[acol[t]];
+                }
+            }
         }
+        for (int r = 0; r < n; ++r)
+            for (int k = row_ptr[r]; k < row_ptr[r + 1]; ++k)
+                if (col_idx[k] == r) {
+                    const int j = S.new_of_orig[r], s = S.col_snode[j], d = j - S.sn_first[s];
+                    S.a_dest[k] = S.sn_loff[s] + static_cast<long long>(d) * S.sn_rows[s] + d;
+                }
     }
-
-    // A entries -> panel positions.
-    S.a_dest.resize(S.nnz_a);
-    for (int r = 0; r < n; ++r)
-        for (int k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
-            const int a = S.new_of_orig[r], b = S.new_of_orig[col_idx[k]];
-            const int col = std::min(a, b), row = std::max(a, b);
-            const int s = S.col_snode[col];
-            const int* sb = S.structs.data() + S.sn_struct_off[s];
-            const int* se = S.structs.data() + S.sn_struct_off[s + 1];
-            const int* it = std::lower_bound(sb, se, row);
-            if (it == se || *it != row) mismatch("analysis: an entry of A has no place in L's structure");
-            S.a_dest[k] = S.sn_loff[s] + static_cast<long long>(col - S.sn_first[s]) * S.sn_rows[s] + (it - sb);
-        }
 
     // Levels.
     S.sn_level.assign(ns, 0);

@@ -78,3 +78,19 @@ def test_refuses_meshes_without_a_conductor():
         ab.Workload.cylinder(0)
     with pytest.raises(ab.AphiError):
         ab.Workload.cylinder(2)    # no centroid within r = 0.2: the reference refuses too
+
+
+@pytest.mark.parametrize("kind,cells", [("cylinder", 12), ("torus", 16)])
+def test_analysis_matches_reference_analyze(kind, cells, ref_or_skip):
+    """The supernodal analysis recomputes the elimination tree and column
+    counts from the pattern and the caller's permutation: on the reference's
+    own analyze output (AMD, src/symbolic.cpp:126-194) both are equal, and the
+    reference's tree and counts handed in are accepted."""
+    r = getattr(ref_or_skip.RefProblem, kind)(cells)
+    rp, ci = r.pattern()
+    a = r.analysis()
+    an = ab.Analysis(rp, ci, a["perm"], a["parent"], a["col_count"])
+    parent, cc = an.etree()
+    np.testing.assert_array_equal(parent, a["parent"])
+    np.testing.assert_array_equal(cc, a["col_count"])
+    assert int(an.info["nnz_l"]) == int(a["col_count"].astype(np.int64).sum())
