@@ -46,7 +46,13 @@ constexpr int kTile = 64;        // update tile
 constexpr int kTrsmRows = 128;   // rows per TRSM block
 constexpr int kPanelGroup = 4;                 // most panels per trailing update of the rest of a front
 constexpr int kWidePair = kPanelGroup * kTcPanel;  // the most panel columns one trailing update applies
-constexpr int kGroup4Rows = 8192;              // fronts this tall group 4 panels, smaller ones 2
+// Fronts this tall group 4 panels, smaller ones 2. A build may lower the
+// threshold (the host-side plan checker does, to reach 4-panel groups on
+// fronts small enough to replay on a CPU).
+#ifndef APHI_GROUP4_ROWS
+#define APHI_GROUP4_ROWS 8192
+#endif
+constexpr int kGroup4Rows = APHI_GROUP4_ROWS;
 constexpr int kEaCols = 32;      // front columns per extend-add item
 constexpr int kSolveBlock = 64;  // columns per triangular-solve block
 constexpr int kSolveRows = 256;  // rows per solve update item
