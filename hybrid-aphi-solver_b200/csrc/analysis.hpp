@@ -7,6 +7,7 @@
 
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <vector>
 
 #include "aphi_b200.h"
@@ -97,6 +98,7 @@ struct aphi_analysis {
     bool fronts = false;   // built from independent dense fronts (no matrix pattern)
     void* ws = nullptr;    // contribution-block workspace shared by this analysis's factors
     size_t ws_bytes = 0;
+    std::mutex ws_mu;      // held while a factorization (or aphi_fronts_read) uses ws
     long long num_items = 0;
     long long upool = 0;   // update-vector pool entries (per rhs)
     int max_parts = 1;

@@ -457,6 +457,9 @@ void fronts_read(const aphi_factor* f, int k, double* panels_out, double* cb_out
     if (!A->fronts) throw Error(APHI_ERR_INVALID, "fronts_read: not a fronts analysis");
     if (k < 0 || k >= f->batch) throw Error(APHI_ERR_BAD_SHAPE, "fronts_read: batch index out of range");
     if (!f->factored) throw Error(APHI_ERR_INVALID, "fronts_read: nothing factorized yet");
+    // The contribution blocks live in the analysis's shared workspace: they
+    // are those of its latest factorization.
+    std::lock_guard<std::mutex> ws_lock(f->an->ws_mu);
     const long long ls = A->S.stored, cs = A->S.cb_pool;
     auto widen = [&](const void* src, long long len, double* dst) {
         if (!dst || len == 0) return;
@@ -516,7 +519,11 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
     }
     // The contribution-block pool is only live during a factorization, so it
     // is a workspace owned by the analysis and shared by every factor made
-    // from it (their factorizations are ordered on the caller's streams).
+    // from it. A factorization holds the analysis's lock from here until its
+    // stream has finished with the pool (the synchronize below), so
+    // factorizations of one analysis from several host threads, on any
+    // streams, take turns.
+    std::unique_lock<std::mutex> ws_lock(f->an->ws_mu);
     {
         aphi_analysis* an = f->an;
         const size_t need = static_cast<size_t>(std::max<long long>(S.cb_pool, 1)) * B * f->elem;
@@ -546,6 +553,7 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
     int err_word = 0;
     APHI_CUDA(cudaMemcpyAsync(&err_word, f->err, sizeof(int), cudaMemcpyDeviceToHost, st));
     APHI_CUDA(cudaStreamSynchronize(st));
+    ws_lock.unlock();
     if (err_word != 0) {
         if (f->profile) collect_profile(f);
         APHI_CUDA(cudaMemsetAsync(f->err, 0, sizeof(int), st));

@@ -237,7 +237,11 @@ int aphi_analysis_etree(const aphi_analysis* a, int* parent, int* col_count);
 
 typedef struct aphi_factor aphi_factor;
 /* A factor holds `batch` numeric factorizations of one analysis (its
- * capacity); every buffer is sized for it once. */
+ * capacity); every buffer is sized for it once. The contribution-block pool,
+ * live only during a factorization, is a workspace of the analysis shared by
+ * all its factors (sized for the largest): factorizations of one analysis take
+ * turns, each holding it until its stream is done with the pool, so they may
+ * come from several host threads and streams. */
 int aphi_factor_create(const aphi_analysis* an, int precision, int batch, aphi_factor** out);
 int aphi_factor_destroy(aphi_factor* f);
 /* Sets how many entries (1..capacity) later calls process, without
@@ -358,7 +362,9 @@ int aphi_solve_symmetric_host(const aphi_analysis* an, const double* values, con
  *   aphi_fronts_read: entry k's factored panels (D on the diagonal, L below)
  *     and contribution blocks (front s's (rows - widths)^2 block, column-major,
  *     lower triangle, at cb_offset[s]), widened to complex128, into device
- *     buffers of stored and cb_pool entries (analysis info[3], info[9]). */
+ *     buffers of stored and cb_pool entries (analysis info[3], info[9]). The
+ *     blocks sit in the analysis's shared workspace: they are those of its
+ *     latest factorization, by this factor or another. */
 int aphi_fronts_create(int count, const int* rows, const int* widths, const aphi_analysis_options* opt,
                        aphi_analysis** out);
 int aphi_fronts_layout(const aphi_analysis* a, int64_t* panel_offset, int64_t* cb_offset);
