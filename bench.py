@@ -115,6 +115,32 @@ def _ref_one(args):
     return time.perf_counter() - t0, rep["factorize_ms"], rep["backward_error"]
 
 
+def host_procs(gb_per_proc: float = 0.5) -> int:
+    """Concurrent reference solves for this host: one per core in the
+    process's CPU affinity, capped so that they use at most half of the
+    memory available (MemAvailable, or what the cgroup limit leaves);
+    a 16^3 reference solve peaks near 0.35 GB."""
+    cpus = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    avail = None
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    avail = int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    try:
+        lim = Path("/sys/fs/cgroup/memory.max").read_text().strip()
+        cur = int(Path("/sys/fs/cgroup/memory.current").read_text().strip())
+        if lim.isdigit():
+            avail = min(avail if avail is not None else 1 << 62, int(lim) - cur)
+    except (OSError, ValueError):
+        pass
+    if avail is None:
+        return cpus
+    return max(1, min(cpus, int(0.5 * avail / (gb_per_proc * 2 ** 30))))
+
+
 def cpu_reference(cells_sample: int, cells_target: int, procs: int):
     """Concurrent reference solves (one frequency each) on the sample mesh;
     solves/s scaled to the target mesh by the factorization-flop ratio."""
@@ -149,9 +175,10 @@ def run_reference(args):
     if not rb.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libaphi_ref.so was not built"}))
         return
-    procs = min(os.cpu_count() or 1, 16)
-    for _ in range(args.warmup if args.warmup < 1 else 0):
-        pass
+    # Every core this process may run on, as far as memory allows. No
+    # warm-up steps: each solve is timed inside its own process, after an
+    # untimed refill of the same system.
+    procs = host_procs()
     vals = []
     for _ in range(max(args.steps, 1)):
         vals.append(cpu_reference(args.sample_cells, args.cells, procs))
