@@ -9,8 +9,9 @@
 // (Amestoy, Davis & Duff) with supervariables detected by hashing, degree
 // buckets kept as last-in-first-out linked lists, and the three-way degree
 // bound -- over the symmetric adjacency of src/ordering.cpp:58-98 (each
-// list ascending, no duplicates, no diagonal). The storage is this project's
-// own: one flat pool of per-vertex lists instead of nested vectors.
+// list ascending, no duplicates, no diagonal). Each vertex keeps growable
+// lists (its variable neighbours, its elements, an element's members, the
+// supervariables merged into it), released when the vertex is absorbed.
 #include <algorithm>
 #include <vector>
 
