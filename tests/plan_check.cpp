@@ -18,7 +18,9 @@
 // panel-group threshold and with a lowered one), run by
 // tests/test_plan_check.py.
 //
-//   plan_check cylinder <cells> [mistake] | torus <cells> [mistake] | fronts <seed> <count> <max_rows>
+//   plan_check cylinder <cells> [mistake] | torus <cells> [mistake]
+//   plan_check fronts <seed> <count> <max_rows>
+//   plan_check pattern <diag|dense|arrow|blocks|band|random> <n> <seed> [natural]
 //
 // With [mistake] (overlap, dup, rel, kcap: see plant_mistake) the plan is
 // corrupted first, and the checks must fail.
@@ -29,6 +31,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <random>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -466,12 +469,49 @@ aphi_analysis_options default_options() {
     return o;
 }
 
-int check_matrix(const Workload& wl, const std::string& plant) {
-    const int n = wl.num_total;
-    const std::vector<int>& rp = wl.row_ptr;
-    const std::vector<int>& ci = wl.col_idx;
+// Synthetic upper CSR patterns (diagonal in every row) for edge cases of the
+// elimination tree: "diag" (no off-diagonal entry), "dense", "arrow" (every
+// unknown coupled to the last), "blocks" (disconnected cliques of 1-40
+// unknowns), "band" (half-bandwidth 20), "random" (0-6 later neighbours per row).
+void make_pattern(const std::string& shape, int n, unsigned seed, std::vector<int>& rp, std::vector<int>& ci) {
+    std::mt19937 rng(seed);
+    std::vector<std::vector<int>> rows(n);
+    int block_end = 0;
+    for (int i = 0; i < n; ++i) {
+        rows[i].push_back(i);
+        if (shape == "dense") {
+            for (int j = i + 1; j < n; ++j) rows[i].push_back(j);
+        } else if (shape == "arrow") {
+            if (i + 1 < n) rows[i].push_back(n - 1);
+        } else if (shape == "blocks") {
+            if (i >= block_end) block_end = std::min(n, i + 1 + static_cast<int>(rng() % 40));
+            for (int j = i + 1; j < block_end; ++j) rows[i].push_back(j);
+        } else if (shape == "band") {
+            for (int j = i + 1; j < std::min(n, i + 21); ++j) rows[i].push_back(j);
+        } else if (shape == "random") {
+            const int k = static_cast<int>(rng() % 7);
+            for (int q = 0; q < k && i + 1 < n; ++q) rows[i].push_back(i + 1 + static_cast<int>(rng() % (n - i - 1)));
+        } else if (shape != "diag") {
+            throw std::invalid_argument("unknown pattern shape " + shape);
+        }
+        std::sort(rows[i].begin(), rows[i].end());
+        rows[i].erase(std::unique(rows[i].begin(), rows[i].end()), rows[i].end());
+    }
+    rp.assign(1, 0);
+    ci.clear();
+    for (const auto& r : rows) {
+        ci.insert(ci.end(), r.begin(), r.end());
+        rp.push_back(static_cast<int>(ci.size()));
+    }
+}
+
+int check_matrix(int n, const std::vector<int>& rp, const std::vector<int>& ci, bool natural,
+                 const std::string& plant) {
     std::vector<int> perm(n);
-    reference_amd(n, rp.data(), ci.data(), perm.data());
+    if (natural)
+        for (int i = 0; i < n; ++i) perm[i] = i;
+    else
+        reference_amd(n, rp.data(), ci.data(), perm.data());
     aphi_analysis* A = analysis_create(n, rp.data(), ci.data(), perm.data(), nullptr, nullptr, default_options());
     const Symbolic& S = A->S;
     if (!plant.empty()) {
@@ -642,13 +682,23 @@ int main(int argc, char** argv) {
             if (mode == "cylinder") build_cylinder(w, std::atoi(argv[2]), 1.0, 0);
             else build_torus(w, std::atoi(argv[2]), 1.0);
             std::printf("group4_rows %d ", kGroup4Rows);
-            return check_matrix(w, argc == 4 ? argv[3] : "");
+            return check_matrix(w.num_total, w.row_ptr, w.col_idx, false, argc == 4 ? argv[3] : "");
+        }
+        if (mode == "pattern" && (argc == 5 || argc == 6)) {
+            std::vector<int> rp, ci;
+            const int n = std::atoi(argv[3]);
+            make_pattern(argv[2], n, static_cast<unsigned>(std::atoi(argv[4])), rp, ci);
+            std::printf("group4_rows %d %s ", kGroup4Rows, argv[2]);
+            return check_matrix(n, rp, ci, argc == 6 && std::string(argv[5]) == "natural", "");
         }
         if (mode == "fronts" && argc == 5) {
             std::printf("group4_rows %d ", kGroup4Rows);
             return check_fronts(static_cast<unsigned>(std::atoi(argv[2])), std::atoi(argv[3]), std::atoi(argv[4]));
         }
-        std::fprintf(stderr, "usage: %s cylinder <cells> [mistake] | torus <cells> [mistake] | fronts <seed> <count> <max_rows>\n", argv[0]);
+        std::fprintf(stderr,
+                     "usage: %s cylinder <cells> [mistake] | torus <cells> [mistake] | fronts <seed> <count> <max_rows>"
+                     " | pattern <shape> <n> <seed> [natural]\n",
+                     argv[0]);
         return 2;
     } catch (const std::exception& e) {
         std::fprintf(stderr, "plan_check: %s\n", e.what());

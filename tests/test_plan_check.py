@@ -55,6 +55,26 @@ def test_plan_replays_clean(plan_check, build, mode, args, reach):
         assert all(g[2] > 0 for g in groups), r.stdout
 
 
+# Edge cases of the elimination tree, each on both builds: nothing to
+# factor, one unknown, no coupling at all, one dense front (wider than a
+# 4-panel group), a star, disconnected cliques (many roots), a band (a path
+# of supernodes, one per level), random sparsity with AMD and natural order.
+PATTERNS = [("diag", 0, 1, ""), ("diag", 1, 1, ""), ("diag", 500, 1, ""), ("dense", 700, 2, ""),
+            ("arrow", 2000, 1, ""), ("blocks", 3000, 5, ""), ("band", 3000, 1, "natural"),
+            ("random", 4000, 7, ""), ("random", 4000, 7, "natural")]
+
+
+@pytest.mark.parametrize("build", ["plan_check", "plan_check_g4"])
+@pytest.mark.parametrize("shape,n,seed,order", PATTERNS, ids=[f"{p[0]}-{p[1]}-{p[3] or 'amd'}" for p in PATTERNS])
+def test_edge_patterns_replay_clean(plan_check, build, shape, n, seed, order):
+    r = plan_check(build, "pattern", shape, n, seed, *([order] if order else []))
+    assert r.returncode == 0, r.stdout + r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if "bounds" in ln]
+    assert len(lines) == 2 and all(ln.endswith(" ok") for ln in lines), r.stdout
+    if shape == "dense" and build == "plan_check_g4":
+        assert all(g[2] > 0 for g in _groups(r.stdout)), r.stdout   # a 4-panel group in the dense front
+
+
 @pytest.mark.parametrize("mistake,caught", [
     ("overlap", r"ww [1-9]\d* rw \d+ stale [1-9]"),   # two live CBs on one another
     ("dup", r"ww [1-9]"),                             # one tile updated by two items of a launch
