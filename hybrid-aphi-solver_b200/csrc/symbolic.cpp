@@ -1,6 +1,7 @@
 #include "symbolic.hpp"
 
 #include <algorithm>
+#include <functional>
 #include <numeric>
 #include <string>
 
@@ -12,94 +13,169 @@ namespace {
 
 [[noreturn]] void mismatch(const std::string& m) { throw Error(APHI_ERR_PATTERN_MISMATCH, m); }
 
-// CB memory: children's contribution blocks stay alive until their parent
-// has been assembled. Blocks are placed by first fit over the level schedule
-// (a block is live from its own level to its parent's level, inclusive), so
-// the pool is far smaller than the sum of all blocks.
-long long place_blocks(const Symbolic& S, std::vector<long long>& off) {
-    struct Live {
-        long long begin, end;
-        long long gap;  // free entries between the previous live block's end (or 0) and begin
-        int until;      // last level at which the block is read
-    };
-    // The live blocks, sorted by begin (they never overlap, so ends are sorted
-    // too), in runs of at most 2 * kRun; each run keeps its largest gap, so the
-    // first-fit search skips the runs with no room. The rule: the first gap
-    // of at least `need` entries, or the end of the last block; rounded up to
-    // 32 entries (512 B for complex128) and, where the rounding reaches the
-    // next block, moved past it, as often as that happens.
-    constexpr size_t kRun = 256;
-    struct Run {
-        std::vector<Live> b;
-        long long max_gap = 0;
-    };
-    auto regap = [](Run& r) {
-        r.max_gap = 0;
-        for (const Live& x : r.b) r.max_gap = std::max(r.max_gap, x.gap);
-    };
-    std::vector<Run> runs;
-    std::vector<Live> flat;
-    long long top = 0;
-    off.assign(S.ns, -1);
-    for (int L = 0; L < S.num_levels; ++L) {
-        // Blocks read for the last time at an earlier level are free now.
-        flat.clear();
-        for (const Run& r : runs)
-            for (const Live& x : r.b)
-                if (x.until >= L) flat.push_back(x);
-        runs.clear();
-        for (size_t i = 0; i < flat.size(); ++i) {
-            flat[i].gap = flat[i].begin - (i ? flat[i - 1].end : 0);
-            if (i % kRun == 0) runs.emplace_back();
-            runs.back().b.push_back(flat[i]);
+// CB memory. Front s's contribution block is written at its own level and
+// read for the last time by its parent's extend-add, so under the level
+// schedule it is live from level(s) to level(parent(s)), inclusive; two
+// blocks may share memory when their lifetimes are disjoint. The pool can be
+// no smaller than the largest total of blocks live at one level.
+//
+// Placement is offline: blocks are taken in a fixed order and each goes to
+// the lowest offset, rounded up to 32 entries (512 B for complex128), that is
+// free at every level of its lifetime. Three orders are tried -- largest
+// block first; largest size x lifetime first; latest-freed first, then
+// largest -- and the one with the smallest pool is kept. On the cylinders
+// and tori measured this lands within 0-4% of the bound (a level-by-level
+// first fit was 20-50% above it).
+
+// The blocks placed at one level, sorted by begin (they never overlap, so ends
+// are sorted too), in runs of at most 2 * kRun; each block records the free
+// gap before it and each run its largest gap, so searches skip full runs.
+class LevelSpace {
+public:
+    // The lowest 32-aligned p >= x (x aligned) with [p, p + need) free here.
+    long long fit(long long x, long long need) const {
+        size_t lo = 0, hi = runs_.size();  // the first run with a block ending after x
+        while (lo < hi) {
+            const size_t mid = (lo + hi) / 2;
+            if (runs_[mid].b.back().end > x) hi = mid;
+            else lo = mid + 1;
         }
-        for (Run& r : runs) regap(r);
-        for (int k = S.level_ptr[L]; k < S.level_ptr[L + 1]; ++k) {
-            const int s = S.level_list[k];
-            const long long w = S.sn_first[s + 1] - S.sn_first[s];
-            const long long c = S.sn_rows[s] - w;
-            if (c <= 0) continue;
-            const long long need = c * c;
-            const int until = S.sn_parent[s] >= 0 ? S.sn_level[S.sn_parent[s]] : L;
-            // (ri, bi): the first block after the chosen gap (ri == runs.size(): none).
-            size_t ri = 0, bi = 0;
-            while (ri < runs.size() && runs[ri].max_gap < need) ++ri;
-            if (ri < runs.size())
-                while (runs[ri].b[bi].gap < need) ++bi;
-            auto end_before = [&](size_t r, size_t i) -> long long {
-                if (i > 0) return runs[r].b[i - 1].end;
-                return r > 0 ? runs[r - 1].b.back().end : 0;
-            };
-            long long at = (end_before(ri, bi) + 31) / 32 * 32;
-            while (ri < runs.size() && runs[ri].b[bi].begin < at + need) {
-                at = (std::max(at, runs[ri].b[bi].end) + 31) / 32 * 32;
-                if (++bi == runs[ri].b.size()) ++ri, bi = 0;
-            }
-            off[s] = at;
-            top = std::max(top, at + need);
-            const Live blk{at, at + need, at - end_before(ri, bi), until};
-            if (ri == runs.size()) {
-                if (runs.empty() || runs.back().b.size() >= 2 * kRun) runs.emplace_back();
-                runs.back().b.push_back(blk);
-                runs.back().max_gap = std::max(runs.back().max_gap, blk.gap);
-                continue;
-            }
-            Run& r = runs[ri];
-            r.b[bi].gap = r.b[bi].begin - blk.end;
-            r.b.insert(r.b.begin() + bi, blk);
-            if (r.b.size() > 2 * kRun) {
-                Run tail;
-                tail.b.assign(r.b.begin() + kRun, r.b.end());
-                r.b.resize(kRun);
-                regap(tail);
-                regap(r);
-                runs.insert(runs.begin() + ri + 1, std::move(tail));
-            } else {
-                regap(r);
+        size_t ri = lo;
+        if (ri == runs_.size()) return x;
+        size_t bi = std::upper_bound(runs_[ri].b.begin(), runs_[ri].b.end(), x,
+                                     [](long long v, const Block& b) { return v < b.end; }) -
+                    runs_[ri].b.begin();
+        long long p = x;
+        while (true) {
+            if (ri == runs_.size() || runs_[ri].b[bi].begin >= p + need) return p;
+            p = align(std::max(p, runs_[ri].b[bi].end));
+            if (++bi == runs_[ri].b.size()) ++ri, bi = 0;
+            // The next block with a gap of at least `need` before it (a smaller
+            // gap cannot hold the block); p moves past every block skipped.
+            while (ri < runs_.size()) {
+                const Run& r = runs_[ri];
+                while (bi < r.b.size() && r.b[bi].gap < need) p = align(std::max(p, r.b[bi++].end));
+                if (bi < r.b.size()) break;
+                ++ri;
+                bi = 0;
+                while (ri < runs_.size() && runs_[ri].max_gap < need) p = align(std::max(p, runs_[ri++].b.back().end));
             }
         }
     }
+    void insert(long long begin, long long end) {
+        if (runs_.empty()) {
+            runs_.push_back(Run{{Block{begin, end, begin}}, begin});
+            return;
+        }
+        size_t lo = 0, hi = runs_.size();  // the first run whose last block begins after `begin`
+        while (lo < hi) {
+            const size_t mid = (lo + hi) / 2;
+            if (runs_[mid].b.back().begin > begin) hi = mid;
+            else lo = mid + 1;
+        }
+        const size_t ri = std::min(lo, runs_.size() - 1);
+        Run& r = runs_[ri];
+        const size_t bi = std::upper_bound(r.b.begin(), r.b.end(), begin,
+                                           [](long long v, const Block& b) { return v < b.begin; }) -
+                          r.b.begin();
+        const long long prev_end = bi > 0 ? r.b[bi - 1].end : (ri > 0 ? runs_[ri - 1].b.back().end : 0);
+        r.b.insert(r.b.begin() + bi, Block{begin, end, begin - prev_end});
+        if (bi + 1 < r.b.size()) {
+            r.b[bi + 1].gap = r.b[bi + 1].begin - end;
+        } else if (ri + 1 < runs_.size()) {
+            Run& next = runs_[ri + 1];
+            next.b[0].gap = next.b[0].begin - end;
+            regap(next);
+        }
+        if (r.b.size() > 2 * kRun) {
+            Run tail;
+            tail.b.assign(r.b.begin() + kRun, r.b.end());
+            r.b.resize(kRun);
+            regap(tail);
+            regap(r);
+            runs_.insert(runs_.begin() + ri + 1, std::move(tail));
+        } else {
+            regap(r);
+        }
+    }
+
+private:
+    static constexpr size_t kRun = 256;
+    struct Block {
+        long long begin, end, gap;
+    };
+    struct Run {
+        std::vector<Block> b;
+        long long max_gap = 0;
+    };
+    static long long align(long long v) { return (v + 31) / 32 * 32; }
+    static void regap(Run& r) {
+        r.max_gap = 0;
+        for (const Block& b : r.b) r.max_gap = std::max(r.max_gap, b.gap);
+    }
+    std::vector<Run> runs_;
+};
+
+struct CbBlock {
+    int s, lo, hi;  // front, first and last level live
+    long long need;
+};
+
+// Places the blocks in `order`; returns the pool size, offsets into `at`.
+long long place_in_order(const std::vector<CbBlock>& blocks, const std::vector<int>& order, int levels,
+                         std::vector<long long>& at) {
+    std::vector<LevelSpace> space(levels);
+    at.assign(blocks.size(), -1);
+    long long top = 0;
+    for (int i : order) {
+        const CbBlock& b = blocks[i];
+        long long x = 0;
+        for (bool moved = true; moved;) {  // until one offset fits at every level
+            moved = false;
+            for (int L = b.lo; L <= b.hi; ++L) {
+                const long long p = space[L].fit(x, b.need);
+                if (p != x) {
+                    x = p;
+                    moved = true;
+                }
+            }
+        }
+        at[i] = x;
+        top = std::max(top, x + b.need);
+        for (int L = b.lo; L <= b.hi; ++L) space[L].insert(x, x + b.need);
+    }
     return top;
+}
+
+long long place_blocks(const Symbolic& S, std::vector<long long>& off) {
+    std::vector<CbBlock> blocks;
+    for (int L = 0; L < S.num_levels; ++L)
+        for (int k = S.level_ptr[L]; k < S.level_ptr[L + 1]; ++k) {
+            const int s = S.level_list[k];
+            const long long c = S.sn_rows[s] - (S.sn_first[s + 1] - S.sn_first[s]);
+            if (c > 0) blocks.push_back({s, L, S.sn_parent[s] >= 0 ? S.sn_level[S.sn_parent[s]] : L, c * c});
+        }
+    auto span = [](const CbBlock& b) { return static_cast<long long>(b.hi - b.lo + 1); };
+    const std::vector<std::function<bool(const CbBlock&, const CbBlock&)>> orders = {
+        [](const CbBlock& a, const CbBlock& b) { return a.need > b.need; },
+        [&](const CbBlock& a, const CbBlock& b) { return a.need * span(a) > b.need * span(b); },
+        [](const CbBlock& a, const CbBlock& b) { return a.hi != b.hi ? a.hi > b.hi : a.need > b.need; },
+    };
+    long long best = -1;
+    std::vector<long long> best_at, at;
+    for (const auto& cmp : orders) {
+        std::vector<int> order(blocks.size());
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cmp(blocks[a], blocks[b]); });
+        const long long top = place_in_order(blocks, order, S.num_levels, at);
+        if (best < 0 || top < best) {
+            best = top;
+            best_at.swap(at);
+        }
+    }
+    off.assign(S.ns, -1);
+    for (size_t i = 0; i < blocks.size(); ++i) off[blocks[i].s] = best_at[i];
+    return std::max(best, 0LL);
 }
 
 }  // namespace
