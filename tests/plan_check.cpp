@@ -565,6 +565,18 @@ int check_matrix(int n, const std::vector<int>& rp, const std::vector<int>& ci, 
         bz[k] = C(b[2 * k], b[2 * k + 1]);
     }
 
+    // The CB pool against its lower bound: the largest total of blocks live
+    // at one level (a block from its front's level to its parent's).
+    {
+        std::vector<long long> live(std::max(S.num_levels, 1), 0);
+        for (int s = 0; s < S.ns; ++s) {
+            const long long c = S.sn_rows[s] - (S.sn_first[s + 1] - S.sn_first[s]);
+            if (c <= 0) continue;
+            const int hi = S.sn_parent[s] >= 0 ? S.sn_level[S.sn_parent[s]] : S.sn_level[s];
+            for (int L = S.sn_level[s]; L <= hi; ++L) live[L] += c * c;
+        }
+        std::printf("cb_pool %lld bound %lld ", S.cb_pool, *std::max_element(live.begin(), live.end()));
+    }
     int bad = 0;
     const std::vector<Launch>* plans[2] = {&A->plan_factor, &A->plan_factor_tc};
     const char* pname[2] = {"dmma", "tc"};

@@ -48,6 +48,9 @@ def test_plan_replays_clean(plan_check, build, mode, args, reach):
     assert lines and all(ln.endswith(" ok") for ln in lines), r.stdout
     for ln in lines:
         assert " bounds 0 ww 0 rw 0 stale 0 " in ln, ln
+    pool = re.search(r"cb_pool (\d+) bound (\d+)", r.stdout)
+    if pool:   # the CB pool within 10% of the largest total of blocks live at one level
+        assert int(pool[2]) <= int(pool[1]) <= 1.1 * int(pool[2]), r.stdout
     groups = _groups(r.stdout)
     if "2" in reach:
         assert all(g[1] > 0 for g in groups), r.stdout
