@@ -4,6 +4,7 @@
 #include <functional>
 #include <numeric>
 #include <string>
+#include <thread>
 
 #include "common.cuh"
 
@@ -161,21 +162,25 @@ long long place_blocks(const Symbolic& S, std::vector<long long>& off) {
         [&](const CbBlock& a, const CbBlock& b) { return a.need * span(a) > b.need * span(b); },
         [](const CbBlock& a, const CbBlock& b) { return a.hi != b.hi ? a.hi > b.hi : a.need > b.need; },
     };
-    long long best = -1;
-    std::vector<long long> best_at, at;
-    for (const auto& cmp : orders) {
+    // The orders are independent: one thread each.
+    std::vector<long long> top(orders.size());
+    std::vector<std::vector<long long>> at(orders.size());
+    auto run = [&](size_t q) {
         std::vector<int> order(blocks.size());
         std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cmp(blocks[a], blocks[b]); });
-        const long long top = place_in_order(blocks, order, S.num_levels, at);
-        if (best < 0 || top < best) {
-            best = top;
-            best_at.swap(at);
-        }
-    }
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return orders[q](blocks[a], blocks[b]); });
+        top[q] = place_in_order(blocks, order, S.num_levels, at[q]);
+    };
+    std::vector<std::thread> pool;
+    for (size_t q = 1; q < orders.size(); ++q) pool.emplace_back(run, q);
+    run(0);
+    for (std::thread& t : pool) t.join();
+    size_t best = 0;  // the smallest pool; on a tie, the earlier order
+    for (size_t q = 1; q < orders.size(); ++q)
+        if (top[q] < top[best]) best = q;
     off.assign(S.ns, -1);
-    for (size_t i = 0; i < blocks.size(); ++i) off[blocks[i].s] = best_at[i];
-    return std::max(best, 0LL);
+    for (size_t i = 0; i < blocks.size(); ++i) off[blocks[i].s] = at[best][i];
+    return std::max(top[best], 0LL);
 }
 
 }  // namespace
