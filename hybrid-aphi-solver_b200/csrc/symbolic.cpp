@@ -1,9 +1,11 @@
 #include "symbolic.hpp"
 
 #include <algorithm>
+#include <exception>
 #include <functional>
 #include <numeric>
 #include <string>
+#include <system_error>
 #include <thread>
 
 #include "common.cuh"
@@ -162,19 +164,38 @@ long long place_blocks(const Symbolic& S, std::vector<long long>& off) {
         [&](const CbBlock& a, const CbBlock& b) { return a.need * span(a) > b.need * span(b); },
         [](const CbBlock& a, const CbBlock& b) { return a.hi != b.hi ? a.hi > b.hi : a.need > b.need; },
     };
-    // The orders are independent: one thread each.
+    // The orders are independent: one thread each. A thread that cannot be
+    // started runs its order here instead; errors are rethrown once every
+    // thread has been joined.
     std::vector<long long> top(orders.size());
     std::vector<std::vector<long long>> at(orders.size());
+    std::vector<std::exception_ptr> err(orders.size());
     auto run = [&](size_t q) {
-        std::vector<int> order(blocks.size());
-        std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return orders[q](blocks[a], blocks[b]); });
-        top[q] = place_in_order(blocks, order, S.num_levels, at[q]);
+        try {
+            std::vector<int> order(blocks.size());
+            std::iota(order.begin(), order.end(), 0);
+            std::stable_sort(order.begin(), order.end(),
+                             [&](int a, int b) { return orders[q](blocks[a], blocks[b]); });
+            top[q] = place_in_order(blocks, order, S.num_levels, at[q]);
+        } catch (...) {
+            err[q] = std::current_exception();
+        }
     };
-    std::vector<std::thread> pool;
-    for (size_t q = 1; q < orders.size(); ++q) pool.emplace_back(run, q);
-    run(0);
-    for (std::thread& t : pool) t.join();
+    {
+        std::vector<std::thread> pool;
+        pool.reserve(orders.size());
+        for (size_t q = 1; q < orders.size(); ++q) {
+            try {
+                pool.emplace_back(run, q);
+            } catch (const std::system_error&) {
+                run(q);
+            }
+        }
+        run(0);
+        for (std::thread& t : pool) t.join();
+    }
+    for (const std::exception_ptr& e : err)
+        if (e) std::rethrow_exception(e);
     size_t best = 0;  // the smallest pool; on a tie, the earlier order
     for (size_t q = 1; q < orders.size(); ++q)
         if (top[q] < top[best]) best = q;
