@@ -4,6 +4,9 @@ import ctypes
 import re
 from pathlib import Path
 
+import numpy as np
+import pytest
+
 import aphi_b200 as ab
 
 HEADER = Path(__file__).resolve().parents[1] / "include" / "aphi_b200.h"
@@ -75,3 +78,43 @@ def test_plan_stats_account_for_the_same_update_work():
     # the trailing and in-panel updates carry (almost) all of the factorization's flops
     total = simt["update_wide"][2] + simt["update_panel"][2]
     assert 0.9 * an.info["flops"] <= total <= 1.5 * an.info["flops"]
+
+
+def _small_pattern():
+    w = ab.Workload.cylinder(4)
+    return w.row_ptr.copy(), w.col_idx.copy(), ab.amd_ordering(w.row_ptr, w.col_idx)
+
+
+def test_analysis_refuses_malformed_input_on_host():
+    """The analysis refuses what the reference refuses, before any device
+    work: a perm that is not a permutation and malformed upper CSR
+    (std::invalid_argument in the reference: InvalidArgument here), column
+    counts that differ from the pattern's (std::logic_error: LogicError)."""
+    rp, ci, perm = _small_pattern()
+    n = rp.size - 1
+    bad = perm.copy()
+    bad[1] = bad[0]
+    with pytest.raises(ab.InvalidArgument, match="permutation"):
+        ab.Analysis(rp, ci, bad)
+    bad = rp.copy()
+    bad[5] = bad[4] - 1
+    with pytest.raises(ab.InvalidArgument, match="row_ptr decreases"):
+        ab.Analysis(bad, ci, perm)
+    bad = ci.copy()
+    bad[-1] = n
+    with pytest.raises(ab.InvalidArgument, match="out of range"):
+        ab.Analysis(rp, bad, perm)
+    bad = ci.copy()
+    r = 10                       # an entry below the diagonal in an upper pattern
+    bad[rp[r]] = r - 1
+    with pytest.raises(ab.InvalidArgument, match="below the diagonal"):
+        ab.Analysis(rp, bad, perm)
+    an = ab.Analysis(rp, ci, perm)
+    parent, cc = an.etree()
+    wrong = cc.copy()
+    wrong[int(np.argmax(cc))] += 1
+    with pytest.raises(ab.LogicError, match="column counts"):
+        ab.Analysis(rp, ci, perm, parent, wrong)
+    # the analysis of an empty pattern is empty, not an error
+    empty = ab.Analysis(np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32))
+    assert empty.info["n"] == 0 and empty.info["supernodes"] == 0
