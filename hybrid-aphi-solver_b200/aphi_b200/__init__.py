@@ -120,6 +120,7 @@ _SIGS = {
     "aphi_workload_array": (I, [P, C.c_char_p, C.POINTER(P), PI64]),
     "aphi_order_nested_dissection": (I, [I, PI, PI, PD, I, PI]),
     "aphi_order_amd": (I, [I, PI, PI, PI]),
+    "aphi_order_rcm": (I, [I, PI, PI, PI]),
     "aphi_assembly_create": (I, [C.POINTER(AssemblyDesc), C.POINTER(P)]),
     "aphi_assembly_destroy": (I, [P]),
     "aphi_assembly_info": (I, [P, PI64]),
@@ -388,6 +389,17 @@ def amd_ordering(row_ptr, col_idx) -> np.ndarray:
     ci = np.ascontiguousarray(col_idx, np.int32)
     perm = np.zeros(rp.size - 1, np.int32)
     check(lib().aphi_order_amd(rp.size - 1, _ptr(rp, C.c_int), _ptr(ci, C.c_int), _ptr(perm, C.c_int)))
+    return perm
+
+
+def rcm_ordering(row_ptr, col_idx) -> np.ndarray:
+    """The reference's reverse Cuthill-McKee permutation (new -> old),
+    compute_ordering with Ordering::ReverseCuthillMcKee
+    (src/ordering.cpp:105-218, :512-537), bit for bit."""
+    rp = np.ascontiguousarray(row_ptr, np.int32)
+    ci = np.ascontiguousarray(col_idx, np.int32)
+    perm = np.zeros(rp.size - 1, np.int32)
+    check(lib().aphi_order_rcm(rp.size - 1, _ptr(rp, C.c_int), _ptr(ci, C.c_int), _ptr(perm, C.c_int)))
     return perm
 
 

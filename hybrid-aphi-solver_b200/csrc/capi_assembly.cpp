@@ -6,6 +6,7 @@
 #include "assembly.hpp"
 #include "capi_util.hpp"
 #include "common.cuh"
+#include "ordering.hpp"
 #include "workload.hpp"
 
 using namespace aphi_b200;
@@ -35,8 +36,6 @@ void set_last_error(const char* msg) {
 }
 static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
-void nested_dissection(int n, const int* row_ptr, const int* col_idx, const double* xyz, int leaf, int* perm);
-void reference_amd(int n, const int* row_ptr, const int* col_idx, int* perm);
 }
 
 extern "C" {
@@ -153,6 +152,13 @@ int aphi_order_amd(int n, const int* row_ptr, const int* col_idx, int* perm) {
     return guard([&] {
         if (n < 0 || (n > 0 && (!row_ptr || !col_idx || !perm))) throw Error(APHI_ERR_INVALID, "aphi_order_amd: null argument");
         if (n > 0) reference_amd(n, row_ptr, col_idx, perm);
+    });
+}
+
+int aphi_order_rcm(int n, const int* row_ptr, const int* col_idx, int* perm) {
+    return guard([&] {
+        if (n < 0 || (n > 0 && (!row_ptr || !col_idx || !perm))) throw Error(APHI_ERR_INVALID, "aphi_order_rcm: null argument");
+        if (n > 0) reference_rcm(n, row_ptr, col_idx, perm);
     });
 }
 

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "ordering.hpp"
 
 namespace aphi_b200 {
 

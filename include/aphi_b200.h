@@ -102,6 +102,10 @@ int aphi_order_nested_dissection(int n, const int* row_ptr, const int* col_idx, 
  * so a caller without the reference's host code factorizes in the reference's
  * column order. */
 int aphi_order_amd(int n, const int* row_ptr, const int* col_idx, int* perm);
+/* The reference's reverse Cuthill-McKee ordering (compute_ordering with
+ * Ordering::ReverseCuthillMcKee, src/ordering.cpp:105-218 and :512-537), bit
+ * for bit: the same arguments and output as aphi_order_amd. */
+int aphi_order_rcm(int n, const int* row_ptr, const int* col_idx, int* perm);
 
 /* ---- assembly: element fill + deterministic scatter -----------------------
  * Replaces refill(SymmetricSystem&, ...) and refill(AssembledSystem&, ...)

@@ -107,3 +107,35 @@ def test_nested_dissection_is_a_fill_reducing_permutation():
     a_nd = ab.Analysis(w.row_ptr, w.col_idx, nd).info
     a_amd = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx)).info
     assert a_nd["nnz_l"] < 0.8 * a_amd["nnz_l"] and a_nd["flops"] < 0.5 * a_amd["flops"]
+
+
+@pytest.mark.parametrize("kind,cells", [("cylinder", 4), ("cylinder", 8), ("cylinder", 12), ("torus", 16)])
+def test_rcm_matches_reference(kind, cells, ref_or_skip):
+    """The reverse Cuthill-McKee restatement gives the reference's own
+    permutation (compute_ordering with Ordering::ReverseCuthillMcKee) bit for
+    bit, voltage-port rows (isolated vertices) included."""
+    w = getattr(ab.Workload, kind)(cells)
+    r = getattr(ref_or_skip.RefProblem, kind)(cells, ordering=1)
+    np.testing.assert_array_equal(ab.rcm_ordering(w.row_ptr, w.col_idx), r.analysis()["perm"])
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_rcm_and_amd_match_reference_on_random_patterns(seed, ref_or_skip):
+    """Random upper patterns with several components, isolated unknowns and
+    uneven degrees: both orderings equal the reference's."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(50, 600))
+    rows = [{i} for i in range(n)]
+    for i in range(n):
+        for j in rng.integers(0, n, size=int(rng.integers(0, 5))):
+            if j != i and rng.random() < 0.8:
+                rows[min(i, j)].add(max(i, j))
+    rp = np.zeros(n + 1, np.int32)
+    ci = []
+    for i, r in enumerate(rows):
+        ci += sorted(r)
+        rp[i + 1] = len(ci)
+    ci = np.array(ci, np.int32)
+    for code, fn in ((1, ab.rcm_ordering), (2, ab.amd_ordering)):
+        ref = ref_or_skip.RefProblem.from_pattern(rp, ci, ordering=code)
+        np.testing.assert_array_equal(fn(rp, ci), ref.analysis()["perm"])
