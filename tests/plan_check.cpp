@@ -36,14 +36,12 @@
 #include <vector>
 
 #include "analysis.hpp"
+#include "ordering.hpp"
 #include "workload.hpp"
 extern "C" {
 #include "oracle.h"
 }
 
-namespace aphi_b200 {
-void reference_amd(int n, const int* row_ptr, const int* col_idx, int* perm_out);
-}
 
 using namespace aphi_b200;
 using C = std::complex<double>;
