@@ -205,7 +205,7 @@ def test_multiple_rhs_and_residuals(cuda, ref_or_skip):
     x = f.solve(b)
     res = ab.residuals(an, vals, x, b)
     assert res.shape == (1, 5, 2)
-    # Random right-hand sides on an ill-conditioned system: judge by the
+    # Random right-hand sides on an ill-conditioned system: measured by the
     # backward error (the relative residual scales with the condition number).
     assert (res[..., 1] <= 1e-15).all(), res
     for k in range(5):
