@@ -56,7 +56,7 @@ def test_torus_refusals():
         ab.Workload.torus(12)   # the tube is too thin for a conductor face on the cut
 
 
-def test_config1_sizes():
+def test_cylinder_6_sizes():
     """6^3 cells: the sizes the reference reports for this problem
     (1,296 tets, 1,358 unknowns = 1,081 A + 275 Phi + 2 ports, 15,164 stored)."""
     w = ab.Workload.cylinder(6)
