@@ -160,10 +160,11 @@ def cpu_reference(cells_sample: int, cells_target: int, procs: int):
     rate_sample = procs / per
     ratio = flops[cells_target] / flops[cells_sample]
     return {"value": rate_sample / ratio, "unit": UNIT, "cores": procs, "kind": "reference",
-            "sample": (f"{procs} concurrent single-threaded reference solve_symmetric calls (refill + "
-                       f"equilibrated FP64 up-looking LDL^T + solve), one {cells_sample}^3 frequency each, "
-                       f"{per:.1f} s; scaled to {cells_target}^3 by its {ratio:.1f}x factorization flops "
-                       f"({flops[cells_target]:.3e} vs {flops[cells_sample]:.3e})"),
+            "sample": ((f"{procs} concurrent single-threaded reference solve_symmetric calls"
+                        if procs > 1 else "one single-threaded reference solve_symmetric call")
+                       + f" (refill + equilibrated FP64 up-looking LDL^T + solve), one {cells_sample}^3 frequency"
+                       + (" each" if procs > 1 else "") + f", {per:.1f} s; scaled to {cells_target}^3 by its "
+                       f"{ratio:.1f}x factorization flops ({flops[cells_target]:.3e} vs {flops[cells_sample]:.3e})"),
             "sample_wall_s": wall, "sample_solve_s": per}
 
 
