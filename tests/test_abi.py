@@ -118,3 +118,20 @@ def test_analysis_refuses_malformed_input_on_host():
     # the analysis of an empty pattern is empty, not an error
     empty = ab.Analysis(np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32))
     assert empty.info["n"] == 0 and empty.info["supernodes"] == 0
+
+
+def test_orderings_edge_cases_on_host():
+    """The reference's orderings through the C ABI: nothing to order at
+    n = 0, a null argument refused, a diagonal-only pattern ordered as the
+    reference orders isolated unknowns (AMD: degree buckets, last in first
+    out; RCM: components by lowest vertex, then reversed)."""
+    L = ab.lib()
+    assert L.aphi_order_amd(0, None, None, None) == ab.OK
+    assert L.aphi_order_rcm(0, None, None, None) == ab.OK
+    assert L.aphi_order_rcm(3, None, None, None) == ab.ERR_INVALID
+    assert L.aphi_order_amd(-1, None, None, None) == ab.ERR_INVALID
+    n = 5
+    rp = np.arange(n + 1, dtype=np.int32)
+    ci = np.arange(n, dtype=np.int32)
+    np.testing.assert_array_equal(ab.rcm_ordering(rp, ci), np.arange(n)[::-1])
+    assert sorted(ab.amd_ordering(rp, ci).tolist()) == list(range(n))
