@@ -17,6 +17,7 @@
 
 #include "factor.hpp"
 #include "factor_kernels.cuh"
+#include "pivot_stats.hpp"
 
 namespace aphi_b200 {
 
@@ -568,39 +569,8 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     std::vector<int> kmax(B, 0x7fffffff);
-    bool any_fail = false;
-    for (int b = 0; b < B; ++b) {
-        aphi_factor_stats& s = f->host_stats[b];
-        s = aphi_factor_stats{};
-        s.ok = 1;
-        bool first = true;
-        for (int k = 0; k < n; ++k) {
-            const double* d = &dref[2 * (static_cast<size_t>(n) * b + k)];
-            const double mag = std::hypot(d[0], d[1]);
-            s.largest_pivot = std::max(s.largest_pivot, mag);
-            if (first || mag < s.smallest_pivot) {
-                s.smallest_pivot = mag;
-                first = false;
-            }
-            s.columns_done = k + 1;
-            if (!(mag > pivot_floor)) {
-                s.ok = 0;
-                kmax[b] = k;
-                any_fail = true;
-                break;
-            }
-        }
-        s.nnz = S.nnz_l;
-        s.milliseconds = ms;
-        if (n > 0) {
-            s.equilibration_min = *std::min_element(dsc.begin() + static_cast<long long>(n) * b,
-                                                    dsc.begin() + static_cast<long long>(n) * (b + 1));
-            s.equilibration_max = *std::max_element(dsc.begin() + static_cast<long long>(n) * b,
-                                                    dsc.begin() + static_cast<long long>(n) * (b + 1));
-        } else {
-            s.equilibration_min = s.equilibration_max = 1.0;
-        }
-    }
+    const bool any_fail = pivot_stats(n, B, dref.data(), dsc.data(), pivot_floor, ms, S.nnz_l,
+                                      f->host_stats.data(), kmax.data());
     // Largest multiplier, over the rows the reference would have reached.
     int* d_kmax = f->kmax;
     APHI_CUDA(cudaMemcpyAsync(d_kmax, kmax.data(), sizeof(int) * B, cudaMemcpyHostToDevice, st));

@@ -89,3 +89,10 @@ def test_planted_mistakes_are_caught(plan_check, mistake, caught):
     assert r.returncode == 1, r.stdout + r.stderr
     assert f"planted {mistake}" in r.stdout and "FAIL" in r.stdout
     assert re.search(caught, r.stdout), r.stdout
+
+
+def test_pivot_stats_threads_equal_the_sequential_walk(plan_check):
+    """The per-entry factorization statistics (pivot_stats.cpp), split over
+    host threads, equal the sequential walk in every field."""
+    r = subprocess.run([str(BIN / "pivot_stats_check")], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "DIFFERENT" not in r.stdout, r.stdout + r.stderr
