@@ -285,7 +285,14 @@ void analysis_destroy(aphi_analysis* a) { delete a; }
 // Device copies are made when the first factor is created, so an analysis can
 // be built and inspected on a host without a GPU.
 void analysis_ensure_device(aphi_analysis* A) {
-    if (A->on_device) return;
+    int dev = 0;
+    APHI_CUDA(cudaGetDevice(&dev));
+    if (A->on_device) {
+        if (dev != A->device)
+            throw Error(APHI_ERR_INVALID, "the analysis's device copy lives on device " + std::to_string(A->device) +
+                                              ", but device " + std::to_string(dev) + " is current");
+        return;
+    }
     const Symbolic& S = A->S;
     long long& b = A->device_bytes;
     DeviceSchedule& d = A->d;
@@ -310,6 +317,7 @@ void analysis_ensure_device(aphi_analysis* A) {
     d.fcol = upload(A->h_fcol, b);
     d.fmap = upload(A->h_fmap, b);
     d.items = upload(A->h_items, b);
+    A->device = dev;
     A->on_device = true;
 }
 

@@ -95,6 +95,7 @@ struct aphi_analysis {
     std::vector<int> h_fptr, h_fcol;
     std::vector<long long> h_fmap;
     bool on_device = false;
+    int device = -1;       // the CUDA device holding the device copy (set with it)
     bool fronts = false;   // built from independent dense fronts (no matrix pattern)
     void* ws = nullptr;    // contribution-block workspace shared by this analysis's factors
     size_t ws_bytes = 0;

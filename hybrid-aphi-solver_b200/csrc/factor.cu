@@ -645,8 +645,13 @@ struct ThreadScratch {
 };
 thread_local ThreadScratch t_residual_scratch;
 
+constexpr long long kMaxGridY = 65535;  // grid.y limit of the residual kernels (one system per y)
+
 void residuals(const aphi_analysis* an, int batch, int nrhs, const double* values, const double* x,
                const double* b, double* out, cudaStream_t st) {
+    if (static_cast<long long>(batch) * nrhs > kMaxGridY)
+        throw Error(APHI_ERR_BAD_SHAPE, "residuals: batch x nrhs exceeds the " + std::to_string(kMaxGridY) +
+                                            " systems one call handles");
     const int n = an->S.n;
     const int nb = ceil_div(std::max(n, 1), 256);
     const size_t np = static_cast<size_t>(nb) * 3 * batch * nrhs;
@@ -704,11 +709,9 @@ namespace {
 // Device address of the scratch array, looked up once per device with that
 // device current. In host code the array's name stands for a host-side
 // shadow, not a device address, so it is never handed to a kernel directly.
-double* residual_scratch() {
+double* residual_scratch(int dev) {
     static std::mutex mu;
     static double* ptrs[64] = {};
-    int dev = 0;
-    APHI_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) throw Error(APHI_ERR_INVALID, "residuals_noalloc: device ordinal out of range");
     std::lock_guard<std::mutex> lock(mu);
     if (!ptrs[dev]) {
@@ -730,9 +733,19 @@ void residuals_noalloc(const aphi_analysis* an, int batch, int nrhs, const doubl
         throw Error(APHI_ERR_INVALID,
                     "residuals_noalloc: the analysis has no device copy yet (create a factor from it first); "
                     "this entry point does not allocate one");
+    int dev = 0;
+    APHI_CUDA(cudaGetDevice(&dev));
+    if (dev != an->device)
+        throw Error(APHI_ERR_INVALID, "residuals_noalloc: the analysis's device copy lives on device " +
+                                          std::to_string(an->device) + ", but device " + std::to_string(dev) +
+                                          " is current");
     const int n = an->S.n;
     const long long nb = ceil_div(std::max(n, 1), 256);
     const long long q = static_cast<long long>(batch) * nrhs;
+    if (q > kMaxGridY || batch > kMaxGridY)
+        throw Error(APHI_ERR_BAD_SHAPE, "residuals_noalloc: batch x nrhs = " + std::to_string(q) +
+                                            " exceeds the " + std::to_string(kMaxGridY) +
+                                            " systems one call handles");
     // partial sums, max|A| words (one per batch entry), norms, ratios
     const long long need = nb * 3 * q + batch + 4 * q + 2 * q;
     if (need > static_cast<long long>(kResidualScratchDoubles))
@@ -741,7 +754,7 @@ void residuals_noalloc(const aphi_analysis* an, int batch, int nrhs, const doubl
                         " right-hand sides need " + std::to_string(need) + " doubles of scratch; the fixed "
                         "array holds " + std::to_string(kResidualScratchDoubles) +
                         " (use aphi_residuals, which allocates, or fewer right-hand sides per call)");
-    double* scratch = residual_scratch();
+    double* scratch = residual_scratch(an->device);
     double* partial = scratch;
     unsigned long long* amax = reinterpret_cast<unsigned long long*>(scratch + nb * 3 * q);
     double* norms = scratch + nb * 3 * q + batch;

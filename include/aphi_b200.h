@@ -300,13 +300,15 @@ int aphi_residuals(const aphi_analysis* an, int batch, int nrhs, const double* v
  * latency-critical path that cannot take cudaFree's device-wide
  * synchronization. No counterpart in the reference. Its scratch is one
  * fixed-size device array inside this library (8 MiB per GPU that loads it,
- * held until exit); sizes needing more -- roughly ceil(N/256) * 3 * batch *
- * nrhs doubles -- are refused with BAD_SHAPE. The analysis must already have
- * a device copy (any factor created from it makes one), or INVALID is
- * returned. The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * All calls share the array: calls that overlap on the GPU race on it, so
- * callers must order them. */
+ * held until exit); sizes needing more -- ceil(N/256) * 3 * batch * nrhs +
+ * batch + 6 * batch * nrhs doubles -- are refused with BAD_SHAPE, and so is
+ * batch * nrhs above 65535. The analysis must already have a device copy
+ * (any factor created from it makes one) on the current device, or INVALID
+ * is returned. The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture. Every call is synchronous on its stream: it returns once the
+ * ratios are in `out`. All calls share the array: calls that overlap on the
+ * GPU race on it, so callers must order them. */
 int aphi_residuals_noalloc(const aphi_analysis* an, int batch, int nrhs, const double* values_dev,
                            const double* x_dev, const double* b_dev, double* out, void* stream);
 
