@@ -162,6 +162,11 @@ _SIGS = {
     "aphi_solve_host": (I, [P, I, PD, PD]),
     "aphi_residuals_host": (I, [P, I, I, PD, PD, PD, PD]),
     "aphi_factor_profile_read": (I, [P, PD, PI64]),
+    "aphi_assembly_create_device_setup": (I, [C.POINTER(AssemblyDesc), C.POINTER(P)]),
+    "aphi_assembly_maps": (I, [P, PI64, PI, PI]),
+    "aphi_pattern_build": (I, [I, I, PI, I, PI, I, PI, PI, C.c_int64, PI64]),
+    "aphi_csc_solve_host": (I, [I, PI, PI, PD, PD, I, PD]),
+    "aphi_csr_residuals_host": (I, [I, PI, PI, PD, I, PD, PD, PD]),
 }
 
 
@@ -367,6 +372,27 @@ def assembly_desc_from(arrays: dict, upper_only: bool = True):
     return d, keep
 
 
+def pattern_build(n: int, tet_idx, diag_rows=(), upper_only: bool = True):
+    """build_sparsity (src/sparsity.cpp:19-136) on the device from the tets' 16
+    DOF indices each plus the voltage-port diagonal rows: (row_ptr, col_idx)."""
+    ti = np.ascontiguousarray(tet_idx, np.int32)
+    dr = np.ascontiguousarray(diag_rows, np.int32)
+    rp = np.zeros(n + 1, np.int32)
+    nnz = C.c_int64(0)
+    cap = max(16 * ti.size, 1)
+    ci = np.zeros(cap, np.int32)
+    rc = lib().aphi_pattern_build(n, ti.size // 16, ti.ctypes.data_as(PI), dr.size, dr.ctypes.data_as(PI),
+                                  1 if upper_only else 0, rp.ctypes.data_as(PI), ci.ctypes.data_as(PI), cap,
+                                  C.byref(nnz))
+    if rc == ERR_BAD_SHAPE and nnz.value > cap:
+        ci = np.zeros(nnz.value, np.int32)
+        rc = lib().aphi_pattern_build(n, ti.size // 16, ti.ctypes.data_as(PI), dr.size, dr.ctypes.data_as(PI),
+                                      1 if upper_only else 0, rp.ctypes.data_as(PI), ci.ctypes.data_as(PI),
+                                      nnz.value, C.byref(nnz))
+    check(rc)
+    return rp, ci[: nnz.value]
+
+
 def workload_arrays(w: Workload) -> dict:
     return {k: w.array(k) for k in Workload.ARRAYS}
 
@@ -438,11 +464,15 @@ class Assembly:
     """Device assembly for one mesh: refill at any frequency (refill,
     src/assembly.cpp:453-494). Values and rhs are complex128 device tensors."""
 
-    def __init__(self, arrays: dict, upper_only: bool = True):
+    def __init__(self, arrays: dict, upper_only: bool = True, device_setup: bool = True):
+        """device_setup: build the per-mesh scatter maps (term destinations
+        and slot -> term lists) on the device; False builds the same arrays on
+        the host."""
         desc, keep = assembly_desc_from(arrays, upper_only)
         self.num_tets = int(desc.num_tets)
         self._h = P()
-        check(lib().aphi_assembly_create(C.byref(desc), C.byref(self._h)))
+        create = lib().aphi_assembly_create_device_setup if device_setup else lib().aphi_assembly_create
+        check(create(C.byref(desc), C.byref(self._h)))
         info = (C.c_int64 * 4)()
         check(lib().aphi_assembly_info(self._h, info))
         self.nnz, self.num_unknowns, self.num_terms, self.device_bytes = list(info)
@@ -458,6 +488,15 @@ class Assembly:
         check(lib().aphi_refill_batch(self._h, nf, _ptr(omegas, C.c_double), conditioning,
                                       dptr(values), dptr(rhs), stream_ptr(stream)))
         return values, rhs
+
+    def maps(self):
+        """(term_off [T+1], dest_ptr [nnz+N+1], dest_terms [num_terms]) on the host."""
+        to = np.zeros(self.num_tets + 1, np.int64)
+        dp = np.zeros(self.nnz + self.num_unknowns + 1, np.int32)
+        dt = np.zeros(max(self.num_terms, 1), np.int32)
+        check(lib().aphi_assembly_maps(self._h, to.ctypes.data_as(PI64), dp.ctypes.data_as(PI),
+                                       dt.ctypes.data_as(PI)))
+        return to, dp, dt[: self.num_terms]
 
     def refill_host(self, omega: float, conditioning=COND_ROW_SCALED):
         v = np.zeros(self.nnz, np.complex128)

@@ -29,6 +29,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O2,-pthread",
 # Element fill and scatter reproduce the host's rounding: no FMA contraction.
 PER_FILE = {
     "assembly.cu": ["-fmad=false"],
+    "csc_solve.cu": ["-fmad=false"],
 }
 
 

@@ -8,16 +8,20 @@
 //
 // Design. The reference accumulates `values[slot] += term` while it walks
 // bodies -> tets -> (AA, A-Phi/Phi-A, Phi-Phi) blocks. Here
-//   K1 (k_tet_terms): one thread per tet computes the tet's geometry and its
-//       element blocks and writes every term it contributes -- already scaled
-//       exactly as the reference forms the addend -- into a term array, in the
-//       reference's loop order. Terms bound for the right-hand side are stored
-//       negated (the reference subtracts them).
-//   K2 (k_slot_sum): one thread per destination (CSR slot or rhs row) sums its
-//       terms in increasing term order through a slot -> term list built once
-//       per mesh. Increasing term order IS the reference's accumulation order,
-//       so the sums are bitwise those of the reference: no float atomics, no
-//       order that depends on scheduling.
+//   K1 (k_tet_terms): one warp per tet, for every frequency of the batch,
+//       stages the tet's tables and its frequency-independent geometry
+//       (barycentric gradients, curls, Whitney values and P2 gradients at the
+//       quadrature points) in shared memory, enumerates the tet's terms in
+//       the reference's emission order, and computes (term, frequency) pairs
+//       across its lanes -- each already scaled exactly as the reference forms
+//       the addend -- into a term array, stored frequency-minor. Terms bound
+//       for the right-hand side are stored negated (the reference subtracts
+//       them).
+//   K2 (k_slot_sum): one thread per (destination, frequency) -- CSR slot or
+//       rhs row -- sums its terms in increasing term order through a slot ->
+//       term list built once per mesh. Increasing term order IS the
+//       reference's accumulation order, so the sums are bitwise those of the
+//       reference: no float atomics, no order that depends on scheduling.
 // This file is compiled with -fmad=false and uses explicitly rounded
 // intrinsics for complex products, so every element entry and every addend is
 // rounded exactly as the host's std::complex<double> arithmetic rounds it.
@@ -30,6 +34,7 @@
 
 #include "assembly.hpp"
 #include "common.cuh"
+#include "setup.hpp"
 
 namespace aphi_b200 {
 
@@ -261,7 +266,6 @@ struct TetArgs {
     const double* tet_coeff;
     const double* tet_fixed;
     const long long* term_off;
-    long long stride;  // terms per frequency
     int* err;          // [0] degenerate tet, [1] term count mismatch
 };
 
@@ -270,99 +274,303 @@ struct Omegas {
     double w[kMaxBatchOmegas];
 };
 
-__global__ void __launch_bounds__(128) k_tet_terms(TetArgs A, Omegas om, int cond, Quad quad,
-                                                    cplx* terms) {
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    const int f = blockIdx.y;
-    if (v >= A.num_tets) return;
-    const double omega = om.w[f];
+// compute_tet_geometry's Gauss-Jordan inverse with every index static (the
+// pivot row swap is a predicated exchange), so the 4 x 4 arrays stay in
+// registers. The same operations on the same values, in the same order, as
+// tet_geometry above: bitwise the same result.
+__device__ __forceinline__ bool tet_geometry_reg(const double (&p)[4][3], double (&grad)[4][3], double& volume) {
+    double m[4][4], inv[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        m[r][0] = 1.0;
+        m[r][1] = p[r][0];
+        m[r][2] = p[r][1];
+        m[r][3] = p[r][2];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) inv[r][c] = (r == c) ? 1.0 : 0.0;
+    }
+#pragma unroll
+    for (int col = 0; col < 4; ++col) {
+        int prow = col;
+        double pval = fabs(m[col][col]);
+#pragma unroll
+        for (int r = col + 1; r < 4; ++r)
+            if (fabs(m[r][col]) > pval) {
+                prow = r;
+                pval = fabs(m[r][col]);
+            }
+        if (pval < 1e-14) return false;
+#pragma unroll
+        for (int r = col + 1; r < 4; ++r) {
+            const bool sw = r == prow;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const double a = m[r][c], b = m[col][c];
+                m[r][c] = sw ? b : a;
+                m[col][c] = sw ? a : b;
+                const double x = inv[r][c], y = inv[col][c];
+                inv[r][c] = sw ? y : x;
+                inv[col][c] = sw ? x : y;
+            }
+        }
+        const double piv = m[col][col];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            m[col][c] = __ddiv_rn(m[col][c], piv);
+            inv[col][c] = __ddiv_rn(inv[col][c], piv);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            if (r == col) continue;
+            const double f = m[r][col];
+            if (f == 0.0) continue;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                m[r][c] = __dsub_rn(m[r][c], __dmul_rn(f, m[col][c]));
+                inv[r][c] = __dsub_rn(inv[r][c], __dmul_rn(f, inv[col][c]));
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        grad[i][0] = inv[1][i];
+        grad[i][1] = inv[2][i];
+        grad[i][2] = inv[3][i];
+    }
+    double a[3], b[3], c[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        a[k] = __dsub_rn(p[1][k], p[0][k]);
+        b[k] = __dsub_rn(p[2][k], p[0][k]);
+        c[k] = __dsub_rn(p[3][k], p[0][k]);
+    }
+    const double x = __dsub_rn(__dmul_rn(a[1], b[2]), __dmul_rn(a[2], b[1]));
+    const double y = __dsub_rn(__dmul_rn(a[2], b[0]), __dmul_rn(a[0], b[2]));
+    const double z = __dsub_rn(__dmul_rn(a[0], b[1]), __dmul_rn(a[1], b[0]));
+    const double dot = __dadd_rn(__dadd_rn(__dmul_rn(x, c[0]), __dmul_rn(y, c[1])), __dmul_rn(z, c[2]));
+    volume = fabs(__ddiv_rn(dot, 6.0));
+    return true;
+}
+
+// Term kinds of the scatter (src/assembly.cpp:268-394), in emission order
+// within a tet: (A,A); (A,Phi) or its prescribed-Phi rhs term, then (Phi,A);
+// (Phi,Phi) or its prescribed-Phi rhs term.
+enum : int { T_AA = 0, T_AP = 1, T_AP_FIXED = 2, T_PA = 3, T_PP = 4, T_PP_FIXED = 5 };
+
+constexpr int kTetWarps = 4;          // tets (warps) per block
+constexpr int kTetMaxTerms = 256;     // 36 + 120 + 100 at most (full storage)
+
+// Per-warp staging: the tet's tables, geometry and the frequency-independent
+// vectors of its element blocks (curls; Whitney values and P2 gradients at
+// the four quadrature points), and its term list.
+struct TetStage {
+    double grad[4][3];
+    double curl[6][3];
+    double wv[4][6][3];
+    double gr[4][10][3];
+    double fixed[10][2];
+    double co[16];
+    double p[4][3];
+    double mat[3];
+    double volume;
+    int idx[16];
+    unsigned short rec[kTetMaxTerms];  // kind << 8 | i << 4 | j
+};
+
+__device__ __forceinline__ double dot3s(const double* u, const double* v) { return dot3(u, v); }
+
+// K1: one warp per tet (in the reference's body -> tet visit order), all the
+// batch's frequencies. The warp stages the tet once, enumerates its terms in
+// the reference's emission order (a warp scan over the 36 + 60 + 100 block
+// positions), then computes (term, frequency) pairs across its lanes: each
+// pair's element entry is rebuilt from the staged vectors with the reference's
+// accumulation over the quadrature points, and scaled exactly as the reference
+// forms its addend. Terms are stored frequency-minor, terms[t * nf + f], so a
+// warp's stores are contiguous and the slot sums read 16 * nf contiguous
+// bytes per term.
+__global__ void __launch_bounds__(32 * kTetWarps) k_tet_terms(TetArgs A, Omegas om, int cond, Quad quad,
+                                                              cplx* terms) {
+    __shared__ TetStage stage[kTetWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int v = blockIdx.x * kTetWarps + warp;
+    if (v >= A.num_tets) return;  // uniform per warp
+    TetStage& S = stage[warp];
     const int t = A.visit_tet[v];
     const int b = A.visit_body[v];
-    const Coeff c = body_coefficients(A.material[3 * b], A.material[3 * b + 1], A.material[3 * b + 2], omega);
-    const Scales sc = scales_of(cond, omega);
+    if (lane < 16) {
+        S.idx[lane] = A.tet_idx[16LL * t + lane];
+        S.co[lane] = A.tet_coeff[16LL * t + lane];
+    }
+    if (lane < 20) (&S.fixed[0][0])[lane] = A.tet_fixed[20LL * t + lane];
+    if (lane < 12) S.p[lane / 3][lane % 3] = A.xyz[3LL * A.tets[4LL * t + lane / 3] + lane % 3];
+    if (lane < 3) S.mat[lane] = A.material[3 * b + lane];
+    __syncwarp();
+    const bool fixed_lane = lane < 10 && !(S.fixed[lane][0] == 0.0 && S.fixed[lane][1] == 0.0);
+    const unsigned fixed_mask = __ballot_sync(0xffffffffu, fixed_lane);
+    const bool need_phi = __ballot_sync(0xffffffffu, lane < 10 && (S.idx[6 + lane] >= 0 || fixed_lane)) != 0;
 
-    int idx[16];
-    double co[16];
-    bool fixed_nz[10];
-    cplx fixed[10];
-    bool need_phi = false;
-    for (int q = 0; q < 16; ++q) {
-        idx[q] = A.tet_idx[16LL * t + q];
-        co[q] = A.tet_coeff[16LL * t + q];
+    // Geometry: every lane computes it (uniform control flow); lane 0 stages it.
+    {
+        double p[4][3], grad[4][3], vol;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) p[r][k] = S.p[r][k];
+        if (!tet_geometry_reg(p, grad, vol)) {
+            if (lane == 0) atomicExch(&A.err[0], 1);
+            return;
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) S.grad[r][k] = grad[r][k];
+            S.volume = vol;
+        }
     }
-    for (int q = 0; q < 10; ++q) {
-        fixed[q] = cplx{A.tet_fixed[20LL * t + 2 * q], A.tet_fixed[20LL * t + 2 * q + 1]};
-        fixed_nz[q] = !(fixed[q].re == 0.0 && fixed[q].im == 0.0);
-        if (idx[6 + q] >= 0 || fixed_nz[q]) need_phi = true;
+    __syncwarp();
+    // Curls (6), Whitney values (4 points x 6 edges), P2 gradients (4 x 10).
+    const int nvec = need_phi ? 70 : 30;
+    for (int it = lane; it < nvec; it += 32) {
+        if (it < 6) {
+            const double* u = S.grad[c_edge_verts[it][0]];
+            const double* w = S.grad[c_edge_verts[it][1]];
+            S.curl[it][0] = __dmul_rn(__dsub_rn(__dmul_rn(u[1], w[2]), __dmul_rn(u[2], w[1])), 2.0);
+            S.curl[it][1] = __dmul_rn(__dsub_rn(__dmul_rn(u[2], w[0]), __dmul_rn(u[0], w[2])), 2.0);
+            S.curl[it][2] = __dmul_rn(__dsub_rn(__dmul_rn(u[0], w[1]), __dmul_rn(u[1], w[0])), 2.0);
+        } else {
+            const int q = it < 30 ? (it - 6) / 6 : (it - 30) / 10;
+            // barycentric coordinate i of quadrature point q: (a, b, b, b) permuted
+            auto L = [&](int i) { return i == q ? quad.a : quad.b; };
+            if (it < 30) {
+                const int e = (it - 6) % 6;
+                const int vi = c_edge_verts[e][0], vj = c_edge_verts[e][1];
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    S.wv[q][e][k] = __dsub_rn(__dmul_rn(S.grad[vj][k], L(vi)), __dmul_rn(S.grad[vi][k], L(vj)));
+            } else {
+                const int bb = (it - 30) % 10;
+                if (bb < 4) {
+                    const double sc = __dsub_rn(__dmul_rn(4.0, L(bb)), 1.0);
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) S.gr[q][bb][k] = __dmul_rn(S.grad[bb][k], sc);
+                } else {
+                    const int v0 = c_edge_verts[bb - 4][0], v1 = c_edge_verts[bb - 4][1];
+                    const double s0 = __dmul_rn(4.0, L(v1)), s1 = __dmul_rn(4.0, L(v0));
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
+                        S.gr[q][bb][k] = __dadd_rn(__dmul_rn(S.grad[v0][k], s0), __dmul_rn(S.grad[v1][k], s1));
+                }
+            }
+        }
     }
-
-    double p[4][3];
-    for (int q = 0; q < 4; ++q) {
-        const int node = A.tets[4LL * t + q];
-        p[q][0] = A.xyz[3LL * node];
-        p[q][1] = A.xyz[3LL * node + 1];
-        p[q][2] = A.xyz[3LL * node + 2];
+    // The tet's terms in emission order: block positions AA (36), then
+    // (A,Phi) pairs (60, up to two terms each) and (Phi,Phi) (100).
+    const bool up = A.upper_only != 0;
+    const int ncand = need_phi ? 196 : 36;
+    int total = 0;
+    for (int c0 = 0; c0 < ncand; c0 += 32) {
+        const int c = c0 + lane;
+        int n = 0, r0 = 0, r1 = 0;
+        if (c < 36) {
+            const int pi = c / 6, qi = c % 6;
+            if (S.idx[pi] >= 0 && S.idx[qi] >= 0 && !(up && S.idx[qi] < S.idx[pi])) {
+                n = 1;
+                r0 = T_AA << 8 | pi << 4 | qi;
+            }
+        } else if (c < 96) {
+            const int pi = (c - 36) / 10, qi = (c - 36) % 10;
+            const int row = S.idx[pi], col = S.idx[6 + qi];
+            if (row >= 0) {
+                if (col >= 0) {
+                    if (!(up && col < row)) r0 = T_AP << 8 | pi << 4 | qi, n = 1;
+                    if (!(up && row < col)) (n ? r1 : r0) = T_PA << 8 | pi << 4 | qi, ++n;
+                } else if ((fixed_mask >> qi) & 1u) {
+                    r0 = T_AP_FIXED << 8 | pi << 4 | qi;
+                    n = 1;
+                }
+            }
+        } else if (c < 196) {
+            const int pi = (c - 96) / 10, qi = (c - 96) % 10;
+            const int row = S.idx[6 + pi], col = S.idx[6 + qi];
+            if (row >= 0) {
+                if (col >= 0) {
+                    if (!(up && col < row)) r0 = T_PP << 8 | pi << 4 | qi, n = 1;
+                } else if ((fixed_mask >> qi) & 1u) {
+                    r0 = T_PP_FIXED << 8 | pi << 4 | qi;
+                    n = 1;
+                }
+            }
+        }
+        int incl = n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int at = total + incl - n;
+        if (n > 0) S.rec[at] = static_cast<unsigned short>(r0);
+        if (n > 1) S.rec[at + 1] = static_cast<unsigned short>(r1);
+        total += __shfl_sync(0xffffffffu, incl, 31);
     }
-    Geometry g;
-    if (!tet_geometry(p, g)) {
-        atomicExch(&A.err[0], 1);
+    const long long off = A.term_off[v];
+    if (total != A.term_off[v + 1] - off) {
+        if (lane == 0) atomicExch(&A.err[1], 1);
         return;
     }
-    cplx aa[36], ap[60], pp[100];
-    element_blocks(g, c, quad, need_phi, aa, ap, pp);
-
-    cplx* out = terms + f * A.stride + A.term_off[v];
-    long long k = 0;
-    const bool up = A.upper_only != 0;
-    // (A, A)
-    for (int pi = 0; pi < 6; ++pi) {
-        if (idx[pi] < 0) continue;
-        for (int qi = 0; qi < 6; ++qi) {
-            if (idx[qi] < 0) continue;
-            if (up && idx[qi] < idx[pi]) continue;
-            out[k++] = cscale_exact(aa[pi * 6 + qi], __dmul_rn(co[pi], co[qi]));
-        }
-    }
-    if (need_phi) {
-        const cplx rjw = cmul_exact(sc.row, sc.jw);
-        // (A, Phi) and (Phi, A)
-        for (int pi = 0; pi < 6; ++pi) {
-            if (idx[pi] < 0) continue;
-            for (int qi = 0; qi < 10; ++qi) {
-                const int col = idx[6 + qi];
-                const cplx blk = ap[pi * 10 + qi];
-                if (col >= 0) {
-                    if (!(up && col < idx[pi]))
-                        out[k++] = cmul_exact(cscale_exact(sc.col, __dmul_rn(co[pi], co[6 + qi])), blk);
-                } else if (fixed_nz[qi]) {
-                    const cplx fx = cdiv_smith(fixed[qi], sc.col);
-                    out[k++] = cneg(cmul_exact(cmul_exact(cscale_exact(sc.col, co[pi]), blk), fx));
-                }
-                if (col >= 0) {
-                    if (!(up && idx[pi] < col))
-                        out[k++] = cmul_exact(cscale_exact(rjw, __dmul_rn(co[6 + qi], co[pi])), blk);
-                }
+    __syncwarp();
+    const int nf = om.n;
+    const double vol = S.volume;
+    const double w = __dmul_rn(0.25, vol);
+    cplx* out = terms + off * nf;
+    for (int it = lane; it < total * nf; it += 32) {
+        const int k = it / nf, f = it - k * nf;
+        const int r = S.rec[k];
+        const int kind = r >> 8, i = (r >> 4) & 15, j = r & 15;
+        const double omega = om.w[f];
+        const Coeff c = body_coefficients(S.mat[0], S.mat[1], S.mat[2], omega);
+        cplx blk{0.0, 0.0};
+        if (kind == T_AA) {
+            // kernel_AA: nu V curl.curl, then the mass term point by point.
+            blk = cplx{__dmul_rn(__dmul_rn(c.nu, vol), dot3s(S.curl[i], S.curl[j])), 0.0};
+            if (!(c.alpha.re == 0.0 && c.alpha.im == 0.0))
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    blk = cadd_exact(blk, cscale_exact(c.alpha, __dmul_rn(w, dot3s(S.wv[q][i], S.wv[q][j]))));
+        } else if (!(c.beta.re == 0.0 && c.beta.im == 0.0)) {
+            // kernel_APhi / kernel_PhiPhi
+            const bool pp = kind >= T_PP;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double* u = pp ? S.gr[q][i] : S.wv[q][i];
+                blk = cadd_exact(blk, cscale_exact(c.beta, __dmul_rn(w, dot3s(u, S.gr[q][j]))));
             }
         }
-        // (Phi, Phi)
-        const cplx rc = cmul_exact(sc.row, sc.col);
-        for (int pi = 0; pi < 10; ++pi) {
-            const int row = idx[6 + pi];
-            if (row < 0) continue;
-            for (int qi = 0; qi < 10; ++qi) {
-                const int col = idx[6 + qi];
-                const cplx blk = pp[pi * 10 + qi];
-                if (col >= 0) {
-                    if (!(up && col < row))
-                        out[k++] = cmul_exact(cscale_exact(rc, __dmul_rn(co[6 + pi], co[6 + qi])), blk);
-                } else if (fixed_nz[qi]) {
-                    const cplx fx = cdiv_smith(fixed[qi], sc.col);
-                    out[k++] = cneg(cmul_exact(cmul_exact(cscale_exact(rc, co[6 + pi]), blk), fx));
-                }
+        const Scales sc = scales_of(cond, omega);
+        cplx term;
+        switch (kind) {
+            case T_AA: term = cscale_exact(blk, __dmul_rn(S.co[i], S.co[j])); break;
+            case T_AP: term = cmul_exact(cscale_exact(sc.col, __dmul_rn(S.co[i], S.co[6 + j])), blk); break;
+            case T_AP_FIXED: {
+                const cplx fx = cdiv_smith(cplx{S.fixed[j][0], S.fixed[j][1]}, sc.col);
+                term = cneg(cmul_exact(cmul_exact(cscale_exact(sc.col, S.co[i]), blk), fx));
+                break;
+            }
+            case T_PA:
+                term = cmul_exact(cscale_exact(cmul_exact(sc.row, sc.jw), __dmul_rn(S.co[6 + j], S.co[i])), blk);
+                break;
+            case T_PP:
+                term = cmul_exact(cscale_exact(cmul_exact(sc.row, sc.col), __dmul_rn(S.co[6 + i], S.co[6 + j])),
+                                  blk);
+                break;
+            default: {
+                const cplx fx = cdiv_smith(cplx{S.fixed[j][0], S.fixed[j][1]}, sc.col);
+                term = cneg(cmul_exact(cmul_exact(cscale_exact(cmul_exact(sc.row, sc.col), S.co[6 + i]), blk), fx));
+                break;
             }
         }
+        out[it] = term;
     }
-    if (k != A.term_off[v + 1] - A.term_off[v]) atomicExch(&A.err[1], 1);
 }
 
 struct PortArgs {
@@ -370,43 +578,60 @@ struct PortArgs {
     const int* current;
     const double* amplitude;
     const double* value;
-    long long first_term;  // index of the first port term within a frequency
-    long long stride;
+    long long first_term;  // index of the first port term
 };
 
 // Port rows, src/assembly.cpp:396-421: a voltage port's unit diagonal and
 // rhs V / c; a current port's rhs r * I. One thread per frequency.
 __global__ void k_port_terms(PortArgs P, Omegas om, int cond, cplx* terms) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= om.n) return;
+    const int nf = om.n;
+    if (f >= nf) return;
     const Scales sc = scales_of(cond, om.w[f]);
-    cplx* out = terms + f * P.stride + P.first_term;
-    int k = 0;
+    cplx* out = terms + P.first_term * nf + f;
+    long long k = 0;
     for (int p = 0; p < P.num_ports; ++p) {
         if (P.current[p]) {
-            out[k++] = cmul_exact(sc.row, cplx{P.amplitude[2 * p], P.amplitude[2 * p + 1]});
+            out[nf * k++] = cmul_exact(sc.row, cplx{P.amplitude[2 * p], P.amplitude[2 * p + 1]});
         } else {
-            out[k++] = cplx{1.0, 0.0};
-            out[k++] = cdiv_smith(cplx{P.value[2 * p], P.value[2 * p + 1]}, sc.col);
+            out[nf * k++] = cplx{1.0, 0.0};
+            out[nf * k++] = cdiv_smith(cplx{P.value[2 * p], P.value[2 * p + 1]}, sc.col);
         }
     }
 }
 
-// K2: one thread per destination; fixed-order sum of its terms.
-__global__ void __launch_bounds__(256) k_slot_sum(int ndest, int nnz, int n, const int* dest_ptr,
-                                                  const int* dest_terms, const cplx* terms,
-                                                  long long stride, cplx* values, cplx* rhs) {
-    const int d = blockIdx.x * blockDim.x + threadIdx.x;
-    const int f = blockIdx.y;
-    if (d >= ndest) return;
-    const cplx* tf = terms + f * stride;
-    cplx s{0.0, 0.0};
-    const int e = dest_ptr[d + 1];
-    for (int k = dest_ptr[d]; k < e; ++k) s = cadd_exact(s, tf[dest_terms[k]]);
-    if (d < nnz)
-        values[static_cast<long long>(f) * nnz + d] = s;
-    else
-        rhs[static_cast<long long>(f) * n + (d - nnz)] = s;
+// K2: fixed-order sum of each destination's terms (increasing term index,
+// the reference's accumulation order), for every frequency of the batch.
+// Thread (slot, frequency) with the frequency fastest, so one term's nf
+// values are read as one contiguous run; the sums are transposed through
+// shared memory so that each frequency's values are written as a contiguous
+// run of slots.
+constexpr int kSlotThreads = 256;
+__global__ void __launch_bounds__(kSlotThreads) k_slot_sum(int ndest, int nnz, int n, int nf, const int* dest_ptr,
+                                                           const int* dest_terms, const cplx* terms,
+                                                           cplx* values, cplx* rhs) {
+    __shared__ cplx sh[kSlotThreads];
+    const int spb = kSlotThreads / nf;  // slots per block
+    const int dl = threadIdx.x / nf, f = threadIdx.x - dl * nf;
+    const int d0 = blockIdx.x * spb;
+    const int d = d0 + dl;
+    if (dl < spb && d < ndest) {
+        cplx s{0.0, 0.0};
+        const int e = dest_ptr[d + 1];
+        for (int k = dest_ptr[d]; k < e; ++k) s = cadd_exact(s, terms[static_cast<long long>(dest_terms[k]) * nf + f]);
+        sh[f * spb + dl] = s;
+    }
+    __syncthreads();
+    const int cnt = min(spb, ndest - d0);
+    for (int e = threadIdx.x; e < nf * spb; e += kSlotThreads) {
+        const int ff = e / spb, x = e - ff * spb;
+        if (x >= cnt) continue;
+        const int dd = d0 + x;
+        if (dd < nnz)
+            values[static_cast<long long>(ff) * nnz + dd] = sh[e];
+        else
+            rhs[static_cast<long long>(ff) * n + (dd - nnz)] = sh[e];
+    }
 }
 
 // Element blocks for a list of tets (parity hook).
@@ -499,7 +724,7 @@ int find_slot(const int* row_ptr, const int* col_idx, int r, int c) {
 
 }  // namespace
 
-std::unique_ptr<Assembly> assembly_create(const aphi_assembly_desc& d) {
+std::unique_ptr<Assembly> assembly_create(const aphi_assembly_desc& d, bool device_setup) {
     if (d.num_tets < 0 || d.num_unknowns < 0 || d.num_bodies < 1 || !d.row_ptr || !d.col_idx ||
         !d.tet_idx || !d.tet_coeff || !d.tets || !d.xyz || !d.body_ptr || !d.body_tets || !d.material)
         throw Error(APHI_ERR_INVALID, "aphi_assembly_create: missing arrays in the description");
@@ -526,88 +751,91 @@ std::unique_ptr<Assembly> assembly_create(const aphi_assembly_desc& d) {
     std::vector<int> visit_tet(d.body_tets, d.body_tets + T), visit_body(T);
     for (int b = 0; b < d.num_bodies; ++b)
         for (int v = d.body_ptr[b]; v < d.body_ptr[b + 1]; ++v) visit_body[v] = b;
-    std::vector<long long> term_off(static_cast<size_t>(T) + 1, 0);
-    std::vector<int> dest;
-    dest.reserve(static_cast<size_t>(T) * 24);
-    const bool up = A->upper_only;
-    auto slot_of = [&](int r, int c) {
-        const int s = find_slot(d.row_ptr, d.col_idx, r, c);
-        if (s < 0)
-            throw Error(APHI_ERR_PATTERN_MISMATCH,
-                        "assemble: no slot for entry (" + std::to_string(r) + ", " + std::to_string(c) +
-                            "). The sparsity pattern and the scatter disagree about the matrix's "
-                            "shape; dropping the term would give a quietly wrong matrix.");
-        return s;
-    };
-    for (int v = 0; v < T; ++v) {
-        const int t = visit_tet[v];
-        if (t < 0 || t >= T) throw Error(APHI_ERR_BAD_SHAPE, "refill: body tet index out of range");
-        const int* idx = d.tet_idx + 16LL * t;
-        const double* fx = d.tet_fixed ? d.tet_fixed + 20LL * t : nullptr;
-        for (int q = 0; q < 16; ++q)
-            if (idx[q] >= N) throw Error(APHI_ERR_BAD_SHAPE, "refill: a DOF index exceeds the unknowns");
-        auto nz = [&](int q) { return fx && (fx[2 * q] != 0.0 || fx[2 * q + 1] != 0.0); };
-        bool need_phi = false;
-        for (int q = 0; q < 10; ++q)
-            if (idx[6 + q] >= 0 || nz(q)) need_phi = true;
-        for (int p = 0; p < 6; ++p) {
-            if (idx[p] < 0) continue;
-            for (int q = 0; q < 6; ++q) {
-                if (idx[q] < 0 || (up && idx[q] < idx[p])) continue;
-                dest.push_back(slot_of(idx[p], idx[q]));
-            }
-        }
-        if (need_phi) {
+    std::vector<long long> term_off;
+    std::vector<int> dest, port_current(d.num_ports), dptr, dterm;
+    for (int p = 0; p < d.num_ports; ++p) port_current[p] = d.port_current[p] ? 1 : 0;
+    const int ndest = nnz + N;
+    if (!device_setup) {
+        term_off.assign(static_cast<size_t>(T) + 1, 0);
+        dest.reserve(static_cast<size_t>(T) * 24);
+        const bool up = A->upper_only;
+        auto slot_of = [&](int r, int c) {
+            const int s = find_slot(d.row_ptr, d.col_idx, r, c);
+            if (s < 0)
+                throw Error(APHI_ERR_PATTERN_MISMATCH,
+                            "assemble: no slot for entry (" + std::to_string(r) + ", " + std::to_string(c) +
+                                "). The sparsity pattern and the scatter disagree about the matrix's "
+                                "shape; dropping the term would give a quietly wrong matrix.");
+            return s;
+        };
+        for (int v = 0; v < T; ++v) {
+            const int t = visit_tet[v];
+            if (t < 0 || t >= T) throw Error(APHI_ERR_BAD_SHAPE, "refill: body tet index out of range");
+            const int* idx = d.tet_idx + 16LL * t;
+            const double* fx = d.tet_fixed ? d.tet_fixed + 20LL * t : nullptr;
+            for (int q = 0; q < 16; ++q)
+                if (idx[q] >= N) throw Error(APHI_ERR_BAD_SHAPE, "refill: a DOF index exceeds the unknowns");
+            auto nz = [&](int q) { return fx && (fx[2 * q] != 0.0 || fx[2 * q + 1] != 0.0); };
+            bool need_phi = false;
+            for (int q = 0; q < 10; ++q)
+                if (idx[6 + q] >= 0 || nz(q)) need_phi = true;
             for (int p = 0; p < 6; ++p) {
                 if (idx[p] < 0) continue;
-                for (int q = 0; q < 10; ++q) {
-                    const int col = idx[6 + q];
-                    if (col >= 0) {
-                        if (!(up && col < idx[p])) dest.push_back(slot_of(idx[p], col));
-                    } else if (nz(q)) {
-                        dest.push_back(nnz + idx[p]);
-                    }
-                    if (col >= 0 && !(up && idx[p] < col)) dest.push_back(slot_of(col, idx[p]));
+                for (int q = 0; q < 6; ++q) {
+                    if (idx[q] < 0 || (up && idx[q] < idx[p])) continue;
+                    dest.push_back(slot_of(idx[p], idx[q]));
                 }
             }
-            for (int p = 0; p < 10; ++p) {
-                const int row = idx[6 + p];
-                if (row < 0) continue;
-                for (int q = 0; q < 10; ++q) {
-                    const int col = idx[6 + q];
-                    if (col >= 0) {
-                        if (!(up && col < row)) dest.push_back(slot_of(row, col));
-                    } else if (nz(q)) {
-                        dest.push_back(nnz + row);
+            if (need_phi) {
+                for (int p = 0; p < 6; ++p) {
+                    if (idx[p] < 0) continue;
+                    for (int q = 0; q < 10; ++q) {
+                        const int col = idx[6 + q];
+                        if (col >= 0) {
+                            if (!(up && col < idx[p])) dest.push_back(slot_of(idx[p], col));
+                        } else if (nz(q)) {
+                            dest.push_back(nnz + idx[p]);
+                        }
+                        if (col >= 0 && !(up && idx[p] < col)) dest.push_back(slot_of(col, idx[p]));
+                    }
+                }
+                for (int p = 0; p < 10; ++p) {
+                    const int row = idx[6 + p];
+                    if (row < 0) continue;
+                    for (int q = 0; q < 10; ++q) {
+                        const int col = idx[6 + q];
+                        if (col >= 0) {
+                            if (!(up && col < row)) dest.push_back(slot_of(row, col));
+                        } else if (nz(q)) {
+                            dest.push_back(nnz + row);
+                        }
                     }
                 }
             }
+            term_off[v + 1] = static_cast<long long>(dest.size());
         }
-        term_off[v + 1] = static_cast<long long>(dest.size());
-    }
-    A->tet_terms = static_cast<long long>(dest.size());
-    std::vector<int> port_current(d.num_ports), h_port(0);
-    for (int p = 0; p < d.num_ports; ++p) {
-        port_current[p] = d.port_current[p] ? 1 : 0;
-        if (port_current[p]) {
-            dest.push_back(nnz + d.port_row[p]);
-        } else {
-            dest.push_back(slot_of(d.port_row[p], d.port_row[p]));
-            dest.push_back(nnz + d.port_row[p]);
+        A->tet_terms = static_cast<long long>(dest.size());
+        for (int p = 0; p < d.num_ports; ++p) {
+            if (port_current[p]) {
+                dest.push_back(nnz + d.port_row[p]);
+            } else {
+                dest.push_back(slot_of(d.port_row[p], d.port_row[p]));
+                dest.push_back(nnz + d.port_row[p]);
+            }
         }
-    }
-    A->num_terms = static_cast<long long>(dest.size());
-    if (A->num_terms >= (1LL << 31))
-        throw Error(APHI_ERR_BAD_SHAPE, "refill: more than 2^31 element terms");
+        A->num_terms = static_cast<long long>(dest.size());
+        if (A->num_terms >= (1LL << 31))
+            throw Error(APHI_ERR_BAD_SHAPE, "refill: more than 2^31 element terms");
 
-    // Slot -> term lists, stable in term order.
-    const int ndest = nnz + N;
-    std::vector<int> dptr(static_cast<size_t>(ndest) + 1, 0), dterm(dest.size());
-    for (int x : dest) ++dptr[x + 1];
-    for (int i = 0; i < ndest; ++i) dptr[i + 1] += dptr[i];
-    {
-        std::vector<int> cur(dptr.begin(), dptr.end() - 1);
-        for (size_t k = 0; k < dest.size(); ++k) dterm[cur[dest[k]]++] = static_cast<int>(k);
+        // Slot -> term lists, stable in term order.
+        dptr.assign(static_cast<size_t>(ndest) + 1, 0);
+        dterm.resize(dest.size());
+        for (int x : dest) ++dptr[x + 1];
+        for (int i = 0; i < ndest; ++i) dptr[i + 1] += dptr[i];
+        {
+            std::vector<int> cur(dptr.begin(), dptr.end() - 1);
+            for (size_t k = 0; k < dest.size(); ++k) dterm[cur[dest[k]]++] = static_cast<int>(k);
+        }
     }
 
     A->d_xyz = upload(d.xyz, 3LL * d.num_nodes);
@@ -620,15 +848,19 @@ std::unique_ptr<Assembly> assembly_create(const aphi_assembly_desc& d) {
     std::vector<double> zeros;
     if (!d.tet_fixed) zeros.assign(20LL * T, 0.0);
     A->d_tet_fixed = upload(d.tet_fixed ? d.tet_fixed : zeros.data(), 20LL * T);
-    A->d_term_off = upload(term_off.data(), term_off.size());
-    A->d_dest_ptr = upload(dptr.data(), dptr.size());
-    A->d_dest_terms = upload(dterm.data(), dterm.size());
+    if (device_setup) {
+        assembly_maps_on_device(*A, d, visit_tet.data());
+    } else {
+        A->d_term_off = upload(term_off.data(), term_off.size());
+        A->d_dest_ptr = upload(dptr.data(), dptr.size());
+        A->d_dest_terms = upload(dterm.data(), dterm.size());
+    }
     A->d_port_current = upload(port_current.data(), port_current.size());
     A->d_port_amp = upload(d.port_amplitude, 2LL * d.num_ports);
     A->d_port_value = upload(d.port_value, 2LL * d.num_ports);
     A->d_err = upload(std::vector<int>(4, 0).data(), 4);
     A->bytes = (3LL * d.num_nodes + 16LL * T + 20LL * T) * 8 + (4LL * T + 2LL * T + 16LL * T) * 4 +
-               (T + 1LL) * 8 + (ndest + 1LL + dest.size()) * 4;
+               (T + 1LL) * 8 + (ndest + 1LL + A->num_terms) * 4;
     return A;
 }
 
@@ -653,8 +885,8 @@ void assembly_refill(Assembly& A, int nfreq, const double* omegas, int cond, dou
         A.terms_capacity = chunk;
     }
     TetArgs ta{A.T, A.upper_only ? 1 : 0, A.d_xyz, A.d_tets, A.d_visit_tet, A.d_visit_body,
-               A.d_material, A.d_tet_idx, A.d_tet_coeff, A.d_tet_fixed, A.d_term_off, A.num_terms, A.d_err};
-    PortArgs pa{A.num_ports, A.d_port_current, A.d_port_amp, A.d_port_value, A.tet_terms, A.num_terms};
+               A.d_material, A.d_tet_idx, A.d_tet_coeff, A.d_tet_fixed, A.d_term_off, A.d_err};
+    PortArgs pa{A.num_ports, A.d_port_current, A.d_port_amp, A.d_port_value, A.tet_terms};
     const Quad q = quad_points();
     for (int f0 = 0; f0 < nfreq; f0 += chunk) {
         Omegas om{};
@@ -662,8 +894,7 @@ void assembly_refill(Assembly& A, int nfreq, const double* omegas, int cond, dou
         for (int i = 0; i < om.n; ++i) om.w[i] = omegas[f0 + i];
         cplx* terms = reinterpret_cast<cplx*>(A.d_terms);
         if (A.T > 0) {
-            dim3 grid(ceil_div(A.T, 128), om.n);
-            k_tet_terms<<<grid, 128, 0, stream>>>(ta, om, cond, q, terms);
+            k_tet_terms<<<ceil_div(A.T, kTetWarps), 32 * kTetWarps, 0, stream>>>(ta, om, cond, q, terms);
             APHI_CHECK_LAUNCH();
         }
         if (A.num_ports > 0) {
@@ -671,11 +902,11 @@ void assembly_refill(Assembly& A, int nfreq, const double* omegas, int cond, dou
             APHI_CHECK_LAUNCH();
         }
         const int ndest = A.nnz + A.N;
-        dim3 g2(ceil_div(ndest, 256), om.n);
-        k_slot_sum<<<g2, 256, 0, stream>>>(ndest, A.nnz, A.N, A.d_dest_ptr, A.d_dest_terms, terms,
-                                           A.num_terms,
-                                           reinterpret_cast<cplx*>(values_dev) + static_cast<long long>(f0) * A.nnz,
-                                           reinterpret_cast<cplx*>(rhs_dev) + static_cast<long long>(f0) * A.N);
+        const int spb = kSlotThreads / om.n;
+        k_slot_sum<<<ceil_div(ndest, spb), kSlotThreads, 0, stream>>>(
+            ndest, A.nnz, A.N, om.n, A.d_dest_ptr, A.d_dest_terms, terms,
+            reinterpret_cast<cplx*>(values_dev) + static_cast<long long>(f0) * A.nnz,
+            reinterpret_cast<cplx*>(rhs_dev) + static_cast<long long>(f0) * A.N);
         APHI_CHECK_LAUNCH();
     }
 }

@@ -63,7 +63,9 @@ std::unique_ptr<Fields> fields_create(const Assembly& A, int num_nodes, int num_
 void fields_compute(Fields& F, double omega, int conditioning, const double* x_dev, const FieldsOut& out,
                     cudaStream_t stream);
 
-std::unique_ptr<Assembly> assembly_create(const aphi_assembly_desc& d);
+// device_setup: build the term offsets and slot -> term lists on the device
+// (setup.cu) instead of on the host; the arrays are identical.
+std::unique_ptr<Assembly> assembly_create(const aphi_assembly_desc& d, bool device_setup = false);
 void assembly_refill(Assembly& A, int nfreq, const double* omegas, int cond, double* values_dev,
                      double* rhs_dev, cudaStream_t stream);
 void assembly_check_errors(Assembly& A, cudaStream_t stream);

@@ -4,6 +4,7 @@
 #include <string>
 
 #include "assembly.hpp"
+#include "setup.hpp"
 #include "capi_util.hpp"
 #include "common.cuh"
 #include "ordering.hpp"
@@ -173,6 +174,50 @@ int aphi_assembly_create(const aphi_assembly_desc* desc, aphi_assembly** out) {
             throw;
         }
         *out = h;
+    });
+}
+
+int aphi_assembly_create_device_setup(const aphi_assembly_desc* desc, aphi_assembly** out) {
+    return guard([&] {
+        if (!desc || !out) throw Error(APHI_ERR_INVALID, "aphi_assembly_create_device_setup: null argument");
+        auto* h = new aphi_assembly;
+        try {
+            h->a = assembly_create(*desc, true);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int aphi_assembly_maps(const aphi_assembly* h, int64_t* term_off, int* dest_ptr, int* dest_terms) {
+    return guard([&] {
+        if (!h) throw Error(APHI_ERR_INVALID, "aphi_assembly_maps: null assembly");
+        const Assembly& A = *h->a;
+        if (term_off)
+            APHI_CUDA(cudaMemcpy(term_off, A.d_term_off, sizeof(long long) * (static_cast<size_t>(A.T) + 1),
+                                 cudaMemcpyDeviceToHost));
+        if (dest_ptr)
+            APHI_CUDA(cudaMemcpy(dest_ptr, A.d_dest_ptr, sizeof(int) * (static_cast<size_t>(A.nnz) + A.N + 1),
+                                 cudaMemcpyDeviceToHost));
+        if (dest_terms)
+            APHI_CUDA(cudaMemcpy(dest_terms, A.d_dest_terms, sizeof(int) * static_cast<size_t>(A.num_terms),
+                                 cudaMemcpyDeviceToHost));
+    });
+}
+
+int aphi_pattern_build(int n, int num_tets, const int* tet_idx, int num_diag, const int* diag_rows, int upper_only,
+                       int* row_ptr, int* col_idx, int64_t capacity, int64_t* nnz) {
+    return guard([&] {
+        if (!tet_idx || !row_ptr || !nnz || (num_diag > 0 && !diag_rows))
+            throw Error(APHI_ERR_INVALID, "aphi_pattern_build: null argument");
+        const long long got = pattern_build(n, num_tets, tet_idx, num_diag, diag_rows, upper_only != 0, row_ptr,
+                                            col_idx, capacity);
+        *nnz = got;
+        if (got > capacity || !col_idx)
+            throw Error(APHI_ERR_BAD_SHAPE, "aphi_pattern_build: the pattern has " + std::to_string(got) +
+                                                " entries, more than the capacity given");
     });
 }
 

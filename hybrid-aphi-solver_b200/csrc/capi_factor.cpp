@@ -201,6 +201,24 @@ int aphi_residuals_host(const aphi_analysis* an_c, int batch, int nrhs, const do
     });
 }
 
+int aphi_csc_solve_host(int n, const int* col_ptr, const int* row_index, const double* value,
+                        const double* diagonal, int nrhs, double* y) {
+    return guard([&] {
+        if (!col_ptr || (n > 0 && (!diagonal || !y)) || (n > 0 && col_ptr[n] > 0 && (!row_index || !value)))
+            throw Error(APHI_ERR_INVALID, "aphi_csc_solve_host: null argument");
+        csc_solve_host(n, col_ptr, row_index, value, diagonal, nrhs, y);
+    });
+}
+
+int aphi_csr_residuals_host(int n, const int* row_ptr, const int* col_idx, const double* values, int nrhs,
+                            const double* x, const double* b, double* out) {
+    return guard([&] {
+        if (!row_ptr || !col_idx || !values || !x || !b || !out)
+            throw Error(APHI_ERR_INVALID, "aphi_csr_residuals_host: null argument");
+        csr_residuals_host(n, row_ptr, col_idx, values, nrhs, x, b, out);
+    });
+}
+
 int aphi_solve_symmetric_host(const aphi_analysis* an_c, const double* values, const double* b, int equil_iters,
                               double pivot_floor, double* x, double* report) {
     int rc = APHI_OK;

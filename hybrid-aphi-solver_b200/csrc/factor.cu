@@ -677,6 +677,82 @@ void residuals(const aphi_analysis* an, int batch, int nrhs, const double* value
     }
 }
 
+// relative_residual and backward_error of a matrix held only as host CSR
+// arrays (upper-stored), with x and b on the host: the mirrored pattern is
+// built on the host (structure only), every product and sum runs on the
+// device with the kernels above. out: nrhs x 2 (relative residual, backward
+// error).
+void csr_residuals_host(int n, const int* row_ptr, const int* col_idx, const double* values, int nrhs,
+                        const double* x, const double* b, double* out) {
+    if (n < 1 || nrhs < 1 || nrhs > kMaxGridY)
+        throw Error(APHI_ERR_BAD_SHAPE, "relative_residual: n must be >= 1 and nrhs in 1..65535");
+    const long long nnz = row_ptr[n];
+    std::vector<int> fptr(static_cast<size_t>(n) + 1, 0), fcol;
+    std::vector<long long> fmap;
+    for (int r = 0; r < n; ++r)
+        for (long long k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
+            const int c = col_idx[k];
+            if (c < r || c >= n) throw Error(APHI_ERR_BAD_SHAPE, "relative_residual: the pattern is not upper");
+            ++fptr[r + 1];
+            if (c != r) ++fptr[c + 1];
+        }
+    for (int r = 0; r < n; ++r) fptr[r + 1] += fptr[r];
+    fcol.resize(fptr[n]);
+    fmap.resize(fptr[n]);
+    {
+        std::vector<int> cur(fptr.begin(), fptr.end() - 1);
+        for (int r = 0; r < n; ++r)
+            for (long long k = row_ptr[r]; k < row_ptr[r + 1]; ++k) {
+                const int c = col_idx[k];
+                fcol[cur[r]] = c;
+                fmap[cur[r]++] = k;
+                if (c != r) {
+                    fcol[cur[c]] = r;
+                    fmap[cur[c]++] = k;
+                }
+            }
+    }
+    const int nb = ceil_div(n, 256);
+    std::vector<void*> owned;
+    auto up = [&](const void* h, size_t bytes) {
+        void* d = nullptr;
+        APHI_CUDA(cudaMalloc(&d, std::max<size_t>(bytes, 16)));
+        owned.push_back(d);
+        if (h && bytes) APHI_CUDA(cudaMemcpy(d, h, bytes, cudaMemcpyHostToDevice));
+        return d;
+    };
+    try {
+        const int* d_fptr = static_cast<const int*>(up(fptr.data(), fptr.size() * sizeof(int)));
+        const int* d_fcol = static_cast<const int*>(up(fcol.data(), fcol.size() * sizeof(int)));
+        const long long* d_fmap = static_cast<const long long*>(up(fmap.data(), fmap.size() * sizeof(long long)));
+        const double* d_v = static_cast<const double*>(up(values, 16 * static_cast<size_t>(nnz)));
+        const double* d_x = static_cast<const double*>(up(x, 16 * static_cast<size_t>(n) * nrhs));
+        const double* d_b = static_cast<const double*>(up(b, 16 * static_cast<size_t>(n) * nrhs));
+        double* partial = static_cast<double*>(up(nullptr, sizeof(double) * 3 * static_cast<size_t>(nb) * nrhs));
+        auto* amax = static_cast<unsigned long long*>(up(nullptr, sizeof(unsigned long long)));
+        double* norms = static_cast<double*>(up(nullptr, sizeof(double) * 4 * static_cast<size_t>(nrhs)));
+        APHI_CUDA(cudaMemset(amax, 0, sizeof(unsigned long long)));
+        k_residual<<<dim3(nb, nrhs), 256>>>(n, nrhs, d_fptr, d_fcol, d_fmap, d_v, nnz, d_x, d_b, nullptr, partial);
+        APHI_CHECK_LAUNCH();
+        k_amax<<<dim3(ceil_div(std::max<long long>(nnz, 1), 256), 1), 256>>>(d_v, nnz, amax);
+        APHI_CHECK_LAUNCH();
+        k_norms_final<<<nrhs, 256>>>(nb, nrhs, partial, amax, norms);
+        APHI_CHECK_LAUNCH();
+        std::vector<double> h(4 * static_cast<size_t>(nrhs));
+        APHI_CUDA(cudaMemcpy(h.data(), norms, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int q = 0; q < nrhs; ++q) {
+            const double rn = h[4 * q], bn = h[4 * q + 1], xn = h[4 * q + 2], am = h[4 * q + 3];
+            out[2 * q] = bn > 0.0 ? rn / bn : rn;
+            const double den = am * xn + bn;
+            out[2 * q + 1] = den > 0.0 ? rn / den : rn;
+        }
+    } catch (...) {
+        for (void* d : owned) cudaFree(d);
+        throw;
+    }
+    for (void* d : owned) cudaFree(d);
+}
+
 // ---------------------------------------------------------------- allocation-free residuals
 // The same residual and backward-error computation as residuals() above, for
 // callers that cannot allocate device memory while they run: a serving loop

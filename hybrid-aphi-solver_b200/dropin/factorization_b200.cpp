@@ -18,8 +18,10 @@
 // device factor it was exported from, registered under the address of the
 // SymmetricFactor it filled together with a fingerprint of its contents. A
 // later solve_in_place / solve of that same, unchanged factor runs on the
-// device; a factor from anywhere else (or modified since) is solved on the
-// host from its CSC arrays.
+// device factor; a factor from anywhere else (or modified since) is solved on
+// the device from its CSC arrays (aphi_csc_solve_host). relative_residual and
+// backward_error run on the device too (aphi_csr_residuals_host). No numeric
+// work of these functions runs on the host.
 #include <algorithm>
 #include <chrono>
 #include <complex>
@@ -146,23 +148,6 @@ std::shared_ptr<DeviceFactor> find_factor(const SymmetricFactor& f) {
 
 void forget_factor(const SymmetricFactor* f) {
     g_factors.remove_if([&](const std::shared_ptr<DeviceFactor>& d) { return d->host == f; });
-}
-
-// Host solve of L D L^T y = y from the CSC arrays (factorized ordering):
-// forward by columns, scale by D, backward by columns of L^T. No conjugation.
-void host_solve_in_place(const SymmetricFactor& f, std::vector<Complex>& y) {
-    const int n = f.rows;
-    for (int j = 0; j < n; ++j) {
-        const Complex yj = y[j];
-        if (yj == Complex(0.0, 0.0)) continue;
-        for (int t = f.col_ptr[j]; t < f.col_ptr[j + 1]; ++t) y[f.row_index[t]] -= f.value[t] * yj;
-    }
-    for (int j = 0; j < n; ++j) y[j] /= f.diagonal[j];
-    for (int j = n - 1; j >= 0; --j) {
-        Complex s = y[j];
-        for (int t = f.col_ptr[j]; t < f.col_ptr[j + 1]; ++t) s -= f.value[t] * y[f.row_index[t]];
-        y[j] = s;
-    }
 }
 
 }  // namespace
@@ -293,7 +278,11 @@ void solve_in_place(const SymmetricFactor& f, std::vector<Complex>& y) {
     std::lock_guard<std::mutex> lock(g_mutex);
     auto d = find_factor(f);
     if (!d) {
-        host_solve_in_place(f, y);
+        // A factor this layer did not produce (built by hand, or modified
+        // since): solved on the device from its CSC arrays.
+        check_status(aphi_csc_solve_host(n, f.col_ptr.data(), f.row_index.data(), as_doubles(f.value),
+                                         reinterpret_cast<const double*>(f.diagonal.data()), 1, as_doubles(y)),
+                     "solve_in_place");
         return;
     }
     // The device factor solves in the original numbering: y is in the
@@ -329,31 +318,34 @@ std::vector<Complex> solve(const SymmetricFactor& f, const Permutation& p, const
     return x;
 }
 
-double relative_residual(const SparseSymmetricZ& a, const std::vector<Complex>& x, const std::vector<Complex>& b) {
+namespace {
+
+// relative_residual and backward_error together, on the device.
+void device_residuals(const char* where, const SparseSymmetricZ& a, const std::vector<Complex>& x,
+                      const std::vector<Complex>& b, double out[2]) {
     if (static_cast<int>(x.size()) != a.rows() || x.size() != b.size())
-        throw std::invalid_argument("relative_residual: lengths must match the matrix");
-    const std::vector<Complex> ax = a.matvec(x);
-    double rr = 0.0, bb = 0.0;
-    for (size_t i = 0; i < x.size(); ++i) {
-        rr += std::norm(ax[i] - b[i]);
-        bb += std::norm(b[i]);
+        throw std::invalid_argument(std::string(where) + ": lengths must match the matrix");
+    if (a.rows() == 0) {
+        out[0] = out[1] = 0.0;
+        return;
     }
-    return bb > 0.0 ? std::sqrt(rr) / std::sqrt(bb) : std::sqrt(rr);
+    check_status(aphi_csr_residuals_host(a.rows(), a.row_ptr().data(), a.col_index().data(), as_doubles(a.values()),
+                                         1, as_doubles(x), as_doubles(b), out),
+                 where);
+}
+
+}  // namespace
+
+double relative_residual(const SparseSymmetricZ& a, const std::vector<Complex>& x, const std::vector<Complex>& b) {
+    double out[2];
+    device_residuals("relative_residual", a, x, b, out);
+    return out[0];
 }
 
 double backward_error(const SparseSymmetricZ& a, const std::vector<Complex>& x, const std::vector<Complex>& b) {
-    if (static_cast<int>(x.size()) != a.rows() || x.size() != b.size())
-        throw std::invalid_argument("backward_error: lengths must match the matrix");
-    const std::vector<Complex> ax = a.matvec(x);
-    double rr = 0.0, bb = 0.0, xx = 0.0, amax = 0.0;
-    for (size_t i = 0; i < x.size(); ++i) {
-        rr += std::norm(ax[i] - b[i]);
-        bb += std::norm(b[i]);
-        xx += std::norm(x[i]);
-    }
-    for (const Complex& v : a.values()) amax = std::max(amax, std::abs(v));
-    const double den = amax * std::sqrt(xx) + std::sqrt(bb);
-    return den > 0.0 ? std::sqrt(rr) / den : std::sqrt(rr);
+    double out[2];
+    device_residuals("backward_error", a, x, b, out);
+    return out[1];
 }
 
 bool solve_symmetric(const SparseSymmetricZ& a, const std::vector<Complex>& b, std::vector<Complex>& x,

@@ -136,6 +136,25 @@ typedef struct {
 
 typedef struct aphi_assembly aphi_assembly;
 int aphi_assembly_create(const aphi_assembly_desc* desc, aphi_assembly** out);
+/* The same assembly with its per-mesh maps built on the device instead of
+ * the host: each tet's term destinations in the scatter's emission order and
+ * their inversion into slot -> term lists (ScatterMap::build and its use by
+ * scatter_into, src/assembly.cpp:196-232, :255-422). The maps equal
+ * aphi_assembly_create's exactly (each list sorted by term index after an
+ * atomic fill), so refill gives the same bits. A missing slot is refused with
+ * PATTERN_MISMATCH naming the entry. */
+int aphi_assembly_create_device_setup(const aphi_assembly_desc* desc, aphi_assembly** out);
+/* Copies of the assembly's maps (any pointer may be NULL): term_off[T+1]
+ * (terms per visited tet, prefix), dest_ptr[nnz+N+1], dest_terms[num_terms]. */
+int aphi_assembly_maps(const aphi_assembly* a, int64_t* term_off, int* dest_ptr, int* dest_terms);
+/* build_sparsity (src/sparsity.cpp:19-136) on the device: the upper (or full)
+ * CSR pattern of every pair of each tet's unique live DOFs (tet_idx: 16 per
+ * tet, -1 for none) plus a diagonal entry for each of diag_rows (voltage-port
+ * constraint rows); rows sorted and unique. row_ptr[n+1]; col_idx holds
+ * capacity entries; *nnz is always set, and BAD_SHAPE is returned when it
+ * exceeds capacity (call again with a larger buffer). */
+int aphi_pattern_build(int n, int num_tets, const int* tet_idx, int num_diag, const int* diag_rows, int upper_only,
+                       int* row_ptr, int* col_idx, int64_t capacity, int64_t* nnz);
 int aphi_assembly_destroy(aphi_assembly* a);
 /* info[0..3]: nnz, unknowns, num_terms, device bytes held */
 int aphi_assembly_info(const aphi_assembly* a, int64_t* info);
@@ -344,6 +363,21 @@ int aphi_factorize_host(aphi_factor* f, const double* values, int equil_iters, d
 int aphi_solve_host(aphi_factor* f, int nrhs, const double* b, double* x);
 int aphi_residuals_host(const aphi_analysis* an, int batch, int nrhs, const double* values, const double* x,
                         const double* b, double* out);
+
+/* solve_in_place (src/factorization.cpp:254-294) for a factor held only as
+ * host arrays in the reference's SymmetricFactor layout (strictly lower CSC,
+ * rows ascending; complex D): forward by L, scale by D^-1, backward by L^T,
+ * no conjugation, on the device. Each unknown is updated in the reference's
+ * order (column by column forward, row by row backward), levels of the
+ * pattern running in parallel. y: n x nrhs complex (rhs-major), in place.
+ * BAD_SHAPE for a malformed pattern, ZERO_PIVOT for a zero D. */
+int aphi_csc_solve_host(int n, const int* col_ptr, const int* row_index, const double* value,
+                        const double* diagonal, int nrhs, double* y);
+/* relative_residual and backward_error (src/factorization.cpp:315-329,
+ * :401-416) of a matrix held only as host upper CSR arrays, computed on the
+ * device; x, b: n x nrhs complex (rhs-major). out: nrhs x 2. */
+int aphi_csr_residuals_host(int n, const int* row_ptr, const int* col_idx, const double* values, int nrhs,
+                            const double* x, const double* b, double* out);
 
 /* The whole solve_symmetric pipeline (src/factorization.cpp:332-398) on
  * host buffers, FP64: equilibrate, factorize, solve, unscale, measure.

@@ -131,7 +131,7 @@ def test_random_patterns_match_reference(small_front, cuda, ref_or_skip):
 OMEGAS = [2 * np.pi * 50.0, 2 * np.pi * 1e4, 2 * np.pi * 1e6]
 
 
-@pytest.mark.parametrize("cells,small_front", [(6, 96), (6, 8), (8, 96), (12, 96), (12, 16)])
+@pytest.mark.parametrize("cells,small_front", [(6, 96), (6, 8), (8, 96), (12, 96), (12, 16), (16, 96)])
 def test_cylinder_solve_symmetric_matches_reference(cells, small_front, cuda, ref_or_skip):
     """solve_symmetric on the cylinder-in-box (10 Ruiz iterations, the
     reference's AMD analysis) against the reference's solve_symmetric.

@@ -1,0 +1,104 @@
+"""The benchmarked configuration against the reference's own solutions.
+
+The 24^3 and 32^3 cylinder-in-box (the 32^3 mesh is the benchmarked sweep),
+at three members of the benchmarked 16-frequency sweep (50 Hz, 9.84 kHz,
+1 MHz), against solutions that the reference's own pipeline produced on the
+CPU (refill, src/assembly.cpp:468-494, then solve_symmetric,
+src/factorization.cpp:332-398, with 10 Ruiz iterations), committed as
+fixtures by tests/golden/make_reference_solutions.py. A 32^3 reference solve
+takes about 35 minutes of one core, so these are fixtures, not live calls.
+
+Checked, per frequency:
+* the AMD permutation and the CSR pattern hash equal to the reference's
+  (bit-exact), and the device refill's values and rhs hash equal to the
+  reference's refill (bitwise);
+* the plain FP64 path (the drop-in's solve_symmetric) and the mixed
+  FP32+refinement sweep (the benchmarked path): relative residual <= 1e-12,
+  and the solution against the reference's under the same criterion as the
+  smaller meshes' live comparison -- within 1e-10 of the reference's wherever
+  the reference's own answer is within 1e-11 of x* (the extended-precision
+  refined solution), and otherwise at least as accurate as the reference's
+  and within 1e-10 + 3 * its error of it.
+"""
+import numpy as np
+import pytest
+import torch
+
+import aphi_b200 as ab
+import reference_solutions as refsol
+from solvecheck import refined_solution, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _check_solution(x, x_ref, xs, what):
+    err_ref = rel(x_ref, xs)
+    err_mine = rel(x, xs)
+    assert err_mine <= max(1e-10, 2.0 * err_ref), (what, err_mine, err_ref)
+    assert rel(x, x_ref) <= 1e-10 + 3.0 * err_ref, (what, rel(x, x_ref), err_ref)
+    if err_ref <= 1e-11:
+        assert rel(x, x_ref) <= 1e-10, (what, rel(x, x_ref), err_ref)
+    return err_ref, err_mine
+
+
+@pytest.fixture(scope="module", params=[24, 32])
+def mesh(request, cuda):
+    cells = request.param
+    fx = refsol.load(cells)
+    assert fx is not None, f"fixture {refsol.path(cells).name} is missing"
+    w = ab.Workload.cylinder(cells)
+    perm = ab.amd_ordering(w.row_ptr, w.col_idx)
+    assert refsol.sha(perm) == fx["sha_perm"], "AMD permutation differs from the reference's"
+    assert refsol.sha(np.concatenate([w.row_ptr, w.col_idx]).astype(np.int32)) == fx["sha_pattern"]
+    an = ab.Analysis(w.row_ptr, w.col_idx, perm)
+    assert an.n == fx["n"] and an.nnz == fx["nnz"] and an.info["nnz_l"] == fx["nnz_l"]
+    asm = ab.Assembly(ab.workload_arrays(w))
+    vals, rhs = asm.refill(fx["omegas"])
+    v_h, b_h = vals.cpu().numpy(), rhs.cpu().numpy()
+    for k in range(len(fx["omegas"])):
+        assert refsol.sha(v_h[k]) == fx["sha_values"][k], "device refill values differ from the reference's"
+        assert refsol.sha(b_h[k]) == fx["sha_rhs"][k], "device refill rhs differs from the reference's"
+    # x*: the reference's solution refined with extended-precision residuals
+    # and FP64-factor corrections.
+    f = ab.Factor(an)
+    xstar = []
+    for k in range(len(fx["omegas"])):
+        assert f.factorize(vals[k:k + 1])
+        xstar.append(refined_solution(f, w.row_ptr, w.col_idx, v_h[k], b_h[k], fx["x"][k]))
+    f.close()
+    yield dict(cells=cells, fx=fx, w=w, an=an, asm=asm, vals=vals, rhs=rhs, v_h=v_h, b_h=b_h, xstar=xstar)
+    asm.close()
+    an.close()
+
+
+def test_fp64_solve_symmetric_matches_reference(mesh):
+    fx, an = mesh["fx"], mesh["an"]
+    for k in range(len(fx["omegas"])):
+        ok, x, rep = ab.solve_symmetric(an, mesh["v_h"][k], mesh["b_h"][k])
+        r = fx["reports"][k]
+        assert ok and r["ok"]
+        assert rep["residual"] <= 1e-12, rep["residual"]
+        assert rep["factor_nnz"] == r["factor_nnz"]
+        assert abs(rep["equilibration_min"] / r["equilibration_min"] - 1) < 1e-12
+        assert abs(rep["equilibration_max"] / r["equilibration_max"] - 1) < 1e-12
+        assert abs(rep["smallest_pivot"] / r["smallest_pivot"] - 1) < 1e-9
+        assert abs(rep["largest_pivot"] / r["largest_pivot"] - 1) < 1e-9
+        err_ref, err_mine = _check_solution(x, fx["x"][k], mesh["xstar"][k], ("fp64", mesh["cells"], k))
+        print(f"{mesh['cells']}^3 f={fx['omegas'][k] / 2 / np.pi:.4g} Hz: |x-x_ref|/|x_ref|="
+              f"{rel(x, fx['x'][k]):.2e}, ref err vs x* {err_ref:.2e}, ours {err_mine:.2e}")
+
+
+def test_mixed_sweep_matches_reference(mesh):
+    """The benchmarked path: FP32 tensor-core factors refined in FP64 (COCG),
+    stalled entries refactorized in FP64."""
+    fx = mesh["fx"]
+    nf = len(fx["omegas"])
+    sw = ab.SweepSolver(mesh["an"], mesh["asm"], nf, "mixed", fp64_batch=nf)
+    x, vals, rhs, reps = sw.solve(fx["omegas"])
+    res = ab.residuals(mesh["an"], vals, x, rhs)
+    xh = x.cpu().numpy()
+    for k in range(nf):
+        assert res[k, 0, 0] <= 1e-12, (k, res[k, 0, 0])
+        _check_solution(xh[k], fx["x"][k], mesh["xstar"][k], ("mixed", mesh["cells"], k, reps[k]["precision"]))
+    sw.close()
+    torch.cuda.empty_cache()
