@@ -91,7 +91,8 @@ class AssemblyDesc(C.Structure):
 
 
 class AnalysisOptions(C.Structure):
-    _fields_ = [("relax_small", I), ("relax_fill", D), ("relax_max_width", I), ("small_front", I)]
+    _fields_ = [("relax_small", I), ("relax_fill", D), ("relax_max_width", I), ("small_front", I),
+                ("group4_rows", I), ("group2_rows", I)]
 
 
 class FactorStats(C.Structure):
@@ -167,6 +168,8 @@ _SIGS = {
     "aphi_pattern_build": (I, [I, I, PI, I, PI, I, PI, PI, C.c_int64, PI64]),
     "aphi_csc_solve_host": (I, [I, PI, PI, PD, PD, I, PD]),
     "aphi_csr_residuals_host": (I, [I, PI, PI, PD, I, PD, PD, PD]),
+    "aphi_factor_set_tc_split": (I, [P, I]),
+    "aphi_selftest_tc_tile_split": (I, [I, I, I, I, I, P, P, P]),
 }
 
 
@@ -744,6 +747,11 @@ class Factor:
         check(lib().aphi_fronts_read(self._h, k, dptr(panels), dptr(cb), stream_ptr(stream)))
         return panels, cb
 
+    def set_tc_split(self, split: int) -> None:
+        """FP32 factors: TF32 pieces per operand in the tensor-core update (3 or 2)."""
+        check(lib().aphi_factor_set_tc_split(self._h, split))
+        self.tc_split = split
+
     def set_batch(self, batch: int) -> None:
         """Process `batch` (1..capacity) entries from now on, without reallocating."""
         check(lib().aphi_factor_set_batch(self._h, batch))
@@ -816,17 +824,18 @@ def bounded_wait_selftest(spin_limit: int = 1 << 12) -> int:
     return int(lib().aphi_selftest_bounded_wait(spin_limit))
 
 
-def tc_tile_selftest(P: np.ndarray, i0: int, j0: int, d: np.ndarray | None = None) -> np.ndarray:
+def tc_tile_selftest(P: np.ndarray, i0: int, j0: int, d: np.ndarray | None = None, split: int = 3) -> np.ndarray:
     """One tensor-core update tile: the 128 x 64 complex64 block
     sum_k (P[i0 + r, k] d[k]) P[j0 + c, k] (rows of P past its end read as
-    zero), computed by the kernel the FP32 factorization uses."""
+    zero), computed by the kernel the FP32 factorization uses, with its
+    operands split into `split` TF32 pieces."""
     Pc = np.asfortranarray(P, np.complex64)
     rows, K = Pc.shape
     dd = None if d is None else np.ascontiguousarray(d, np.complex64)
     out = np.zeros((64, 128), np.complex64)
-    check(lib().aphi_selftest_tc_tile(rows, K, i0, j0, C.c_void_p(Pc.ctypes.data),
-                                      None if dd is None else C.c_void_p(dd.ctypes.data),
-                                      C.c_void_p(out.ctypes.data)))
+    check(lib().aphi_selftest_tc_tile_split(split, rows, K, i0, j0, C.c_void_p(Pc.ctypes.data),
+                                            None if dd is None else C.c_void_p(dd.ctypes.data),
+                                            C.c_void_p(out.ctypes.data)))
     return out.T
 
 
@@ -887,7 +896,8 @@ class SweepSolver:
 
     def __init__(self, analysis: Analysis, assembly: Assembly, batch: int, precision: str = "mixed",
                  fp64_batch: int = 8, rtol: float = 1e-14, tol: float = 1e-16, max_iters: int = 40,
-                 fp32_batch: int | None = None, predict: bool = True, fp64_refine: bool = False):
+                 fp32_batch: int | None = None, predict: bool = True, fp64_refine: bool = False,
+                 tc_split: int = 3):
         if precision not in ("mixed", "fp64"):
             raise InvalidArgument(ERR_BAD_SHAPE, f"SweepSolver: precision {precision!r} is not 'mixed' or 'fp64'")
         self.analysis, self.assembly = analysis, assembly
@@ -897,6 +907,7 @@ class SweepSolver:
         self.fp32_batch = max(1, min(fp32_batch or batch, batch))
         self.predict = predict
         self.fp64_refine = fp64_refine
+        self.tc_split = tc_split
         self.stall_omega = None      # lowest frequency whose FP32 refinement stalled
         self._factors = {}
         self._profile = False
@@ -913,6 +924,8 @@ class SweepSolver:
                 f.close()
                 self._factors.pop(precision)
             f = Factor(self.analysis, precision, size)
+            if precision == PREC_FP32 and self.tc_split != 3:
+                f.set_tc_split(self.tc_split)
             if self._profile:
                 f.profile(True)
             self._factors[precision] = f

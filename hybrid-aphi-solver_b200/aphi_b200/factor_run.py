@@ -29,6 +29,8 @@ def main() -> None:
     ap.add_argument("--f-lo", type=float, default=50.0)
     ap.add_argument("--f-hi", type=float, default=1.0e3)
     ap.add_argument("--simt", action="store_true", help="FP32 on the SIMT kernels instead of tcgen05")
+    ap.add_argument("--tc-split", type=int, default=3, choices=[2, 3],
+                    help="TF32 pieces per operand in the tensor-core update")
     a = ap.parse_args()
     import torch
     if a.simt:
@@ -38,6 +40,8 @@ def main() -> None:
     asm = ab.Assembly(ab.workload_arrays(w))
     vals, _ = asm.refill(2 * np.pi * np.geomspace(a.f_lo, a.f_hi, a.batch))
     f = ab.Factor(an, precision=a.precision, batch=a.batch)
+    if a.precision == 32:
+        f.set_tc_split(a.tc_split)
     ok = True
     ms = 0.0
     kinds = {}
@@ -52,6 +56,7 @@ def main() -> None:
         kinds = f.profile_read()
     plan = an.plan_stats(1 if a.precision == 32 and not a.simt else 0, flops=True)
     out = {"cells": a.cells, "batch": a.batch, "precision": a.precision, "tensor_cores": a.precision == 32 and not a.simt,
+           "tc_split": a.tc_split if a.precision == 32 else None,
            "ok": ok, "factorize_ms": ms, "flops_per_factorization": an.info["flops"],
            "kinds": {k: {"launches": n, "ms": t, "useful_flops": plan.get(k, (0, 0, 0.0))[2] * a.batch,
                          "tflops": (plan.get(k, (0, 0, 0.0))[2] * a.batch / (t / 1000.0) / 1e12) if t else None}

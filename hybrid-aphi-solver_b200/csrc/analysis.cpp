@@ -39,11 +39,15 @@ void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing,
     // last, the rest of the front with all of the group's panels, so every
     // trailing entry is read and written once per group instead of once per
     // 128 columns. Groups are 4 panels (K up to 512) in fronts of at least
-    // kGroup4Rows rows, where the trailing matrix dwarfs the group's columns,
-    // and 2 panels (K up to 256) elsewhere, where the in-group updates would
-    // cost more than the traffic they save. Only full groups are grouped: the
+    // group4_rows rows (8192 by default), where the trailing matrix dwarfs the
+    // group's columns, 2 panels (K up to 256) in fronts of at least
+    // group2_rows, and single panels below that, where the in-group updates
+    // would cost more than the traffic they save. The thresholds are analysis
+    // options, which the autotuner (aphi_b200.autotune) picks per mesh. Only full groups are grouped: the
     // narrow tiles then end exactly at the group's last column, and a front's
     // incomplete last group is updated panel by panel.
+    const int group4 = A.opt.group4_rows > 0 ? A.opt.group4_rows : kGroup4Rows;
+    const int group2 = A.opt.group2_rows > 0 ? A.opt.group2_rows : 0;
     for (int L = 0; L < S.num_levels; ++L) {
         const int* lb = S.level_list.data() + S.level_ptr[L];
         const int* le = S.level_list.data() + S.level_ptr[L + 1];
@@ -105,7 +109,7 @@ void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing,
                     const bool panel_done = (k0 + kStep) % kTcPanel == 0 || k0 + kStep >= w;
                     if (!panel_done) continue;
                     const int m = S.sn_rows[s];
-                    const int G = m >= kGroup4Rows ? 4 : 2;
+                    const int G = m >= group4 ? 4 : (m >= group2 ? 2 : 1);
                     const int q = (k0 / kTcPanel) % G;        // the panel's place in its group
                     int p0 = (k0 / kTcPanel) * kTcPanel;
                     const int pe = std::min(w, p0 + kTcPanel);

@@ -15,6 +15,8 @@ void aphi_analysis_default_options(aphi_analysis_options* o) {
     o->relax_fill = 0.05;
     o->relax_max_width = 256;
     o->small_front = 96;
+    o->group4_rows = kGroup4Rows;
+    o->group2_rows = 0;
 }
 
 int aphi_analysis_create(int n, const int* row_ptr, const int* col_idx, const int* perm, const int* parent,

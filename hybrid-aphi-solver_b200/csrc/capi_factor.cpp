@@ -70,6 +70,14 @@ int aphi_factor_set_batch(aphi_factor* f, int batch) {
     });
 }
 
+int aphi_factor_set_tc_split(aphi_factor* f, int split) {
+    return guard([&] {
+        if (!f) throw Error(APHI_ERR_INVALID, "aphi_factor_set_tc_split: null factor");
+        if (split != 2 && split != 3) throw Error(APHI_ERR_BAD_SHAPE, "aphi_factor_set_tc_split: split must be 2 or 3");
+        f->tc_split = split;
+    });
+}
+
 int aphi_factor_profile(aphi_factor* f, int enable) {
     return guard([&] {
         if (!f) throw Error(APHI_ERR_INVALID, "aphi_factor_profile: null factor");

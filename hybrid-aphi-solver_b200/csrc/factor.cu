@@ -284,9 +284,14 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
                 k_update_panel<R><<<grid, 256, 2 * kStep * kTile * sizeof(cx<R>), st>>>(S, l.first, L, CB, ls, cs);
                 break;
             case K_UPDATE_TC:
-                if constexpr (sizeof(R) == 4)
-                    k_update_tc<<<grid, kTcThreads, kTcSmem, st>>>(S, l.first, L, CB, ls, cs, l.kcap, f->err);
-                else
+                if constexpr (sizeof(R) == 4) {
+                    if (f->tc_split == 2)
+                        k_update_tc<2><<<grid, kTcThreads, TcSmem<2>::bytes, st>>>(S, l.first, L, CB, ls, cs,
+                                                                                   l.kcap, f->err);
+                    else
+                        k_update_tc<3><<<grid, kTcThreads, TcSmem<3>::bytes, st>>>(S, l.first, L, CB, ls, cs,
+                                                                                   l.kcap, f->err);
+                } else
                     throw Error(APHI_ERR_INVALID, "tensor-core update planned for an FP64 factor");
                 break;
             case K_FWD_GATHER: k_fwd_gather<R><<<grid, 256, 0, st>>>(S, l.first, *sa, y, U); break;
@@ -334,7 +339,10 @@ void set_smem_limits(int small_front) {
     if constexpr (sizeof(R) == 8)
         APHI_CUDA(cudaFuncSetAttribute(k_update_wide_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, kDmmaSmem));
     if constexpr (sizeof(R) == 4)
-        APHI_CUDA(cudaFuncSetAttribute(k_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+        APHI_CUDA(cudaFuncSetAttribute(k_update_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TcSmem<3>::bytes));
+        APHI_CUDA(cudaFuncSetAttribute(k_update_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TcSmem<2>::bytes));
     APHI_CUDA(cudaFuncSetAttribute(k_fwd_diag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    kSolveDiagSmem * static_cast<int>(sizeof(cx<R>))));
     APHI_CUDA(cudaFuncSetAttribute(k_bwd_diag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -434,6 +442,8 @@ aphi_factor* factor_create(aphi_analysis* an, int precision, int batch) {
         f->elem = precision == 64 ? 16 : 8;
         const char* no_tc = std::getenv("APHI_NO_TC");
         f->use_tc = !(no_tc && no_tc[0] == '1');
+        const char* split = std::getenv("APHI_TC_SPLIT");
+        f->tc_split = split && split[0] == '2' ? 2 : 3;
         const Symbolic& S = an->S;
         APHI_CUDA(cudaMalloc(&f->L, static_cast<size_t>(std::max<long long>(S.stored, 1)) * batch * f->elem));
         f->dscale = dalloc<double>(static_cast<size_t>(S.n) * batch);

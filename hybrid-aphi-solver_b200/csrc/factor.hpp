@@ -36,6 +36,7 @@ struct aphi_factor {
     int kr_cap = 0;
     bool factored = false;
     bool use_tc = true;         // FP32: tensor-core updates (APHI_NO_TC=1 selects the SIMT kernels)
+    int tc_split = 3;           // FP32 tensor-core updates: TF32 pieces per operand (3, or 2: hh + hl + lh)
     int* err = nullptr;         // device error word (bounded waits)
     int* kmax = nullptr;        // capacity: the column where each entry's factorization stopped
     // Per-kind launch timing (aphi_factor_profile).

@@ -13,10 +13,11 @@
 namespace aphi_b200 {
 namespace {
 
+template <int Split>
 __global__ void __launch_bounds__(kTcThreads) k_tc_selftest(const float2* P, int rows, int K, int i0, int j0,
                                                            const float2* d, float2* out, int* err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const bool ok = tc_tile(smem_raw, P, rows, rows, K, i0, j0, d, 1,
+    const bool ok = tc_tile<Split>(smem_raw, P, rows, rows, K, i0, j0, d, 1,
                             [&](int r, int c0, const float(&re)[16], const float(&im)[16]) {
                                 for (int c = 0; c < 16; ++c) out[r + (c0 + c) * kTcM] = make_float2(re[c], im[c]);
                             });
@@ -63,10 +64,12 @@ extern "C" int aphi_selftest_bounded_wait(long long spin_limit) {
     });
 }
 
-extern "C" int aphi_selftest_tc_tile(int rows, int K, int i0, int j0, const float* P, const float* d, float* out) {
+extern "C" int aphi_selftest_tc_tile_split(int split, int rows, int K, int i0, int j0, const float* P,
+                                           const float* d, float* out) {
     using namespace aphi_b200;
     return guard([&] {
         if (!P || !out) throw Error(APHI_ERR_INVALID, "selftest: null pointer");
+        if (split != 2 && split != 3) throw Error(APHI_ERR_BAD_SHAPE, "selftest: split must be 2 or 3");
         if (rows < 1 || K < 1 || K > kTcPanel || i0 < 0 || j0 < 0)
             throw Error(APHI_ERR_BAD_SHAPE, "selftest: rows >= 1, 1 <= K <= 128, i0, j0 >= 0");
         float2 *dP = nullptr, *dd = nullptr, *dout = nullptr;
@@ -82,8 +85,15 @@ extern "C" int aphi_selftest_tc_tile(int rows, int K, int i0, int j0, const floa
                 APHI_CUDA(cudaMalloc(&dd, static_cast<size_t>(K) * sizeof(float2)));
                 APHI_CUDA(cudaMemcpy(dd, d, static_cast<size_t>(K) * sizeof(float2), cudaMemcpyHostToDevice));
             }
-            APHI_CUDA(cudaFuncSetAttribute(k_tc_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
-            k_tc_selftest<<<1, kTcThreads, kTcSmem>>>(dP, rows, K, i0, j0, dd, dout, derr);
+            if (split == 3) {
+                APHI_CUDA(cudaFuncSetAttribute(k_tc_selftest<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               TcSmem<3>::bytes));
+                k_tc_selftest<3><<<1, kTcThreads, TcSmem<3>::bytes>>>(dP, rows, K, i0, j0, dd, dout, derr);
+            } else {
+                APHI_CUDA(cudaFuncSetAttribute(k_tc_selftest<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               TcSmem<2>::bytes));
+                k_tc_selftest<2><<<1, kTcThreads, TcSmem<2>::bytes>>>(dP, rows, K, i0, j0, dd, dout, derr);
+            }
             APHI_CHECK_LAUNCH();
             int e = 0;
             APHI_CUDA(cudaMemcpy(&e, derr, sizeof(int), cudaMemcpyDeviceToHost));
@@ -102,4 +112,8 @@ extern "C" int aphi_selftest_tc_tile(int rows, int K, int i0, int j0, const floa
         cudaFree(dout);
         cudaFree(derr);
     });
+}
+
+extern "C" int aphi_selftest_tc_tile(int rows, int K, int i0, int j0, const float* P, const float* d, float* out) {
+    return aphi_selftest_tc_tile_split(3, rows, K, i0, j0, P, d, out);
 }

@@ -127,8 +127,11 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Four values -> hi, mid, lo (each exactly a TF32 number, hi + mid + lo == v)
-// stored as one 16-byte row of a core matrix in each of three planes.
+// Four values -> their TF32 pieces, stored as one 16-byte row of a core
+// matrix in each of Split planes. Split 3: hi, mid, lo, each exactly a TF32
+// number, hi + mid + lo == v. Split 2: hi and lo = the rounded remainder,
+// hi + lo == v to 2^-22 relative.
+template <int Split>
 __device__ __forceinline__ void split_store4(unsigned char* plane0, int plane_bytes, uint32_t off, const float (&v)[4]) {
     float4 h, m, l;
     float* hp = &h.x;
@@ -145,7 +148,7 @@ __device__ __forceinline__ void split_store4(unsigned char* plane0, int plane_by
     }
     *reinterpret_cast<float4*>(plane0 + off) = h;
     *reinterpret_cast<float4*>(plane0 + plane_bytes + off) = m;
-    *reinterpret_cast<float4*>(plane0 + 2 * plane_bytes + off) = l;
+    if constexpr (Split == 3) *reinterpret_cast<float4*>(plane0 + 2 * plane_bytes + off) = l;
 }
 
 // Raw stage: A rows [k][128], B rows [k][64], pivots [k] (complex64). Thread
@@ -181,13 +184,14 @@ __device__ __forceinline__ void tc_fetch(unsigned char* raw, const float2* P, lo
 }
 
 // Raw stage -> split planes (A scaled by the pivots).
+template <int Split>
 __device__ __forceinline__ void tc_split(const unsigned char* raw, unsigned char* stage) {
     const int tid = threadIdx.x;
     const float2* rA = reinterpret_cast<const float2*>(raw);
     const float2* rB = reinterpret_cast<const float2*>(raw + kTcRawA);
     const float2* rD = reinterpret_cast<const float2*>(raw + kTcRawA + kTcRawB);
-    unsigned char* A = stage;                                   // Ar hi/mid/lo, Ai hi/mid/lo
-    unsigned char* B = stage + 2 * kTcSplit * kTcPlaneA;        // Br hi/mid/lo, Bi hi/mid/lo
+    unsigned char* A = stage;                                   // Ar pieces, then Ai pieces
+    unsigned char* B = stage + 2 * Split * kTcPlaneA;           // Br pieces, then Bi pieces
 #pragma unroll
     for (int g = 0; g < kTcK / 4; ++g) {
         float re[4], im[4];
@@ -198,8 +202,8 @@ __device__ __forceinline__ void tc_split(const unsigned char* raw, unsigned char
             im[q] = v.x * d.y + v.y * d.x;
         }
         const uint32_t o = plane_off(tid, 4 * g);
-        split_store4(A, kTcPlaneA, o, re);
-        split_store4(A + kTcSplit * kTcPlaneA, kTcPlaneA, o, im);
+        split_store4<Split>(A, kTcPlaneA, o, re);
+        split_store4<Split>(A + Split * kTcPlaneA, kTcPlaneA, o, im);
     }
     const int rowb = tid & (kTcN - 1), qb = tid >> 6;
     float re[4], im[4];
@@ -210,24 +214,27 @@ __device__ __forceinline__ void tc_split(const unsigned char* raw, unsigned char
         im[q] = v.y;
     }
     const uint32_t o = plane_off(rowb, 4 * qb);
-    split_store4(B, kTcPlaneB, o, re);
-    split_store4(B + kTcSplit * kTcPlaneB, kTcPlaneB, o, im);
+    split_store4<Split>(B, kTcPlaneB, o, re);
+    split_store4<Split>(B + Split * kTcPlaneB, kTcPlaneB, o, im);
 }
 
-// The 24 MMAs of one stage: for each kept split pair (pa, pb), the four real
+// The MMAs of one stage: for each kept split pair (pa, pb), the four real
 // products into Cr, Ci; pair 0 (hi, hi) into the main accumulators (restarted
 // when fresh_main), the rest into the correction accumulators (restarted when
-// fresh_corr).
+// fresh_corr). Split 3 keeps six pairs (hh, hm, mh, hl, lh, mm: 24 MMAs),
+// split 2 three (hh, hl, lh: 12 MMAs).
+template <int Split>
 __device__ __forceinline__ void tc_issue(uint32_t stage_addr, uint32_t tmem, bool fresh_main, bool fresh_corr) {
-    const uint32_t A0 = stage_addr, B0 = stage_addr + 2 * kTcSplit * kTcPlaneA;
+    const uint32_t A0 = stage_addr, B0 = stage_addr + 2 * Split * kTcPlaneA;
     const uint32_t id_pos = instr_desc(0), id_neg = instr_desc(1);
+    constexpr int np = Split == 3 ? 6 : 3;
     const int pa[6] = {0, 0, 1, 0, 2, 1}, pb[6] = {0, 1, 0, 2, 0, 1};
 #pragma unroll
-    for (int t = 0; t < 6; ++t) {
+    for (int t = 0; t < np; ++t) {
         const uint64_t ar = smem_desc(A0 + pa[t] * kTcPlaneA);
-        const uint64_t ai = smem_desc(A0 + (kTcSplit + pa[t]) * kTcPlaneA);
+        const uint64_t ai = smem_desc(A0 + (Split + pa[t]) * kTcPlaneA);
         const uint64_t br = smem_desc(B0 + pb[t] * kTcPlaneB);
-        const uint64_t bi = smem_desc(B0 + (kTcSplit + pb[t]) * kTcPlaneB);
+        const uint64_t bi = smem_desc(B0 + (Split + pb[t]) * kTcPlaneB);
         const uint32_t d_re = tmem + (t == 0 ? 0 : 2 * kTcN);
         const uint32_t d_im = d_re + kTcN;
         const bool fresh = t == 0 ? fresh_main : (t == 1 && fresh_corr);
@@ -265,13 +272,14 @@ __device__ __forceinline__ void tc_drain(uint32_t tmem, float (&sr)[kTcN], float
 // (warp r / 32, lane r % 32). Requires kTcSmem bytes of dynamic shared
 // memory (16-byte aligned). Returns false if a bounded wait expired (the
 // caller records the error).
-template <class Store>
+template <int Split, class Store>
 __device__ bool tc_tile(unsigned char* smem, const float2* P, long long ldp, int rows, int K, int i0, int j0,
                         const float2* dk, long long dstride, Store store) {
+    constexpr int kStage = TcBytes<Split>::stage;
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     unsigned char* planes = smem;
-    unsigned char* raws = smem + kTcPlaneStages * kTcStage;
+    unsigned char* raws = smem + kTcPlaneStages * kStage;
     uint64_t* mbar = reinterpret_cast<uint64_t*>(raws + kTcRawStages * kTcRawStage);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + kTcPlaneStages);
 
@@ -314,7 +322,7 @@ __device__ bool tc_tile(unsigned char* smem, const float2* P, long long ldp, int
             mine = mbar_wait(smem_u32(mbar + buf), ((c - kTcPlaneStages) / kTcPlaneStages) & 1);
         ok = __syncthreads_and(mine) != 0;  // also: every thread's raw copies of stage c are visible
         if (!ok) break;
-        tc_split(raws + (c % kTcRawStages) * kTcRawStage, planes + buf * kTcStage);
+        tc_split<Split>(raws + (c % kTcRawStages) * kTcRawStage, planes + buf * kStage);
         // Generic-proxy stores -> visible to the tensor core's async proxy.
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         // A new group starts: the previous group's main products, complete
@@ -332,7 +340,7 @@ __device__ bool tc_tile(unsigned char* smem, const float2* P, long long ldp, int
         asm volatile("tcgen05.fence::after_thread_sync;");
         if (!ok) break;
         if (tid == 0) {
-            tc_issue(smem_u32(planes + buf * kTcStage), tmem, group_start, c == 0);
+            tc_issue<Split>(smem_u32(planes + buf * kStage), tmem, group_start, c == 0);
             mma_commit(smem_u32(mbar + buf));
         }
         ++issued;

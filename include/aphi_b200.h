@@ -230,6 +230,8 @@ typedef struct {
     double relax_fill;     /* otherwise merge while padded zeros stay below this fraction */
     int relax_max_width;   /* never grow a supernode past this many columns */
     int small_front;       /* fronts up to this many rows use the one-CTA kernel */
+    int group4_rows;       /* fronts this tall apply their trailing updates 4 panels at a time (<= 0: 8192) */
+    int group2_rows;       /* shorter fronts this tall, 2 panels at a time; shorter still, one (<= 0: all 2) */
 } aphi_analysis_options;
 
 typedef struct aphi_analysis aphi_analysis;
@@ -272,6 +274,12 @@ int aphi_factor_destroy(aphi_factor* f);
  * entries. Discards the current factorization. For continuous batching,
  * where each batch's size is known only when it is formed. */
 int aphi_factor_set_batch(aphi_factor* f, int batch);
+/* FP32 factors: how many TF32 pieces the tensor-core trailing update splits
+ * each FP32 operand into. 3 (the default): hi + mid + lo, six cross products
+ * kept, every product more accurate than an FP32 multiply. 2: hi + lo, the
+ * products hh + hl + lh, half the tensor-core work, each product to about
+ * 2^-21 relative. The environment variable APHI_TC_SPLIT=2 sets the default. */
+int aphi_factor_set_tc_split(aphi_factor* f, int split);
 
 typedef struct {
     int ok;                    /* FactorStats::ok */
@@ -447,6 +455,9 @@ int aphi_measure_peaks(double* tflops);
  * NULL for ones). Rows of P at or beyond `rows` read as zero. K <= 128. The
  * kernel the FP32 factorization uses for its trailing updates. */
 int aphi_selftest_tc_tile(int rows, int K, int i0, int j0, const float* P, const float* d, float* out);
+/* The same tile with the operands split into `split` (2 or 3) TF32 pieces. */
+int aphi_selftest_tc_tile_split(int split, int rows, int K, int i0, int j0, const float* P, const float* d,
+                                float* out);
 /* The bounded device wait, exercised: one CTA waits on an mbarrier that
  * nothing will complete, with the tensor-core tile's own wait, giving up
  * after spin_limit tries (1 .. the tile's limit). Returns APHI_ERR_TIMEOUT,

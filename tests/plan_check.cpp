@@ -464,6 +464,8 @@ aphi_analysis_options default_options() {
     o.relax_fill = 0.05;
     o.relax_max_width = 256;
     o.small_front = 96;
+    o.group4_rows = kGroup4Rows;
+    o.group2_rows = 0;
     return o;
 }
 

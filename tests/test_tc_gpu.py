@@ -57,6 +57,22 @@ def test_tile_against_host_product(shape, with_d, cuda):
     assert (err <= 1e-5 * mag + 1e-30).all(), (err / np.maximum(mag, 1e-30)).max()
 
 
+@pytest.mark.parametrize("shape", SHAPES)
+def test_two_piece_split_tile(shape, cuda):
+    """The cheaper split (hi + lo, products hh + hl + lh: half the MMAs): each
+    product carries about 2^-21 relative error, so the tile must be within
+    2e-5 of the magnitude sum -- an FP32 dot product's accuracy to within a
+    few ulps."""
+    rows, K, i0, j0 = shape
+    rng = np.random.default_rng(rows * 1000 + K + 7)
+    P = (rng.normal(size=(rows, K)) + 1j * rng.normal(size=(rows, K))).astype(np.complex64)
+    d = (rng.normal(size=K) + 1j * rng.normal(size=K)).astype(np.complex64)
+    out = ab.tc_tile_selftest(P, i0, j0, d, split=2)
+    ref, mag = host_tile(P, i0, j0, d)
+    err = np.abs(out.astype(np.complex128) - ref)
+    assert (err <= 2e-5 * mag + 1e-30).all(), (err / np.maximum(mag, 1e-30)).max()
+
+
 def test_split_keeps_more_than_tf32(cuda):
     """Values that TF32 alone would round (10-bit mantissas) come out to FP32
     accuracy: the split carries the low bits through the tensor cores."""

@@ -89,19 +89,23 @@ def test_noalloc_at_the_size_limit_with_many_entries(cuda):
 
 
 def test_noalloc_refuses_sizes_beyond_its_array(cuda):
-    w = ab.Workload.cylinder(4)
-    an = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx))
+    """Both refusals come before any launch, so the buffers handed in are
+    never read: a scratch need beyond the array (300,000 unknowns x 400
+    right-hand sides), and more systems than one launch's grid.y holds."""
+    n = 300000
+    an = ab.Analysis(np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), np.arange(n, dtype=np.int32))
     f = ab.Factor(an)
-    vals = torch.zeros((1, an.nnz), dtype=torch.complex128, device="cuda")
-    v = torch.zeros((1, an.n), dtype=torch.complex128, device="cuda")
+    dummy = torch.zeros(2, dtype=torch.complex128, device="cuda")
     out = np.zeros(2)
-    rc = ab.lib().aphi_residuals_noalloc(an._h, 1, 1 << 22, ab.dptr(vals), ab.dptr(v), ab.dptr(v),
+    rc = ab.lib().aphi_residuals_noalloc(an._h, 1, 400, ab.dptr(dummy), ab.dptr(dummy), ab.dptr(dummy),
                                          out.ctypes.data_as(C.POINTER(C.c_double)), None)
     assert rc == ab.ERR_BAD_SHAPE
     assert "fixed" in ab.lib().aphi_last_error().decode()
-    # more systems than one launch's grid.y holds, though the scratch would fit
-    rc = ab.lib().aphi_residuals_noalloc(an._h, 1, 65536, ab.dptr(vals), ab.dptr(v), ab.dptr(v),
+    w = ab.Workload.cylinder(4)
+    an4 = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx))
+    f4 = ab.Factor(an4)
+    rc = ab.lib().aphi_residuals_noalloc(an4._h, 1, 65536, ab.dptr(dummy), ab.dptr(dummy), ab.dptr(dummy),
                                          out.ctypes.data_as(C.POINTER(C.c_double)), None)
     assert rc == ab.ERR_BAD_SHAPE
     assert "65535" in ab.lib().aphi_last_error().decode()
-    del f
+    del f, f4
