@@ -355,12 +355,24 @@ def run_ours(args):
         perm = ab.amd_ordering(w.row_ptr, w.col_idx)
     else:
         perm = ab.nested_dissection(w.row_ptr, w.col_idx, w.dof_xyz)
-    an = ab.Analysis(w.row_ptr, w.col_idx, perm)
-    info = an.info
     asm = ab.Assembly(ab.workload_arrays(w))
-    n = an.n
     # Each rank solves its own sweep: the frequencies shifted per rank.
     omegas = replicas.rank_omegas(rank, args.nfreq, F_LO, F_HI)
+    tune_record = None
+    if args.autotune:
+        # The schedule's knobs (panel groups, one-CTA fronts) tuned on this
+        # mesh by timed factorizations of two of the sweep's frequencies, in
+        # both precisions, weighted by how many entries each precision takes.
+        from aphi_b200 import autotune
+        tv, _ = asm.refill(omegas[[0, -1]])
+        an, tune_record = autotune.tune(w.row_ptr, w.col_idx, perm, tv, precisions=(ab.PREC_FP64, ab.PREC_FP32),
+                                        weights={ab.PREC_FP64: 9.0, ab.PREC_FP32: 7.0})
+        del tv
+        torch.cuda.empty_cache()
+    else:
+        an = ab.Analysis(w.row_ptr, w.col_idx, perm)
+    info = an.info
+    n = an.n
     stream = torch.cuda.current_stream()
 
     solver = ab.SweepSolver(an, asm, args.nfreq, "mixed", fp64_batch=args.fp64_batch, rtol=args.rtol,
@@ -551,6 +563,7 @@ def run_ours(args):
             "assembly_roofline": assembly_line,
             "solve_roofline": solve_line,
             "parity_vs_reference": parity,
+            "autotune": tune_record,
         }
         print(json.dumps(out))
     if world > 1:
@@ -575,6 +588,7 @@ def main():
                     help="TF32 pieces per FP32 operand in the tensor-core update (3: six products, 2: three)")
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--sample-cells", type=int, default=16)
+    ap.add_argument("--autotune", type=int, default=1, help="tune the schedule on this mesh first (untimed)")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

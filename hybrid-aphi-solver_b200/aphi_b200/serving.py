@@ -32,8 +32,14 @@ How it runs:
   * precision="mixed": FP32 factorization plus FP64 preconditioned COCG;
     entries whose refinement stalls are refactorized in FP64, and the mesh
     remembers the lowest frequency at which that happened so that later
-    requests at or above it go to FP64 directly. precision="fp64": FP64
+    requests at or above it go to FP64 directly. Each mesh is calibrated
+    first (`MeshCache.calibrate`): where one FP32-refined request costs more
+    than one FP64 request, the mesh's requests all go to FP64, so the mixed
+    server is never slower than the plain one. precision="fp64": FP64
     factorization and direct solve (the plain drop-in path).
+  * Load shedding (`max_queue`): a request that finds its mesh's queue full
+    is rejected at once, so an offered load beyond the device's rate gives a
+    bounded queue and honest latencies for the requests served.
 
 Each request's result depends only on its own system: batches never mix the
 arithmetic of different entries, so a request gives the same answer alone and
@@ -92,6 +98,37 @@ class MeshCache:
         self.lock = threading.Lock()
         # the analysis uploads its schedule when its first factor is made
         ab.Factor(self.analysis, ab.PREC_FP64, 1).close()
+        self.fp32_pays = True     # set by calibrate()
+        self.calibration = None
+
+    def calibrate(self, rtol: float = 1e-12, tol: float = 1e-15, max_iters: int = 40) -> dict:
+        """Times one request's worth of work both ways on this mesh, at the
+        low end of the band where FP32 refinement converges (50 Hz): FP64
+        factorization + direct solve, and FP32 factorization + FP64-refined
+        solve. Where the mixed path is not the faster one (small meshes, whose
+        factorizations are cheap next to the refinement's solves), mixed
+        serving routes this mesh's requests to FP64, so mixed never serves
+        slower than plain FP64."""
+        import torch
+        vals, rhs = self.assembly.refill(2 * np.pi * 50.0)
+        ms = {}
+        for name, prec in (("fp64", ab.PREC_FP64), ("fp32_ir", ab.PREC_FP32)):
+            f = ab.Factor(self.analysis, prec, 1)
+            for rep in range(2):      # the first pass is untimed
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                f.factorize(vals)
+                if prec == ab.PREC_FP64:
+                    f.solve(rhs)
+                else:
+                    f.solve_refined(vals, rhs, tol=tol, rtol=rtol, max_iters=max_iters)
+                e1.record()
+                torch.cuda.synchronize()
+                ms[name] = e0.elapsed_time(e1)
+            f.close()
+        self.fp32_pays = ms["fp32_ir"] < ms["fp64"]
+        self.calibration = ms
+        return ms
 
     def footprint(self, batch: int, nrhs: int, precision: int) -> int:
         """Device bytes a batch needs: the factor (panels), the contribution
@@ -110,7 +147,7 @@ class _Worker:
 class Server:
     def __init__(self, meshes: dict, precision: str = "mixed", workers: int = 2, max_batch: dict | None = None,
                  hbm_budget: float = 150e9, rtol: float = 1e-12, tol: float = 1e-15, max_iters: int = 40,
-                 target_residual: float = 1e-10):
+                 target_residual: float = 1e-10, max_queue: int | None = None):
         import torch
         if precision not in ("mixed", "fp64"):
             raise ab.InvalidArgument(ab.ERR_BAD_SHAPE, f"Server: precision {precision!r} is not mixed or fp64")
@@ -119,6 +156,10 @@ class Server:
         self.rtol, self.tol, self.max_iters = rtol, tol, max_iters
         self.target = target_residual
         self.budget = hbm_budget
+        # Load shedding: a request that finds this many requests of its mesh
+        # already waiting is rejected at once rather than queued without bound
+        # (None: no bound).
+        self.max_queue = max_queue
         self.max_batch = dict(max_batch or {c: (4 if c >= 32 else 8 if c >= 24 else 16) for c in meshes})
         # Admission by HBM footprint: every mesh keeps an FP64 factor (and an
         # FP32 one in mixed mode) of its batch capacity resident, allocated
@@ -157,6 +198,10 @@ class Server:
         with self.cv:
             if m is None or not 1 <= nrhs <= 8:
                 req.error = "rejected: no resident analysis for this mesh, or not 1-8 excitations"
+                self.rejected.append(req)
+                return
+            if self.max_queue is not None and len(self.queues[req.cells]) >= self.max_queue:
+                req.error = "shed: the mesh's queue is full"
                 self.rejected.append(req)
                 return
             self.queues[req.cells].append(req)
@@ -236,7 +281,7 @@ class Server:
             x = torch.empty_like(b)
             prec_of = ["fp64"] * nb
             todo = list(range(nb))
-            if self.precision == "mixed":
+            if self.precision == "mixed" and m.fp32_pays:
                 fp32 = [i for i in range(nb) if m.stall_omega is None or om[i] < m.stall_omega]
                 todo = [i for i in range(nb) if i not in fp32]
                 if fp32:
@@ -313,6 +358,7 @@ def run_trace(server: Server, trace: list) -> dict:
     span = max(r.done for r in done) - min(r.arrival for r in trace) if done else 1.0
     rhs = sum(len(r.voltages) for r in done)
     return {"requests": len(trace), "completed": len(done), "rejected": len(server.rejected),
+            "shed": sum(1 for r in server.rejected if r.error.startswith("shed")),
             "failed": sum(1 for r in server.finished if r.error),
             "solves_per_s": len(done) / span, "rhs_per_s": rhs / span, "span_s": span,
             "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
@@ -337,17 +383,21 @@ def main() -> None:
     ap.add_argument("--workers", type=int, default=2)
     ap.add_argument("--f-hi", type=float, default=1e8)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--max-queue", type=int, default=0, help="per-mesh queue bound (0: unbounded)")
     a = ap.parse_args()
     cells = [int(c) for c in a.cells.split(",")]
     t0 = time.perf_counter()
     meshes = {c: MeshCache(c) for c in cells}
+    calib = {}
+    if a.precision == "mixed":
+        calib = {c: dict(m.calibrate(), fp32_pays=m.fp32_pays) for c, m in meshes.items()}
     setup = time.perf_counter() - t0
     trace = make_trace(a.rate, a.duration, cells, f_hi=a.f_hi, seed=a.seed)
-    srv = Server(meshes, a.precision, workers=a.workers)
+    srv = Server(meshes, a.precision, workers=a.workers, max_queue=a.max_queue or None)
     out = run_trace(srv, trace)
     srv.close()
     out.update({"precision": a.precision, "rate": a.rate, "duration_s": a.duration, "workers": a.workers,
-                "mesh_setup_s": setup, "cells": cells})
+                "mesh_setup_s": setup, "cells": cells, "max_queue": a.max_queue or None, "calibration": calib})
     print(json.dumps(out))
 
 

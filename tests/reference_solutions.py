@@ -28,7 +28,7 @@ def load(cells: int) -> dict | None:
         return None
     z = np.load(p)
     shape = tuple(int(v) for v in z["x_shape"])
-    x = np.ascontiguousarray(z["x_shuffled"].T).view(np.complex128).reshape(shape)
+    x = np.ascontiguousarray(z["x_shuffled"].T).reshape(-1).view(np.complex128).reshape(shape)
     keys = [str(k) for k in z["report_keys"]]
     return dict(omegas=z["omegas"], sweep_index=z["sweep_index"], x=x,
                 reports=[dict(zip(keys, row.tolist())) for row in z["report"]],
