@@ -584,7 +584,7 @@ def main():
     ap.add_argument("--rtol", type=float, default=1e-14,
                     help="relative-residual target of the refinement (the FP64 direct solve's own level)")
     ap.add_argument("--fp64-batch", type=int, default=8)
-    ap.add_argument("--tc-split", type=int, default=3, choices=[2, 3],
+    ap.add_argument("--tc-split", type=int, default=2, choices=[2, 3],
                     help="TF32 pieces per FP32 operand in the tensor-core update (3: six products, 2: three)")
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--sample-cells", type=int, default=16)

@@ -169,6 +169,7 @@ _SIGS = {
     "aphi_csc_solve_host": (I, [I, PI, PI, PD, PD, I, PD]),
     "aphi_csr_residuals_host": (I, [I, PI, PI, PD, I, PD, PD, PD]),
     "aphi_factor_set_tc_split": (I, [P, I]),
+    "aphi_spmv": (I, [P, I, I, P, P, P, P]),
     "aphi_selftest_tc_tile_split": (I, [I, I, I, I, I, P, P, P]),
 }
 
@@ -811,6 +812,20 @@ def residuals(analysis: Analysis, values, x, b, stream=None) -> np.ndarray:
     return out
 
 
+def spmv(analysis: Analysis, values, x, stream=None):
+    """A x on the original upper-stored systems (device tensors; x [batch, n]
+    or [batch, nrhs, n]), SparseSymmetric::matvec
+    (include/aphi_solver/sparse_symmetric.hpp:120-136)."""
+    import torch
+    xx = (x.unsqueeze(1) if x.dim() == 2 else x).contiguous()
+    batch, nrhs = xx.shape[0], xx.shape[1]
+    _expect_device(values, (batch, analysis.nnz), "spmv: values")
+    _expect_device(xx, (batch, nrhs, analysis.n), "spmv: x")
+    y = torch.empty_like(xx)
+    check(lib().aphi_spmv(analysis._h, batch, nrhs, dptr(values), dptr(xx), dptr(y), stream_ptr(stream)))
+    return y.squeeze(1) if x.dim() == 2 else y
+
+
 def measure_peaks() -> dict:
     """Arithmetic peaks of the current device in TFLOP/s (aphi_measure_peaks)."""
     out = np.zeros(5)
@@ -888,6 +903,10 @@ class SweepSolver:
     most fp64_batch (FP64) or fp32_batch (FP32) entries per factorization, so
     no factorization is spent on padding.
 
+    tc_split: TF32 pieces per FP32 operand in the tensor-core updates of the
+    FP32 factors. 2 (hh + hl + lh, half the tensor-core work of 3) by default:
+    on the 32^3 sweep it needs the same refinement iterations as 3 (4-13).
+
     fp64_refine=True refines every FP64-factorized entry (fallbacks included)
     by COCG preconditioned with its own FP64 factor, to the same rtol / tol:
     for systems whose plain FP64 direct solve stops short of the residual
@@ -897,7 +916,7 @@ class SweepSolver:
     def __init__(self, analysis: Analysis, assembly: Assembly, batch: int, precision: str = "mixed",
                  fp64_batch: int = 8, rtol: float = 1e-14, tol: float = 1e-16, max_iters: int = 40,
                  fp32_batch: int | None = None, predict: bool = True, fp64_refine: bool = False,
-                 tc_split: int = 3):
+                 tc_split: int = 2):
         if precision not in ("mixed", "fp64"):
             raise InvalidArgument(ERR_BAD_SHAPE, f"SweepSolver: precision {precision!r} is not 'mixed' or 'fp64'")
         self.analysis, self.assembly = analysis, assembly
@@ -924,7 +943,7 @@ class SweepSolver:
                 f.close()
                 self._factors.pop(precision)
             f = Factor(self.analysis, precision, size)
-            if precision == PREC_FP32 and self.tc_split != 3:
+            if precision == PREC_FP32:
                 f.set_tc_split(self.tc_split)
             if self._profile:
                 f.profile(True)

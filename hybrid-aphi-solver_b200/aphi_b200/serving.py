@@ -114,6 +114,8 @@ class MeshCache:
         ms = {}
         for name, prec in (("fp64", ab.PREC_FP64), ("fp32_ir", ab.PREC_FP32)):
             f = ab.Factor(self.analysis, prec, 1)
+            if prec == ab.PREC_FP32:
+                f.set_tc_split(2)
             for rep in range(2):      # the first pass is untimed
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record()
@@ -175,6 +177,9 @@ class Server:
                 self.max_batch[c] //= 2
         self.footprint = total()
         self.factors = {(c, p): ab.Factor(m.analysis, p, self.max_batch[c]) for c, m in meshes.items() for p in precs}
+        for (c, p), f in self.factors.items():
+            if p == ab.PREC_FP32:
+                f.set_tc_split(2)     # hh + hl + lh: the refinement needs no more iterations than with 3
         self.queues = {c: collections.deque() for c in meshes}
         self.busy = set()
         self.cv = threading.Condition()

@@ -375,6 +375,9 @@ struct TetStage {
     double volume;
     int idx[16];
     unsigned short rec[kTetMaxTerms];  // kind << 8 | i << 4 | j
+    // per frequency of the batch: the body's coefficients and the scalings
+    Coeff cf[kMaxBatchOmegas];
+    cplx col[kMaxBatchOmegas], rjw[kMaxBatchOmegas], rc[kMaxBatchOmegas];
 };
 
 __device__ __forceinline__ double dot3s(const double* u, const double* v) { return dot3(u, v); }
@@ -520,6 +523,17 @@ __global__ void __launch_bounds__(32 * kTetWarps) k_tet_terms(TetArgs A, Omegas 
     }
     __syncwarp();
     const int nf = om.n;
+    // The body's coefficients and the formulation's scalings, once per
+    // frequency (they hold divisions), for every term of the tet.
+    for (int f = lane; f < nf; f += 32) {
+        const double omega = om.w[f];
+        S.cf[f] = body_coefficients(S.mat[0], S.mat[1], S.mat[2], omega);
+        const Scales sc = scales_of(cond, omega);
+        S.col[f] = sc.col;
+        S.rjw[f] = cmul_exact(sc.row, sc.jw);
+        S.rc[f] = cmul_exact(sc.row, sc.col);
+    }
+    __syncwarp();
     const double vol = S.volume;
     const double w = __dmul_rn(0.25, vol);
     cplx* out = terms + off * nf;
@@ -527,8 +541,7 @@ __global__ void __launch_bounds__(32 * kTetWarps) k_tet_terms(TetArgs A, Omegas 
         const int k = it / nf, f = it - k * nf;
         const int r = S.rec[k];
         const int kind = r >> 8, i = (r >> 4) & 15, j = r & 15;
-        const double omega = om.w[f];
-        const Coeff c = body_coefficients(S.mat[0], S.mat[1], S.mat[2], omega);
+        const Coeff& c = S.cf[f];
         cplx blk{0.0, 0.0};
         if (kind == T_AA) {
             // kernel_AA: nu V curl.curl, then the mass term point by point.
@@ -546,26 +559,21 @@ __global__ void __launch_bounds__(32 * kTetWarps) k_tet_terms(TetArgs A, Omegas 
                 blk = cadd_exact(blk, cscale_exact(c.beta, __dmul_rn(w, dot3s(u, S.gr[q][j]))));
             }
         }
-        const Scales sc = scales_of(cond, omega);
+        const cplx col = S.col[f];
         cplx term;
         switch (kind) {
             case T_AA: term = cscale_exact(blk, __dmul_rn(S.co[i], S.co[j])); break;
-            case T_AP: term = cmul_exact(cscale_exact(sc.col, __dmul_rn(S.co[i], S.co[6 + j])), blk); break;
+            case T_AP: term = cmul_exact(cscale_exact(col, __dmul_rn(S.co[i], S.co[6 + j])), blk); break;
             case T_AP_FIXED: {
-                const cplx fx = cdiv_smith(cplx{S.fixed[j][0], S.fixed[j][1]}, sc.col);
-                term = cneg(cmul_exact(cmul_exact(cscale_exact(sc.col, S.co[i]), blk), fx));
+                const cplx fx = cdiv_smith(cplx{S.fixed[j][0], S.fixed[j][1]}, col);
+                term = cneg(cmul_exact(cmul_exact(cscale_exact(col, S.co[i]), blk), fx));
                 break;
             }
-            case T_PA:
-                term = cmul_exact(cscale_exact(cmul_exact(sc.row, sc.jw), __dmul_rn(S.co[6 + j], S.co[i])), blk);
-                break;
-            case T_PP:
-                term = cmul_exact(cscale_exact(cmul_exact(sc.row, sc.col), __dmul_rn(S.co[6 + i], S.co[6 + j])),
-                                  blk);
-                break;
+            case T_PA: term = cmul_exact(cscale_exact(S.rjw[f], __dmul_rn(S.co[6 + j], S.co[i])), blk); break;
+            case T_PP: term = cmul_exact(cscale_exact(S.rc[f], __dmul_rn(S.co[6 + i], S.co[6 + j])), blk); break;
             default: {
-                const cplx fx = cdiv_smith(cplx{S.fixed[j][0], S.fixed[j][1]}, sc.col);
-                term = cneg(cmul_exact(cmul_exact(cscale_exact(cmul_exact(sc.row, sc.col), S.co[6 + i]), blk), fx));
+                const cplx fx = cdiv_smith(cplx{S.fixed[j][0], S.fixed[j][1]}, col);
+                term = cneg(cmul_exact(cmul_exact(cscale_exact(S.rc[f], S.co[6 + i]), blk), fx));
                 break;
             }
         }

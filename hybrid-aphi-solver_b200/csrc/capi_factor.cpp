@@ -113,6 +113,16 @@ int aphi_residuals(const aphi_analysis* an, int batch, int nrhs, const double* v
     });
 }
 
+int aphi_spmv(const aphi_analysis* an, int batch, int nrhs, const double* values_dev, const double* x_dev,
+              double* y_dev, void* stream) {
+    return guard([&] {
+        if (!an || !values_dev || !x_dev || !y_dev) throw Error(APHI_ERR_INVALID, "aphi_spmv: null argument");
+        if (batch < 1 || nrhs < 1) throw Error(APHI_ERR_BAD_SHAPE, "aphi_spmv: batch and nrhs must be >= 1");
+        analysis_ensure_device(const_cast<aphi_analysis*>(an));
+        spmv(an, batch, nrhs, values_dev, x_dev, y_dev, as_stream(stream));
+    });
+}
+
 int aphi_residuals_noalloc(const aphi_analysis* an, int batch, int nrhs, const double* values_dev,
                            const double* x_dev, const double* b_dev, double* out, void* stream) {
     return guard([&] {

@@ -1198,6 +1198,17 @@ int solve_krylov(aphi_factor* f, int nrhs, const double* values, const double* b
     return status;
 }
 
+void spmv(const aphi_analysis* an, int batch, int nrhs, const double* values, const double* x, double* y,
+          cudaStream_t st) {
+    if (static_cast<long long>(batch) * nrhs > kMaxGridY)
+        throw Error(APHI_ERR_BAD_SHAPE, "spmv: batch x nrhs exceeds the 65535 systems one call handles");
+    const int n = an->S.n;
+    if (n == 0) return;
+    k_spmv<<<dim3(ceil_div(n, 256), batch * nrhs), 256, 0, st>>>(n, nrhs, an->d.fptr, an->d.fcol, an->d.fmap, values,
+                                                               an->S.nnz_a, x, y);
+    APHI_CHECK_LAUNCH();
+}
+
 void factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, double* value, double* diagonal,
                    double* d_scale) {
     const aphi_analysis* A = f->an;

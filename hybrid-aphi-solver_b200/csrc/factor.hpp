@@ -71,6 +71,8 @@ void residuals(const aphi_analysis* an, int batch, int nrhs, const double* value
                const double* b_dev, double* out, cudaStream_t stream);
 void residuals_noalloc(const aphi_analysis* an, int batch, int nrhs, const double* values_dev,
                        const double* x_dev, const double* b_dev, double* out, cudaStream_t stream);
+void spmv(const aphi_analysis* an, int batch, int nrhs, const double* values_dev, const double* x_dev, double* y_dev,
+          cudaStream_t stream);
 void csc_solve_host(int n, const int* col_ptr, const int* row_index, const double* value, const double* diagonal,
                     int nrhs, double* y);
 void csr_residuals_host(int n, const int* row_ptr, const int* col_idx, const double* values, int nrhs,

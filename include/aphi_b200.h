@@ -321,6 +321,12 @@ int aphi_factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index
 int aphi_residuals(const aphi_analysis* an, int batch, int nrhs, const double* values_dev,
                    const double* x_dev, const double* b_dev, double* out, void* stream);
 
+/* y = A x on the original upper-stored A (both triangles), per batch entry
+ * and rhs: SparseSymmetric::matvec, include/aphi_solver/sparse_symmetric.hpp:
+ * 120-136. x, y: batch x nrhs x N complex (device). */
+int aphi_spmv(const aphi_analysis* an, int batch, int nrhs, const double* values_dev, const double* x_dev,
+              double* y_dev, void* stream);
+
 /* The same numbers as aphi_residuals, computed without allocating device
  * memory: for callers that cannot call cudaMalloc while they run -- a serving
  * loop whose memory pool already owns the device's free memory, or a
