@@ -907,6 +907,11 @@ class SweepSolver:
     FP32 factors. 2 (hh + hl + lh, half the tensor-core work of 3) by default:
     on the 32^3 sweep it needs the same refinement iterations as 3 (4-13).
 
+    overlap=True: entries predicted to need FP64 are factorized and solved on
+    a side stream, from a second host thread, while the FP32 entries are
+    being refined (results are the same either way; only the schedule
+    changes).
+
     fp64_refine=True refines every FP64-factorized entry (fallbacks included)
     by COCG preconditioned with its own FP64 factor, to the same rtol / tol:
     for systems whose plain FP64 direct solve stops short of the residual
@@ -916,7 +921,7 @@ class SweepSolver:
     def __init__(self, analysis: Analysis, assembly: Assembly, batch: int, precision: str = "mixed",
                  fp64_batch: int = 8, rtol: float = 1e-14, tol: float = 1e-16, max_iters: int = 40,
                  fp32_batch: int | None = None, predict: bool = True, fp64_refine: bool = False,
-                 tc_split: int = 2):
+                 tc_split: int = 2, overlap: bool = True):
         if precision not in ("mixed", "fp64"):
             raise InvalidArgument(ERR_BAD_SHAPE, f"SweepSolver: precision {precision!r} is not 'mixed' or 'fp64'")
         self.analysis, self.assembly = analysis, assembly
@@ -927,6 +932,8 @@ class SweepSolver:
         self.predict = predict
         self.fp64_refine = fp64_refine
         self.tc_split = tc_split
+        self.overlap = overlap
+        self._side_stream = None
         self.stall_omega = None      # lowest frequency whose FP32 refinement stalled
         self._factors = {}
         self._profile = False
@@ -996,6 +1003,50 @@ class SweepSolver:
         size = -(-len(idx) // nb) if nb else 0
         return [idx[c:c + size] for c in range(0, len(idx), size)] if size else []
 
+    def _fp64_chunk(self, idx, vals, rhs, stream):
+        import torch
+        f = self._factor(PREC_FP64, len(idx))
+        sel = torch.tensor(idx, device=vals.device)
+        v = vals.index_select(0, sel)
+        f.factorize(v, 10, 0.0, stream=stream)
+        self.factorized[PREC_FP64] += len(idx)
+        iters = [0] * len(idx)
+        if self.fp64_refine:
+            xs, it, _, _ = f.solve_refined(v, rhs.index_select(0, sel), tol=self.tol, rtol=self.rtol,
+                                           max_iters=self.max_iters, stream=stream)
+            iters = [int(it[q, 0]) for q in range(len(idx))]
+        else:
+            xs = f.solve(rhs.index_select(0, sel), stream=stream)
+        return xs, iters
+
+    def _start_fp64(self, todo, vals, rhs, stream):
+        """FP64 factorizations and solves of `todo` on the side stream, in a
+        thread; returns (thread, box) with box["parts"] = [(idx, x, iters)] and
+        box["event"] recorded on the side stream after the last of them."""
+        import threading
+        import torch
+        if self._side_stream is None:
+            self._side_stream = torch.cuda.Stream(device=vals.device)
+        side = self._side_stream
+        ready = torch.cuda.Event()
+        ready.record(stream or torch.cuda.current_stream())
+        box = {"parts": [], "error": None, "event": torch.cuda.Event()}
+
+        def run():
+            try:
+                with torch.cuda.stream(side):
+                    side.wait_event(ready)
+                    for idx in self._chunks(sorted(todo), self.fp64_batch):
+                        xs, iters = self._fp64_chunk(idx, vals, rhs, side)
+                        box["parts"].append((idx, xs, iters))
+                    box["event"].record(side)
+            except Exception as e:  # re-raised by the caller after join
+                box["error"] = e
+
+        t = threading.Thread(target=run, daemon=True)
+        t.start()
+        return t, box
+
     def close(self):
         for f in self._factors.values():
             f.close()
@@ -1024,6 +1075,16 @@ class SweepSolver:
             else:
                 todo.append(k)
                 reports[k]["predicted_fp64"] = self.precision == "mixed"
+        # Entries known in advance to need FP64 are factorized on a side stream
+        # from a second host thread while the FP32 entries are refined: the
+        # refinement's solves are small, latency-bound launches that leave
+        # most of the device to the FP64 factorization. The two factorizations
+        # share the analysis's workspace and take turns on it; the solves do
+        # not touch it.
+        side = None
+        side_todo = []
+        if self.overlap and todo and fp32_idx:
+            side_todo, todo = todo, []
         for idx in self._chunks(fp32_idx, self.fp32_batch):
             f = self._factor(PREC_FP32, len(idx))
             whole = len(idx) == self.batch
@@ -1032,6 +1093,9 @@ class SweepSolver:
             b = rhs if whole else rhs.index_select(0, sel)
             f.factorize(v, 10, 0.0, stream=stream)
             self.factorized[PREC_FP32] += len(idx)
+            if side_todo and side is None:
+                # after the FP32 factorization has released the workspace
+                side = self._start_fp64(side_todo, vals, rhs, stream)
             xs, iters, berr, _ = f.solve_refined(v, b, tol=self.tol, rtol=self.rtol, max_iters=self.max_iters,
                                                  stream=stream)
             res = residuals(self.analysis, v, xs, b, stream=stream)
@@ -1047,6 +1111,19 @@ class SweepSolver:
                     todo.append(k)
                     if self.stall_omega is None or om[k] < self.stall_omega:
                         self.stall_omega = float(om[k])
+        if side is not None:
+            thread, box = side
+            thread.join()
+            if box.get("error") is not None:
+                raise box["error"]
+            done_ev, parts = box["event"], box["parts"]
+            main = stream or torch.cuda.current_stream()
+            main.wait_event(done_ev)
+            for idx, xs, iters in parts:
+                xs.record_stream(main)   # read here, allocated on the side stream
+                x.index_copy_(0, torch.tensor(idx, device=vals.device), xs)
+                for q, k in enumerate(idx):
+                    reports[k]["iterations"] = iters[q]
         todo.sort()
         for idx in self._chunks(todo, self.fp64_batch):
             f = self._factor(PREC_FP64, len(idx))

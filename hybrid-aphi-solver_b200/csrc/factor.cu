@@ -285,12 +285,16 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
                 break;
             case K_UPDATE_TC:
                 if constexpr (sizeof(R) == 4) {
-                    if (f->tc_split == 2)
-                        k_update_tc<2><<<grid, kTcThreads, TcSmem<2>::bytes, st>>>(S, l.first, L, CB, ls, cs,
-                                                                                   l.kcap, f->err);
-                    else
-                        k_update_tc<3><<<grid, kTcThreads, TcSmem<3>::bytes, st>>>(S, l.first, L, CB, ls, cs,
-                                                                                   l.kcap, f->err);
+                    // split 3: two plane stages (3 would leave one CTA per SM);
+                    // split 2: plane stages and accumulator group as configured.
+                    const int v = f->tc_split == 3 ? 0 : (f->tc_stages == 3 ? 2 : 0) + (f->tc_group == 4 ? 1 : 0) + 1;
+                    switch (v) {
+                        case 0: k_update_tc<3, 2, 2><<<grid, kTcThreads, TcSmem<3, 2>::bytes, st>>>(S, l.first, L, CB, ls, cs, l.kcap, f->err); break;
+                        case 1: k_update_tc<2, 2, 2><<<grid, kTcThreads, TcSmem<2, 2>::bytes, st>>>(S, l.first, L, CB, ls, cs, l.kcap, f->err); break;
+                        case 2: k_update_tc<2, 2, 4><<<grid, kTcThreads, TcSmem<2, 2>::bytes, st>>>(S, l.first, L, CB, ls, cs, l.kcap, f->err); break;
+                        case 3: k_update_tc<2, 3, 2><<<grid, kTcThreads, TcSmem<2, 3>::bytes, st>>>(S, l.first, L, CB, ls, cs, l.kcap, f->err); break;
+                        default: k_update_tc<2, 3, 4><<<grid, kTcThreads, TcSmem<2, 3>::bytes, st>>>(S, l.first, L, CB, ls, cs, l.kcap, f->err); break;
+                    }
                 } else
                     throw Error(APHI_ERR_INVALID, "tensor-core update planned for an FP64 factor");
                 break;
@@ -339,10 +343,16 @@ void set_smem_limits(int small_front) {
     if constexpr (sizeof(R) == 8)
         APHI_CUDA(cudaFuncSetAttribute(k_update_wide_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, kDmmaSmem));
     if constexpr (sizeof(R) == 4)
-        APHI_CUDA(cudaFuncSetAttribute(k_update_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       TcSmem<3>::bytes));
-        APHI_CUDA(cudaFuncSetAttribute(k_update_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       TcSmem<2>::bytes));
+        APHI_CUDA(cudaFuncSetAttribute(k_update_tc<3, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TcSmem<3, 2>::bytes));
+        APHI_CUDA(cudaFuncSetAttribute(k_update_tc<2, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TcSmem<2, 2>::bytes));
+        APHI_CUDA(cudaFuncSetAttribute(k_update_tc<2, 2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TcSmem<2, 2>::bytes));
+        APHI_CUDA(cudaFuncSetAttribute(k_update_tc<2, 3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TcSmem<2, 3>::bytes));
+        APHI_CUDA(cudaFuncSetAttribute(k_update_tc<2, 3, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TcSmem<2, 3>::bytes));
     APHI_CUDA(cudaFuncSetAttribute(k_fwd_diag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    kSolveDiagSmem * static_cast<int>(sizeof(cx<R>))));
     APHI_CUDA(cudaFuncSetAttribute(k_bwd_diag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -444,6 +454,10 @@ aphi_factor* factor_create(aphi_analysis* an, int precision, int batch) {
         f->use_tc = !(no_tc && no_tc[0] == '1');
         const char* split = std::getenv("APHI_TC_SPLIT");
         f->tc_split = split && split[0] == '2' ? 2 : 3;
+        const char* stages = std::getenv("APHI_TC_STAGES");
+        f->tc_stages = stages && stages[0] == '3' ? 3 : 2;
+        const char* group = std::getenv("APHI_TC_GROUP");
+        f->tc_group = group && group[0] == '4' ? 4 : 2;
         const Symbolic& S = an->S;
         APHI_CUDA(cudaMalloc(&f->L, static_cast<size_t>(std::max<long long>(S.stored, 1)) * batch * f->elem));
         f->dscale = dalloc<double>(static_cast<size_t>(S.n) * batch);

@@ -37,6 +37,8 @@ struct aphi_factor {
     bool factored = false;
     bool use_tc = true;         // FP32: tensor-core updates (APHI_NO_TC=1 selects the SIMT kernels)
     int tc_split = 3;           // FP32 tensor-core updates: TF32 pieces per operand (3, or 2: hh + hl + lh)
+    int tc_stages = 2;          // split 2: split-operand stages in flight (2 or 3; APHI_TC_STAGES)
+    int tc_group = 2;           // split 2: stages per fresh main accumulator (2 or 4; APHI_TC_GROUP)
     int* err = nullptr;         // device error word (bounded waits)
     int* kmax = nullptr;        // capacity: the column where each entry's factorization stopped
     // Per-kind launch timing (aphi_factor_profile).

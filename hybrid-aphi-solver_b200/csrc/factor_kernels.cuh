@@ -603,7 +603,7 @@ __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long ite
 // one panel (128) or a group of them (up to kWidePair). Split: TF32 pieces per
 // operand (3, or 2 for the cheaper hh + hl + lh products). A bounded wait that
 // expires sets err[0] and leaves the tile unchanged; the host reports it.
-template <int Split>
+template <int Split, int Stages = kTcPlaneStages, int Group = kTcGroup>
 __global__ void __launch_bounds__(kTcThreads) k_update_tc(Sched S, long long item0, cx<float>* Lb, cx<float>* CBb,
                                                           long long lstride, long long cbstride, int kcap, int* err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -621,7 +621,7 @@ __global__ void __launch_bounds__(kTcThreads) k_update_tc(Sched S, long long ite
     const float2* dk = reinterpret_cast<const float2*>(Ls + p0 + static_cast<long long>(p0) * m);
     // Read-modify-write of 16 entries of row i: all loads first, so their
     // latencies overlap, then the stores.
-    const bool ok = tc_tile<Split>(smem_raw, P, m, m, K, i0, j0, dk, static_cast<long long>(m) + 1,
+    const bool ok = tc_tile<Split, Stages, Group>(smem_raw, P, m, m, K, i0, j0, dk, static_cast<long long>(m) + 1,
                             [&](int r, int c0, const float(&re)[16], const float(&im)[16]) {
                                 const int i = i0 + r;
                                 if (i >= m) return;

@@ -17,18 +17,27 @@ constexpr int kTcPlaneA = kTcM * kTcK * 4;      // bytes of one A plane in one s
 constexpr int kTcPlaneB = kTcN * kTcK * 4;      // bytes of one B plane in one stage
 // Bytes of one split-operand stage, and the dynamic shared memory of a tile,
 // for a split into `Split` TF32 planes.
+// The two-piece split stacks its B planes (-Bi, Br, Bi per piece) so that
+// the complex product needs two M128 N128 MMAs per kept pair; the
+// three-piece split keeps separate Br, Bi planes and four M128 N64 MMAs (its
+// stacked form would not leave room for two CTAs per SM).
+template <int Split>
+struct TcLayout {
+    static constexpr bool stacked = Split == 2;
+    static constexpr int b_planes = stacked ? 3 : 2;  // B planes per piece
+};
 template <int Split>
 struct TcBytes {
-    static constexpr int stage = 2 * Split * (kTcPlaneA + kTcPlaneB);
+    static constexpr int stage = 2 * Split * kTcPlaneA + TcLayout<Split>::b_planes * Split * kTcPlaneB;
 };
 constexpr int kTcStage = TcBytes<kTcSplit>::stage;
 constexpr int kTcRawA = kTcK * kTcM * 8;        // complex64 A rows of one stage
 constexpr int kTcRawB = kTcK * kTcN * 8;
 constexpr int kTcRawStage = kTcRawA + kTcRawB + kTcK * 8;  // + the stage's pivots
 constexpr int kTcTmemCols = 4 * kTcN;           // Cr, Ci main + Cr, Ci corrections
-template <int Split>
+template <int Split, int Stages = kTcPlaneStages>
 struct TcSmem {
-    static constexpr int bytes = kTcPlaneStages * TcBytes<Split>::stage + kTcRawStages * kTcRawStage + 64;
+    static constexpr int bytes = Stages * TcBytes<Split>::stage + kTcRawStages * kTcRawStage + 64;
 };
 constexpr int kTcSmem = TcSmem<kTcSplit>::bytes;
 

@@ -23,6 +23,12 @@
 // below, accumulate over the whole K in their own TMEM accumulator (Cr, Ci:
 // 2 x 64 columns), where their truncation is negligible.
 //
+// Two-piece split (hi + lo; products hh, hl, lh) uses a stacked B layout:
+// per piece the planes -Bi, Br, Bi lie back to back, so [Br; Bi] and
+// [-Bi; Br] are 128-row operands and each kept pair costs two M128 N128 MMAs
+// ([Cr | Ci] += Ar [Br | Bi]^T + Ai [-Bi | Br]^T) instead of four M128 N64
+// ones: half the MMA instructions and a third less operand traffic.
+//
 // Pipeline: K advances 8 columns per stage. Raw operands (A rows, B rows and
 // the stage's pivots, complex64) are fetched by cp.async into a ring of
 // kTcRawStages buffers, two stages ahead, so no registers hold them in
@@ -71,10 +77,11 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
     return d;                                        // base offset 0, no swizzle
 }
 
-// kind::tf32 instruction descriptor: F32 accumulate, TF32 A and B, K-major.
-__device__ __forceinline__ uint32_t instr_desc(int negate_a) {
+// kind::tf32 instruction descriptor: F32 accumulate, TF32 A and B, K-major,
+// M = kTcM, N = n (a multiple of 16, 16..256).
+__device__ __forceinline__ uint32_t instr_desc(int negate_a, int n = kTcN) {
     return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(negate_a) << 13) |
-           (static_cast<uint32_t>(kTcN >> 3) << 17) | (static_cast<uint32_t>(kTcM >> 4) << 24);
+           (static_cast<uint32_t>(n >> 3) << 17) | (static_cast<uint32_t>(kTcM >> 4) << 24);
 }
 
 __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
@@ -131,8 +138,9 @@ __device__ __forceinline__ void cp_async_wait() {
 // matrix in each of Split planes. Split 3: hi, mid, lo, each exactly a TF32
 // number, hi + mid + lo == v. Split 2: hi and lo = the rounded remainder,
 // hi + lo == v to 2^-22 relative.
-template <int Split>
-__device__ __forceinline__ void split_store4(unsigned char* plane0, int plane_bytes, uint32_t off, const float (&v)[4]) {
+template <int Split, bool Negate = false>
+__device__ __forceinline__ void split_store4(unsigned char* plane0, int plane_bytes, uint32_t off, const float (&v)[4],
+                                             unsigned char* neg0 = nullptr) {
     float4 h, m, l;
     float* hp = &h.x;
     float* mp = &m.x;
@@ -149,6 +157,12 @@ __device__ __forceinline__ void split_store4(unsigned char* plane0, int plane_by
     *reinterpret_cast<float4*>(plane0 + off) = h;
     *reinterpret_cast<float4*>(plane0 + plane_bytes + off) = m;
     if constexpr (Split == 3) *reinterpret_cast<float4*>(plane0 + 2 * plane_bytes + off) = l;
+    if constexpr (Negate) {  // the pieces of -v: the negated pieces of v, exactly
+        *reinterpret_cast<float4*>(neg0 + off) = make_float4(-h.x, -h.y, -h.z, -h.w);
+        *reinterpret_cast<float4*>(neg0 + plane_bytes + off) = make_float4(-m.x, -m.y, -m.z, -m.w);
+        if constexpr (Split == 3)
+            *reinterpret_cast<float4*>(neg0 + 2 * plane_bytes + off) = make_float4(-l.x, -l.y, -l.z, -l.w);
+    }
 }
 
 // Raw stage: A rows [k][128], B rows [k][64], pivots [k] (complex64). Thread
@@ -191,7 +205,7 @@ __device__ __forceinline__ void tc_split(const unsigned char* raw, unsigned char
     const float2* rB = reinterpret_cast<const float2*>(raw + kTcRawA);
     const float2* rD = reinterpret_cast<const float2*>(raw + kTcRawA + kTcRawB);
     unsigned char* A = stage;                                   // Ar pieces, then Ai pieces
-    unsigned char* B = stage + 2 * Split * kTcPlaneA;           // Br pieces, then Bi pieces
+    unsigned char* B = stage + 2 * Split * kTcPlaneA;           // B pieces (layout: TcLayout<Split>)
 #pragma unroll
     for (int g = 0; g < kTcK / 4; ++g) {
         float re[4], im[4];
@@ -214,8 +228,14 @@ __device__ __forceinline__ void tc_split(const unsigned char* raw, unsigned char
         im[q] = v.y;
     }
     const uint32_t o = plane_off(rowb, 4 * qb);
-    split_store4<Split>(B, kTcPlaneB, o, re);
-    split_store4<Split>(B + Split * kTcPlaneB, kTcPlaneB, o, im);
+    if constexpr (TcLayout<Split>::stacked) {
+        // per piece p: [-Bi_p | Br_p | Bi_p], three 64-row planes in a row
+        split_store4<Split>(B + kTcPlaneB, 3 * kTcPlaneB, o, re);
+        split_store4<Split, true>(B + 2 * kTcPlaneB, 3 * kTcPlaneB, o, im, B);
+    } else {
+        split_store4<Split>(B, kTcPlaneB, o, re);
+        split_store4<Split>(B + Split * kTcPlaneB, kTcPlaneB, o, im);
+    }
 }
 
 // The MMAs of one stage: for each kept split pair (pa, pb), the four real
@@ -229,6 +249,24 @@ __device__ __forceinline__ void tc_issue(uint32_t stage_addr, uint32_t tmem, boo
     const uint32_t id_pos = instr_desc(0), id_neg = instr_desc(1);
     constexpr int np = Split == 3 ? 6 : 3;
     const int pa[6] = {0, 0, 1, 0, 2, 1}, pb[6] = {0, 1, 0, 2, 0, 1};
+    if constexpr (TcLayout<Split>::stacked) {
+        // [Cr | Ci] (128 accumulator columns) += Ar [Br | Bi]^T + Ai [-Bi | Br]^T:
+        // two M128 N128 MMAs per kept pair, the B operands 128-row stacks.
+        const uint32_t id128 = instr_desc(0, 2 * kTcN);
+#pragma unroll
+        for (int t = 0; t < np; ++t) {
+            const uint64_t ar = smem_desc(A0 + pa[t] * kTcPlaneA);
+            const uint64_t ai = smem_desc(A0 + (Split + pa[t]) * kTcPlaneA);
+            const uint32_t blk = B0 + pb[t] * 3 * kTcPlaneB;
+            const uint64_t b_ri = smem_desc(blk + kTcPlaneB);   // [Br; Bi]
+            const uint64_t b_nr = smem_desc(blk);               // [-Bi; Br]
+            const uint32_t d = tmem + (t == 0 ? 0 : 2 * kTcN);
+            const bool fresh = t == 0 ? fresh_main : (t == 1 && fresh_corr);
+            mma_tf32(d, ar, b_ri, id128, fresh ? 0u : 1u);
+            mma_tf32(d, ai, b_nr, id128, 1);
+        }
+        return;
+    }
 #pragma unroll
     for (int t = 0; t < np; ++t) {
         const uint64_t ar = smem_desc(A0 + pa[t] * kTcPlaneA);
@@ -272,16 +310,16 @@ __device__ __forceinline__ void tc_drain(uint32_t tmem, float (&sr)[kTcN], float
 // (warp r / 32, lane r % 32). Requires kTcSmem bytes of dynamic shared
 // memory (16-byte aligned). Returns false if a bounded wait expired (the
 // caller records the error).
-template <int Split, class Store>
+template <int Split, int Stages = kTcPlaneStages, int Group = kTcGroup, class Store>
 __device__ bool tc_tile(unsigned char* smem, const float2* P, long long ldp, int rows, int K, int i0, int j0,
                         const float2* dk, long long dstride, Store store) {
     constexpr int kStage = TcBytes<Split>::stage;
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     unsigned char* planes = smem;
-    unsigned char* raws = smem + kTcPlaneStages * kStage;
+    unsigned char* raws = smem + Stages * kStage;
     uint64_t* mbar = reinterpret_cast<uint64_t*>(raws + kTcRawStages * kTcRawStage);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + kTcPlaneStages);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + Stages);
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -289,7 +327,7 @@ __device__ bool tc_tile(unsigned char* smem, const float2* P, long long ldp, int
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        for (int s = 0; s < kTcPlaneStages; ++s)
+        for (int s = 0; s < Stages; ++s)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar + s)));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
@@ -310,7 +348,7 @@ __device__ bool tc_tile(unsigned char* smem, const float2* P, long long ldp, int
     bool ok = true;
     int issued = 0;  // stages whose MMAs were issued and committed
     for (int c = 0; c < nst; ++c) {
-        const int buf = c % kTcPlaneStages;
+        const int buf = c % Stages;
         if (c + 2 < nst)
             tc_fetch(raws + ((c + 2) % kTcRawStages) * kTcRawStage, P, ldp, rows, K, i0, j0, dk, dstride,
                      (c + 2) * kTcK);
@@ -318,8 +356,8 @@ __device__ bool tc_tile(unsigned char* smem, const float2* P, long long ldp, int
         cp_async_wait<2>();  // this thread's copies of stage c have landed
         bool mine = true;
         // The plane buffer's previous MMAs (stage c - 2) must be done.
-        if (c >= kTcPlaneStages)
-            mine = mbar_wait(smem_u32(mbar + buf), ((c - kTcPlaneStages) / kTcPlaneStages) & 1);
+        if (c >= Stages)
+            mine = mbar_wait(smem_u32(mbar + buf), ((c - Stages) / Stages) & 1);
         ok = __syncthreads_and(mine) != 0;  // also: every thread's raw copies of stage c are visible
         if (!ok) break;
         tc_split<Split>(raws + (c % kTcRawStages) * kTcRawStage, planes + buf * kStage);
@@ -328,10 +366,10 @@ __device__ bool tc_tile(unsigned char* smem, const float2* P, long long ldp, int
         // A new group starts: the previous group's main products, complete
         // once stage c - 1's commit has arrived, go to the running sums
         // (after the split, so the split overlaps those MMAs).
-        const bool group_start = c % kTcGroup == 0;
+        const bool group_start = c % Group == 0;
         if (group_start && c > 0) {
             const int p = c - 1;
-            mine = mbar_wait(smem_u32(mbar + p % kTcPlaneStages), (p / kTcPlaneStages) & 1);
+            mine = mbar_wait(smem_u32(mbar + p % Stages), (p / Stages) & 1);
             asm volatile("tcgen05.fence::after_thread_sync;");
             if (mine) tc_drain(tmem, sr, si);
         }
@@ -348,8 +386,8 @@ __device__ bool tc_tile(unsigned char* smem, const float2* P, long long ldp, int
     cp_async_wait<0>();
     // Drain: every committed stage not yet waited for, oldest first.
     bool drained = true;
-    for (int c = (issued > kTcPlaneStages ? issued - kTcPlaneStages : 0); c < issued; ++c)
-        drained = mbar_wait(smem_u32(mbar + c % kTcPlaneStages), (c / kTcPlaneStages) & 1) && drained;
+    for (int c = (issued > Stages ? issued - Stages : 0); c < issued; ++c)
+        drained = mbar_wait(smem_u32(mbar + c % Stages), (c / Stages) & 1) && drained;
     drained = __syncthreads_and(drained) != 0;
     asm volatile("tcgen05.fence::after_thread_sync;");
     ok = ok && drained;

@@ -249,6 +249,30 @@ def test_fp32_factor_with_fp64_refinement(cuda, ref_or_skip):
         assert err <= max(1e-10, 2.0 * err_ref), (omega, err, err_ref, reports[k])
 
 
+def test_overlapped_fp64_entries_equal_sequential(cuda):
+    """The second sweep of a mixed SweepSolver sends the frequencies it learned
+    need FP64 straight to FP64; with overlap they are factorized on a side
+    stream from a second thread while the FP32 entries refine. The answers
+    must be the same bits as the sequential schedule's."""
+    w = ab.Workload.cylinder(16)
+    an = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx))
+    asm = ab.Assembly(ab.workload_arrays(w))
+    om = 2 * np.pi * np.geomspace(50.0, 1.0e6, 8)
+    out = {}
+    for overlap in (False, True):
+        sw = ab.SweepSolver(an, asm, len(om), "mixed", fp64_batch=3, overlap=overlap)
+        sw.solve(om)                       # learns the FP64 threshold
+        x, vals, rhs, reps = sw.solve(om)  # predicted entries go to FP64 directly
+        torch.cuda.synchronize()
+        out[overlap] = (x.clone(), [r["precision"] for r in reps], [r["predicted_fp64"] for r in reps])
+        sw.close()
+    assert any(out[True][2]), "no entry was predicted to need FP64: the test does not exercise the overlap"
+    assert out[True][1] == out[False][1]
+    assert bool((out[True][0] == out[False][0]).all())
+    res = ab.residuals(an, vals, out[True][0], rhs)
+    assert (res[:, 0, 0] <= 1e-12).all()
+
+
 def test_cocg_refinement_converges(cuda):
     """At 50 Hz and 20 kHz on 8^3 the FP32 factor preconditions COCG down to
     relative residual 1e-13, with the residual recomputed from x each step."""
