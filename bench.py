@@ -391,7 +391,10 @@ def run_ours(args):
     launches0 = ab.launch_count()
     # Per-kind device time of the factorizations inside the timed steps: CUDA
     # events around each launch, on the stream the kernels run on.
-    solver.profile(True)
+    # Only the trailing-update kinds are timed (two events per launch): the
+    # roofline needs the dominant kernel's durations, and fewer events
+    # perturb the timed sweep less.
+    solver.profile(True, kinds=("update_wide", "update_tc", "update_panel"))
     step_ms = []
     torch.cuda.nvtx.range_push("timed")   # ncu --nvtx --nvtx-include "timed/" captures exactly these steps
     with Clocks(local) as clk:
@@ -512,11 +515,22 @@ def run_ours(args):
     del fp64
 
     hbm, bf16, bf16s, src = peaks()
+    # DRAM traffic of the dominant kernel per launch of the timed steps: the
+    # per-entry traffic of a one-pass ncu capture of the same kernel on this
+    # mesh (profiles/traffic.json), times the frequencies each of the timed
+    # launches carried (a launch's traffic grows with its entries: each
+    # entry's panels and blocks are separate memory).
     traffic_path = ROOT / "profiles" / "traffic.json"
-    traffic = None
+    traffic, traffic_note = None, None
     if traffic_path.exists():
         t = json.loads(traffic_path.read_text()).get(f"{top['precision']}_{top['kind']}_{args.cells}")
-        traffic = t["bytes_per_launch"] if t else None
+        st = plan_flops[top["precision"]].get(top["kind"])
+        if t and st and top["launches"]:
+            calls = top["launches"] / st[0]
+            per_call = entries[top["precision"]] / calls
+            traffic = t["bytes_per_launch"] / t["batch"] * per_call
+            traffic_note = (f"{t['bytes_per_launch'] / t['batch'] / 1e9:.3f} GB per entry per launch from a capture "
+                            f"at batch {t['batch']} (default schedule), x {per_call:.2f} entries per launch here")
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -550,7 +564,7 @@ def run_ours(args):
                          "frac": top["tflops"] / live_peaks[peak_key],
                          "peak_source": (f"{peak_key}: measured live on this device by aphi_measure_peaks "
                                          f"(MEASURED_PEAKS.json has only HBM and bf16: bf16 {bf16:.0f} TF/s, {src})"),
-                         "traffic": traffic,
+                         "traffic": traffic, "traffic_method": traffic_note,
                          "algorithmic": (f"useful Schur-update flops: {plan_flops[top['precision']][top['kind']][2]:.4e} "
                                          f"per factorization x {entries[top['precision']]} factorizations in the "
                                          f"timed steps"),

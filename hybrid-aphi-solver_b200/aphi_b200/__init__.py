@@ -170,6 +170,7 @@ _SIGS = {
     "aphi_csr_residuals_host": (I, [I, PI, PI, PD, I, PD, PD, PD]),
     "aphi_factor_set_tc_split": (I, [P, I]),
     "aphi_spmv": (I, [P, I, I, P, P, P, P]),
+    "aphi_factor_profile_kinds": (I, [P, C.c_uint]),
     "aphi_selftest_tc_tile_split": (I, [I, I, I, I, I, P, P, P]),
 }
 
@@ -758,9 +759,16 @@ class Factor:
         check(lib().aphi_factor_set_batch(self._h, batch))
         self.batch = batch
 
-    def profile(self, enable: bool = True) -> None:
-        """Per-kind device timing of later factorizations (clears the totals)."""
-        check(lib().aphi_factor_profile(self._h, 1 if enable else 0))
+    def profile(self, enable: bool = True, kinds=None) -> None:
+        """Per-kind device timing of later factorizations (clears the totals);
+        kinds: names of the kinds to time (all when None)."""
+        if enable and kinds:
+            mask = 0
+            for k in kinds:
+                mask |= 1 << Analysis.PLAN_KINDS.index(k)
+            check(lib().aphi_factor_profile_kinds(self._h, mask))
+        else:
+            check(lib().aphi_factor_profile(self._h, 1 if enable else 0))
 
     def profile_read(self) -> dict:
         """{kind: (launches, ms)} accumulated since profile(True)."""
@@ -937,6 +945,7 @@ class SweepSolver:
         self.stall_omega = None      # lowest frequency whose FP32 refinement stalled
         self._factors = {}
         self._profile = False
+        self._profile_kinds = None
         self._prof_done = {}         # precision -> {kind: (launches, ms)} of factors since replaced
         self.factorized = {PREC_FP32: 0, PREC_FP64: 0}   # entries factorized since profile(True)
 
@@ -953,7 +962,7 @@ class SweepSolver:
             if precision == PREC_FP32:
                 f.set_tc_split(self.tc_split)
             if self._profile:
-                f.profile(True)
+                f.profile(True, self._profile_kinds)
             self._factors[precision] = f
         if f.batch != size:
             f.set_batch(size)
@@ -967,13 +976,15 @@ class SweepSolver:
             a = acc.get(k, (0, 0.0))
             acc[k] = (a[0] + n, a[1] + ms)
 
-    def profile(self, enable: bool = True) -> None:
-        """Per-kind device timing of every factorization from now on."""
+    def profile(self, enable: bool = True, kinds=None) -> None:
+        """Per-kind device timing of every factorization from now on (only the
+        named kinds when `kinds` is given)."""
         self._profile = enable
+        self._profile_kinds = kinds
         self._prof_done = {}
         self.factorized = {PREC_FP32: 0, PREC_FP64: 0}
         for f in self._factors.values():
-            f.profile(enable)
+            f.profile(enable, kinds)
 
     def profile_read(self) -> dict:
         """{"fp32" | "fp64": {kind: (launches, ms)}} since profile(True)."""

@@ -85,6 +85,13 @@ int aphi_factor_profile(aphi_factor* f, int enable) {
     });
 }
 
+int aphi_factor_profile_kinds(aphi_factor* f, unsigned mask) {
+    return guard([&] {
+        if (!f) throw Error(APHI_ERR_INVALID, "aphi_factor_profile_kinds: null factor");
+        factor_profile(f, mask != 0, mask);
+    });
+}
+
 int aphi_factor_profile_read(const aphi_factor* f, double* ms, int64_t* launches) {
     return guard([&] {
         if (!f || !ms || !launches) throw Error(APHI_ERR_INVALID, "aphi_factor_profile_read: null argument");

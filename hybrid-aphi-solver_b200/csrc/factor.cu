@@ -260,7 +260,8 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
     const bool prof = f->profile && !sa;
     for (const Launch& l : plan) {
         dim3 grid(l.count, sa && sa->ny > 0 ? sa->ny : f->batch);
-        if (prof) {
+        const bool timed = prof && ((f->prof_mask >> l.kind) & 1u);
+        if (timed) {
             cudaEvent_t e[2];
             APHI_CUDA(cudaEventCreate(&e[0]));
             APHI_CUDA(cudaEventCreate(&e[1]));
@@ -309,7 +310,7 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
                 break;
         }
         APHI_CHECK_LAUNCH();
-        if (prof) APHI_CUDA(cudaEventRecord(fm->prof_events.back(), st));
+        if (timed) APHI_CUDA(cudaEventRecord(fm->prof_events.back(), st));
     }
 }
 
@@ -506,8 +507,9 @@ void factor_set_batch(aphi_factor* f, int batch) {
     f->factored = false;
 }
 
-void factor_profile(aphi_factor* f, bool enable) {
+void factor_profile(aphi_factor* f, bool enable, unsigned mask) {
     f->profile = enable;
+    f->prof_mask = mask;
     for (int k = 0; k < APHI_PLAN_KINDS; ++k) {
         f->prof_ms[k] = 0;
         f->prof_launches[k] = 0;

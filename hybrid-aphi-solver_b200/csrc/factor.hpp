@@ -43,6 +43,7 @@ struct aphi_factor {
     int* kmax = nullptr;        // capacity: the column where each entry's factorization stopped
     // Per-kind launch timing (aphi_factor_profile).
     bool profile = false;
+    unsigned prof_mask = ~0u;  // kinds (bit k: kind k) timed while profiling
     std::vector<cudaEvent_t> prof_events;  // pairs, one per launch of the current factorization
     std::vector<int> prof_kinds;
     double prof_ms[APHI_PLAN_KINDS] = {};
@@ -60,7 +61,7 @@ namespace aphi_b200 {
 
 aphi_factor* factor_create(aphi_analysis* an, int precision, int batch);
 void factor_destroy(aphi_factor* f);
-void factor_profile(aphi_factor* f, bool enable);
+void factor_profile(aphi_factor* f, bool enable, unsigned mask = ~0u);
 void factor_set_batch(aphi_factor* f, int batch);
 int factorize(aphi_factor* f, const double* values_dev, int equil_iters, double pivot_floor,
               aphi_factor_stats* stats, cudaStream_t stream, const double* panels_dev = nullptr);

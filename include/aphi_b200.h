@@ -448,6 +448,10 @@ int aphi_analysis_plan_stats(const aphi_analysis* a, int plan, int64_t* launches
  * runs, not for timed ones. */
 int aphi_factor_profile(aphi_factor* f, int enable);
 int aphi_factor_profile_read(const aphi_factor* f, double* ms, int64_t* launches);
+/* The same, timing only the kinds whose bit is set in mask (bit k: kind k of
+ * aphi_analysis_plan_stats); 0 disables. Fewer events, so a timed run that
+ * needs one kernel's durations perturbs the rest less. */
+int aphi_factor_profile_kinds(aphi_factor* f, unsigned mask);
 
 /* Arithmetic peaks of the current device, measured by short register- or
  * shared-memory-resident loops (2 CTAs per SM, CUDA events): tflops[0] FP64
