@@ -376,7 +376,7 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
 
     solver = ab.SweepSolver(an, asm, args.nfreq, "mixed", fp64_batch=args.fp64_batch, rtol=args.rtol,
-                            tol=args.tol, tc_split=args.tc_split)
+                            tol=args.tol, tc_split=args.tc_split, fp32_batch=args.fp32_batch or None)
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
 
     def sweep():
@@ -598,6 +598,7 @@ def main():
     ap.add_argument("--rtol", type=float, default=1e-14,
                     help="relative-residual target of the refinement (the FP64 direct solve's own level)")
     ap.add_argument("--fp64-batch", type=int, default=8)
+    ap.add_argument("--fp32-batch", type=int, default=0, help="FP32 entries per factorization (0: the whole sweep)")
     ap.add_argument("--tc-split", type=int, default=2, choices=[2, 3],
                     help="TF32 pieces per FP32 operand in the tensor-core update (3: six products, 2: three)")
     ap.add_argument("--fp64-steps", type=int, default=1)

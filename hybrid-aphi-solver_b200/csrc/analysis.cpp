@@ -30,10 +30,14 @@ T* upload(const std::vector<T>& h, long long& bytes) {
 // reads and writes it a quarter as often.
 void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing, std::vector<Launch>& plan) {
     const Symbolic& S = A.S;
-    auto push = [&](int kind, long long first, int kcap = kTcPanel) {
+    auto push = [&](int kind, long long first, int kcap = kTcPanel, int wide = 0) {
         const int count = static_cast<int>(items.size() - first);
-        if (count > 0) plan.push_back({kind, first, count, kcap});
+        if (count > 0) plan.push_back({kind, first, count, kcap, wide});
     };
+    // The FP64 plan (and the SIMT FP32 one) runs the in-panel updates on the
+    // trailing-update kernel as 128 x 64 tiles of K = 32, its columns capped
+    // at the panel's end; the tensor-core plan keeps the 64 x 64 SIMT tiles.
+    const bool panel_wide = trailing == K_UPDATE_WIDE;
     // Panels are grouped for the trailing update: after each panel but a
     // group's last only the group's remaining columns are updated; after its
     // last, the rest of the front with all of the group's panels, so every
@@ -94,10 +98,16 @@ void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing,
                 const int k1 = std::min(w, k0 + kStep);
                 const int m = S.sn_rows[s];
                 const int jend = std::min(w, (k0 / kTcPanel) * kTcPanel + kTcPanel);
-                for (int j = k1; j < jend; j += kTile)
-                    for (int i = j; i < m; i += kTile) items.push_back({s, k0, i, j});
+                if (panel_wide) {
+                    for (int j = k1; j < jend; j += kTcN)
+                        for (int i = k1; i < m; i += kTcM)
+                            if (i + kTcM > j) items.push_back({s, k0, i, j});
+                } else {
+                    for (int j = k1; j < jend; j += kTile)
+                        for (int i = j; i < m; i += kTile) items.push_back({s, k0, i, j});
+                }
             }
-            push(K_UPDATE_PANEL, f0);
+            push(K_UPDATE_PANEL, f0, panel_wide ? kStep : kTcPanel, panel_wide ? 1 : 0);
             // A panel's trailing update follows its last 32-column step. Tiles
             // cover rows and columns [pe, jend) x ..., lower part only.
             // One launch per K cap: a group's last panel applies the whole group.

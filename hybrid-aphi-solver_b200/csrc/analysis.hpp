@@ -36,6 +36,7 @@ struct Launch {
     long long first;  // offset into the item array
     int count;
     int kcap = kTcPanel;  // trailing updates: panel columns applied at once (K = min(kcap, w - p0))
+    int wide = 0;         // K_UPDATE_PANEL: 128 x 64 tiles on the trailing-update kernels (column cap at the panel's end)
 };
 
 struct Item {

@@ -109,8 +109,9 @@ int aphi_analysis_plan_stats(const aphi_analysis* a, int plan, int64_t* launches
                 } else if (l.kind == K_UPDATE_PANEL) {
                     const int kb = std::min(kStep, w - it.a);
                     const int jend = std::min(w, (it.a / kTcPanel) * kTcPanel + kTcPanel);
-                    u = 8.0 * kb * lower(it.b, std::min(m, it.b + kTile), it.c, std::min(jend, it.c + kTile));
-                    e = 8.0 * kb * kTile * kTile;
+                    const int tm = l.wide ? kTcM : kTile, tn = l.wide ? kTcN : kTile;
+                    u = 8.0 * kb * lower(it.b, std::min(m, it.b + tm), it.c, std::min(jend, it.c + tn));
+                    e = 8.0 * kb * tm * tn;
                 }
                 if (useful) useful[l.kind] += u;
                 if (executed) executed[l.kind] += e;

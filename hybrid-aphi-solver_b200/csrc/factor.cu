@@ -276,13 +276,17 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
             case K_DIAG: k_diag_block<R><<<grid, 128, 0, st>>>(S, l.first, L, ls); break;
             case K_TRSM: k_panel_trsm<R><<<grid, kTrsmRows, 0, st>>>(S, l.first, L, ls); break;
             case K_UPDATE_WIDE:
-                if constexpr (sizeof(R) == 8)
-                    k_update_wide_dmma<<<grid, 256, kDmmaSmem, st>>>(S, l.first, L, CB, ls, cs, l.kcap);
-                else
-                    k_update_wide<R><<<grid, 256, wide_smem<R>(), st>>>(S, l.first, L, CB, ls, cs, l.kcap);
-                break;
             case K_UPDATE_PANEL:
-                k_update_panel<R><<<grid, 256, 2 * kStep * kTile * sizeof(cx<R>), st>>>(S, l.first, L, CB, ls, cs);
+                if (l.kind == K_UPDATE_PANEL && !l.wide) {
+                    k_update_panel<R><<<grid, 256, 2 * kStep * kTile * sizeof(cx<R>), st>>>(S, l.first, L, CB, ls, cs);
+                    break;
+                }
+                if constexpr (sizeof(R) == 8)
+                    k_update_wide_dmma<<<grid, 256, kDmmaSmem, st>>>(S, l.first, L, CB, ls, cs, l.kcap,
+                                                                    l.kind == K_UPDATE_PANEL ? 1 : 0);
+                else
+                    k_update_wide<R><<<grid, 256, wide_smem<R>(), st>>>(S, l.first, L, CB, ls, cs, l.kcap,
+                                                                      l.kind == K_UPDATE_PANEL ? 1 : 0);
                 break;
             case K_UPDATE_TC:
                 if constexpr (sizeof(R) == 4) {

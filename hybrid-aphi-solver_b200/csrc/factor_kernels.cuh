@@ -349,7 +349,7 @@ constexpr int wide_smem() {
 
 template <class R>
 __global__ void __launch_bounds__(256) k_update_wide(Sched S, long long item0, cx<R>* Lb, cx<R>* CBb,
-                                                     long long lstride, long long cbstride, int kcap) {
+                                                     long long lstride, long long cbstride, int kcap, int panel) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<R>* As = reinterpret_cast<cx<R>*>(smem_raw);   // [2][KC][128], scaled by D
     cx<R>* Bs = As + 2 * kWideKC * kWideM;            // [2][KC][64]
@@ -427,6 +427,8 @@ __global__ void __launch_bounds__(256) k_update_wide(Sched S, long long item0, c
         if (c + 1 < nc) stash((c + 1) & 1);
         __syncthreads();
     }
+    // In-panel updates (panel != 0) stop at the current panel's last column.
+    const int jcap = panel ? min(w, (p0 / kTcPanel) * kTcPanel + kTcPanel) : m;
     // Read-modify-write, one column block at a time: 8 loads, then 8 stores.
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
@@ -437,7 +439,7 @@ __global__ void __launch_bounds__(256) k_update_wide(Sched S, long long item0, c
         for (int a = 0; a < 8; ++a) {
             const int i = i0 + tx + 16 * a;
             dst[a] = nullptr;
-            if (j < m && i < m && i >= j)
+            if (j < jcap && i < m && i >= j)
                 dst[a] = (j < w) ? Ls + i + static_cast<long long>(j) * m
                                  : CBs + (i - w) + static_cast<long long>(j - w) * cs;
             if (dst[a]) old[a] = *dst[a];
@@ -492,7 +494,7 @@ __device__ __forceinline__ void red_sub(double* p, double v) {
 
 __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long item0, cx<double>* Lb,
                                                           cx<double>* CBb, long long lstride, long long cbstride,
-                                                          int kcap) {
+                                                          int kcap, int panel) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<double>* Ds = reinterpret_cast<cx<double>*>(smem_raw);  // [kWidePair] pivots of the group's panels
     cx<double>* Ring = Ds + kWidePair;                           // [stage][A: KC x ldA | B: KC x ldB]
@@ -580,14 +582,16 @@ __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long ite
         }
     }
     // Thread holds C[g][2 t4 + e] of each 8 x 8 block: rows i0 + 32 wm + 8a + g,
-    // columns j0 + 32 wn + 8b + 2 t4 + e.
+    // columns j0 + 32 wn + 8b + 2 t4 + e. In-panel updates (panel != 0) stop
+    // at the current panel's last column.
+    const int jcap = panel ? min(w, (p0 / kTcPanel) * kTcPanel + kTcPanel) : m;
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
         const int i = i0 + 32 * wm + 8 * a + g;
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const int j = j0 + 32 * wn + 8 * (q >> 1) + 2 * t4 + (q & 1);
-            if (j < m && i < m && i >= j) {
+            if (j < jcap && i < m && i >= j) {
                 cx<double>* dst = (j < w) ? Ls + i + static_cast<long long>(j) * m
                                           : CBs + (i - w) + static_cast<long long>(j - w) * cs;
                 red_sub(&dst->re, cr[a][q >> 1][q & 1]);

@@ -287,7 +287,10 @@ void run_factor_plan(Fronts& F, const std::vector<Launch>& plan, const std::vect
                 case K_UPDATE_PANEL: {
                     const int k0 = it.a, kb = std::min(kStep, w - k0);
                     const int jend = std::min(w, (k0 / kTcPanel) * kTcPanel + kTcPanel);
-                    update_tile(F, it.s, k0, kb, it.b, it.c, kTile, kTile, jend);
+                    if (l.wide)  // on the trailing-update kernel: 128 x 64, K = min(kcap, w - k0)
+                        update_tile(F, it.s, k0, std::min(l.kcap, w - k0), it.b, it.c, kTcM, kTcN, jend);
+                    else
+                        update_tile(F, it.s, k0, kb, it.b, it.c, kTile, kTile, jend);
                     break;
                 }
                 case K_UPDATE_WIDE:
