@@ -71,7 +71,10 @@ def test_plan_stats_account_for_the_same_update_work():
     assert "update_tc" not in simt and "update_wide" not in tc
     assert simt["update_wide"][1] == tc["update_tc"][1]
     assert simt["update_wide"][2] == tc["update_tc"][2]
-    assert simt["update_panel"] == tc["update_panel"]
+    # in-panel updates: 128 x 64 tiles on the trailing kernel in the FP64 plan,
+    # 64 x 64 SIMT tiles in the tensor-core plan -- the same launches and work
+    assert simt["update_panel"][0] == tc["update_panel"][0]
+    assert simt["update_panel"][2] == tc["update_panel"][2]
     for st in (simt, tc):
         for kind, (_, _, useful, executed) in st.items():
             assert useful <= executed
