@@ -563,17 +563,18 @@ class Analysis:
         self.row_ptr, self.col_idx = rp, ci
 
     PLAN_KINDS = ["extend_add", "small_front", "diag_block", "panel_rows", "update_wide", "fwd_gather", "fwd_diag",
-                  "fwd_update", "bwd_update", "bwd_diag", "update_panel", "update_tc"]
+                  "fwd_update", "bwd_update", "bwd_diag", "update_panel", "update_tc", "tc_split"]
 
     def plan_stats(self, plan: int, flops: bool = False) -> dict:
         """{kind: (launches, items)} of launch plan `plan` (0 factorization,
         1 tensor-core factorization, 2 forward solve, 3 backward solve); with
         flops=True, {kind: (launches, items, useful_flops, executed_flops)}
         (flops counted for the update kinds only)."""
-        la = np.zeros(12, np.int64)
-        it = np.zeros(12, np.int64)
-        us = np.zeros(12)
-        ex = np.zeros(12)
+        nk = len(self.PLAN_KINDS)
+        la = np.zeros(nk, np.int64)
+        it = np.zeros(nk, np.int64)
+        us = np.zeros(nk)
+        ex = np.zeros(nk)
         check(lib().aphi_analysis_plan_stats(self._h, plan, la.ctypes.data_as(PI64), it.ctypes.data_as(PI64),
                                              us.ctypes.data_as(PD) if flops else None,
                                              ex.ctypes.data_as(PD) if flops else None))
@@ -772,8 +773,8 @@ class Factor:
 
     def profile_read(self) -> dict:
         """{kind: (launches, ms)} accumulated since profile(True)."""
-        ms = np.zeros(12)
-        la = np.zeros(12, np.int64)
+        ms = np.zeros(len(Analysis.PLAN_KINDS))
+        la = np.zeros(len(Analysis.PLAN_KINDS), np.int64)
         check(lib().aphi_factor_profile_read(self._h, ms.ctypes.data_as(PD), la.ctypes.data_as(PI64)))
         return {k: (int(a), float(t)) for k, a, t in zip(Analysis.PLAN_KINDS, la, ms) if a}
 

@@ -113,6 +113,12 @@ void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing,
             // One launch per K cap: a group's last panel applies the whole group.
             for (int cap_group : {1, 2, 4}) {
                 f0 = static_cast<long long>(items.size());
+                struct SplitFront {
+                    int s, p0, pe, d;
+                };
+                std::vector<SplitFront> split_fronts;
+                long long region = 0;
+                auto count_since = [&](long long first) { return static_cast<long long>(items.size()) - first; };
                 for (int s : large) {
                     const int w = width(s);
                     if (k0 >= w) continue;
@@ -130,10 +136,39 @@ void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing,
                     int jend = m;
                     if (full && !last) jend = g0 + G * kTcPanel;  // the group's remaining columns
                     if (last) p0 = g0;                            // all of the group's panels
+                    const long long before = static_cast<long long>(items.size());
                     for (int j = pe; j < jend; j += kTcN)
                         for (int i = pe; i < m; i += kTcM)
                             if (i + kTcM > j) items.push_back({s, p0, i, j});
+                    if (trailing == K_UPDATE_TC && static_cast<long long>(items.size()) > before) {
+                        // The front's trailing operands (rows [pe, m), the group's K
+                        // columns) split once into TF32 planes: a region of the
+                        // launch's workspace, 10 planes x 8-column stages x R rows
+                        // (R = m - pe rounded up to 128), 32 bytes per row and stage.
+                        const int K = std::min(cap_group * kTcPanel, w - p0);
+                        const long long R = (m - pe + kTcM - 1) / kTcM * kTcM;
+                        const long long units = ((K + kTcK - 1) / kTcK) * kTcPlanes * R / 8;
+                        for (long long t = before; t < static_cast<long long>(items.size()); ++t)
+                            items[t].d = static_cast<int>(region);
+                        split_fronts.push_back({s, p0, pe, static_cast<int>(region)});
+                        region += units;
+                    }
                 }
+                if (trailing == K_UPDATE_TC && count_since(f0) > 0) {
+                    // The split of every front of the launch runs just before it.
+                    std::vector<Item> upd(items.begin() + f0, items.end());
+                    items.resize(f0);
+                    for (const auto& sf : split_fronts) {
+                        const int m = S.sn_rows[sf.s];
+                        for (int r0 = 0; r0 < m - sf.pe; r0 += kTcM) items.push_back({sf.s, sf.p0, r0, sf.d});
+                    }
+                    push(K_TC_SPLIT, f0, cap_group * kTcPanel);
+                    A.tc_ws_units = std::max(A.tc_ws_units, region);
+                    f0 = static_cast<long long>(items.size());
+                    items.insert(items.end(), upd.begin(), upd.end());
+                }
+                split_fronts.clear();
+                region = 0;
                 push(trailing, f0, cap_group * kTcPanel);
             }
         }

@@ -28,7 +28,8 @@ enum Kind : int {
     K_BWD_UPDATE = 8,  // (s, blk, row0, slot): partial L^T x sums over a row chunk
     K_BWD_DIAG = 9,    // (s, blk, first slot, slots): block of the transposed solve
     K_UPDATE_PANEL = 10,  // (s, k0, i0, j0): update tile restricted to the current 128-column panel
-    K_UPDATE_TC = 11,     // (s, p0, i0, j0): tensor-core trailing update by a whole panel
+    K_UPDATE_TC = 11,     // (s, p0, i0, j0, d): tensor-core trailing update by a whole panel
+    K_TC_SPLIT = 12,      // (s, p0, r0, d): a front's trailing operands split into TF32 planes, 128 rows
 };
 
 struct Launch {
@@ -41,6 +42,7 @@ struct Launch {
 
 struct Item {
     int s, a, b, c;
+    int d = 0;  // K_UPDATE_TC / K_TC_SPLIT: the front's plane region, in 256-byte units of an entry's workspace
 };
 
 constexpr int kStep = 32;        // pivot block width of the blocked factorization
@@ -106,6 +108,7 @@ struct aphi_analysis {
     int max_parts = 1;
     long long stat_first = 0;  // items of the statistics pass (s, col0)
     int stat_count = 0;     // partial-sum slots of the largest backward update launch
+    long long tc_ws_units = 0;  // split-operand workspace of the tensor-core plan, per entry (256-byte units)
     long long device_bytes = 0;
     ~aphi_analysis();
 };

@@ -258,7 +258,10 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
     const int smallsm = A->opt.small_front * A->opt.small_front * static_cast<int>(sizeof(cx<R>));
     aphi_factor* fm = const_cast<aphi_factor*>(f);
     const bool prof = f->profile && !sa;
+    const bool presplit = sizeof(R) == 4 && f->tc_split == 2 && f->presplit && f->tcws;
     for (const Launch& l : plan) {
+        // Without pre-split operands the tile splits them itself: no split launch.
+        if (l.kind == K_TC_SPLIT && !presplit) continue;
         dim3 grid(l.count, sa && sa->ny > 0 ? sa->ny : f->batch);
         const bool timed = prof && ((f->prof_mask >> l.kind) & 1u);
         if (timed) {
@@ -288,8 +291,28 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
                     k_update_wide<R><<<grid, 256, wide_smem<R>(), st>>>(S, l.first, L, CB, ls, cs, l.kcap,
                                                                       l.kind == K_UPDATE_PANEL ? 1 : 0);
                 break;
+            case K_TC_SPLIT:
+                if constexpr (sizeof(R) == 4)
+                    k_tc_split<<<grid, kTcThreads, 0, st>>>(S, l.first, L, ls, f->tcws, f->tcws_stride, l.kcap);
+                else
+                    throw Error(APHI_ERR_INVALID, "operand split planned for an FP64 factor");
+                break;
             case K_UPDATE_TC:
                 if constexpr (sizeof(R) == 4) {
+                    if (presplit) {
+                        auto go = [&](auto kern, int smem) {
+                            kern<<<grid, kTcThreads, smem, st>>>(S, l.first, L, CB, ls, cs, l.kcap, f->tcws,
+                                                                 f->tcws_stride, f->err);
+                        };
+                        if (f->pre_stages == 4) {
+                            if (f->tc_group == 4) go(k_update_tc_presplit<4, 4>, TcPreSmem<4>::bytes);
+                            else go(k_update_tc_presplit<2, 4>, TcPreSmem<4>::bytes);
+                        } else {
+                            if (f->tc_group == 4) go(k_update_tc_presplit<4, 3>, TcPreSmem<3>::bytes);
+                            else go(k_update_tc_presplit<2, 3>, TcPreSmem<3>::bytes);
+                        }
+                        break;
+                    }
                     // split 3: two plane stages (3 would leave one CTA per SM);
                     // split 2: plane stages and accumulator group as configured.
                     const int v = f->tc_split == 3 ? 0 : (f->tc_stages == 3 ? 2 : 0) + (f->tc_group == 4 ? 1 : 0) + 1;
@@ -358,6 +381,14 @@ void set_smem_limits(int small_front) {
                                        TcSmem<2, 3>::bytes));
         APHI_CUDA(cudaFuncSetAttribute(k_update_tc<2, 3, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        TcSmem<2, 3>::bytes));
+        APHI_CUDA(cudaFuncSetAttribute(k_update_tc_presplit<2, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TcPreSmem<3>::bytes));
+        APHI_CUDA(cudaFuncSetAttribute(k_update_tc_presplit<4, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TcPreSmem<3>::bytes));
+        APHI_CUDA(cudaFuncSetAttribute(k_update_tc_presplit<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TcPreSmem<4>::bytes));
+        APHI_CUDA(cudaFuncSetAttribute(k_update_tc_presplit<4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TcPreSmem<4>::bytes));
     APHI_CUDA(cudaFuncSetAttribute(k_fwd_diag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    kSolveDiagSmem * static_cast<int>(sizeof(cx<R>))));
     APHI_CUDA(cudaFuncSetAttribute(k_bwd_diag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -463,6 +494,14 @@ aphi_factor* factor_create(aphi_analysis* an, int precision, int batch) {
         f->tc_stages = stages && stages[0] == '3' ? 3 : 2;
         const char* group = std::getenv("APHI_TC_GROUP");
         f->tc_group = group && group[0] == '4' ? 4 : 2;
+        const char* pre = std::getenv("APHI_TC_PRESPLIT");
+        f->presplit = !(pre && pre[0] == '0');
+        const char* pst = std::getenv("APHI_TC_PRESTAGES");
+        f->pre_stages = pst && pst[0] == '4' ? 4 : 3;
+        if (precision == 32 && an->tc_ws_units > 0) {
+            f->tcws_stride = an->tc_ws_units * 256;
+            APHI_CUDA(cudaMalloc(&f->tcws, static_cast<size_t>(f->tcws_stride) * batch));
+        }
         const Symbolic& S = an->S;
         APHI_CUDA(cudaMalloc(&f->L, static_cast<size_t>(std::max<long long>(S.stored, 1)) * batch * f->elem));
         f->dscale = dalloc<double>(static_cast<size_t>(S.n) * batch);
@@ -1307,7 +1346,7 @@ void factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, do
 
 aphi_factor::~aphi_factor() {
     for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
-    void* ptrs[] = {L, dscale, rowmax, stats, dref, y, U, part, ir, red, norms, kr, err, kmax, hvals, hvec};
+    void* ptrs[] = {L, dscale, rowmax, stats, dref, y, U, part, ir, red, norms, kr, err, kmax, hvals, hvec, tcws};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }

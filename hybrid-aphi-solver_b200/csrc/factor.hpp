@@ -39,6 +39,10 @@ struct aphi_factor {
     int tc_split = 3;           // FP32 tensor-core updates: TF32 pieces per operand (3, or 2: hh + hl + lh)
     int tc_stages = 2;          // split 2: split-operand stages in flight (2 or 3; APHI_TC_STAGES)
     int tc_group = 2;           // split 2: stages per fresh main accumulator (2 or 4; APHI_TC_GROUP)
+    bool presplit = true;       // split 2: operands split once per panel group (k_tc_split; APHI_TC_PRESPLIT=0: in the tile)
+    int pre_stages = 3;         // plane buffers of the pre-split tile (APHI_TC_PRESTAGES=4: four)
+    unsigned char* tcws = nullptr;  // the pre-split operand planes, tcws_stride bytes per entry (capacity entries)
+    long long tcws_stride = 0;
     int* err = nullptr;         // device error word (bounded waits)
     int* kmax = nullptr;        // capacity: the column where each entry's factorization stopped
     // Per-kind launch timing (aphi_factor_profile).

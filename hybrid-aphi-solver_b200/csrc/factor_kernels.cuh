@@ -648,6 +648,107 @@ __global__ void __launch_bounds__(kTcThreads) k_update_tc(Sched S, long long ite
     if (!ok && threadIdx.x == 0) atomicExch(err, 1);
 }
 
+// K_TC_SPLIT item (s, p0, r0, d): rows pe + r0 .. pe + r0 + 127 of front s's
+// trailing part (pe = p0 + K, the group's K columns from p0) split into the
+// pre-split tile's planes, stage by stage: A = L D (the pivots on the panel
+// diagonal, the same product tc_split forms) and B = L, each as hi + lo TF32
+// pieces (hi = round(x), lo = round(x - hi)); B also as -Bi. Plane q of stage
+// c starts at region + (c * kTcPlanes + q) * (R / 8) * 256 and holds the rows in
+// the canonical K-major core-matrix layout; rows past the front and columns
+// past K are zeros. One thread per row.
+__global__ void __launch_bounds__(kTcThreads) k_tc_split(Sched S, long long item0, const cx<float>* Lb,
+                                                         long long lstride, unsigned char* ws, long long ws_stride,
+                                                         int kcap) {
+    const Item it = S.items[item0 + blockIdx.x];
+    const int s = it.s, p0 = it.a, r0 = it.b;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int K = min(kcap, w - p0), pe = p0 + K;
+    const int R = (m - pe + kTcM - 1) / kTcM * kTcM;
+    const int nst = (K + kTcK - 1) / kTcK;
+    const long long plane = static_cast<long long>(R / 8) * 256;
+    unsigned char* region = ws + ws_stride * blockIdx.y + static_cast<long long>(it.d) * 256;
+    const cx<float>* P = Lb + lstride * blockIdx.y + S.loff[s];
+    const int r = r0 + threadIdx.x;  // row within the trailing part
+    const int row = pe + r;
+    const bool in = row < m;
+    const uint32_t o = (r >> 3) * 256 + (r & 7) * 16;
+    for (int c = 0; c < nst; ++c) {
+        unsigned char* st = region + static_cast<long long>(c) * kTcPlanes * plane;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            float ar[4], ai[4], br[4], bi[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int k = kTcK * c + 4 * h + q;
+                ar[q] = ai[q] = br[q] = bi[q] = 0.f;
+                if (in && k < K) {
+                    const int col = p0 + k;
+                    const cx<float> v = P[row + static_cast<long long>(col) * m];
+                    const cx<float> d = P[col + static_cast<long long>(col) * m];
+                    ar[q] = v.re * d.re - v.im * d.im;
+                    ai[q] = v.re * d.im + v.im * d.re;
+                    br[q] = v.re;
+                    bi[q] = v.im;
+                }
+            }
+            const uint32_t off = o + h * 128;
+            // A: re hi, re lo, im hi, im lo; B per piece: -Bi, Br, Bi
+            split_store4<2>(st, static_cast<int>(plane), off, ar);
+            split_store4<2>(st + 2 * plane, static_cast<int>(plane), off, ai);
+            split_store4<2>(st + 5 * plane, static_cast<int>(3 * plane), off, br);
+            split_store4<2, true>(st + 6 * plane, static_cast<int>(3 * plane), off, bi, st + 4 * plane);
+        }
+    }
+}
+
+// The tensor-core trailing update on pre-split operands (K_UPDATE_TC with
+// the two-piece split): item (s, p0, i0, j0, d), the front's planes in the
+// workspace region d written by the launch's k_tc_split. Same tile and
+// epilogue as k_update_tc.
+template <int Group, int Stages>
+__global__ void __launch_bounds__(kTcThreads) k_update_tc_presplit(Sched S, long long item0, cx<float>* Lb,
+                                                                   cx<float>* CBb, long long lstride,
+                                                                   long long cbstride, int kcap,
+                                                                   const unsigned char* ws, long long ws_stride,
+                                                                   int* err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Item it = S.items[item0 + blockIdx.x];
+    const int s = it.s, p0 = it.a, i0 = it.b, j0 = it.c;
+    cx<float>* L = Lb + lstride * blockIdx.y;
+    cx<float>* CB = CBb + cbstride * blockIdx.y;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int cs = m - w;
+    const int K = min(kcap, w - p0), pe = p0 + K;
+    const int R = (m - pe + kTcM - 1) / kTcM * kTcM;
+    const int nst = (K + kTcK - 1) / kTcK;
+    cx<float>* Ls = L + S.loff[s];
+    cx<float>* CBs = CB + (cs > 0 ? S.cboff[s] : 0);
+    const unsigned char* region = ws + ws_stride * blockIdx.y + static_cast<long long>(it.d) * 256;
+    const bool ok = tc_tile_presplit<Group, Stages>(smem_raw, region, R, nst, (i0 - pe) / 8, (j0 - pe) / 8,
+                                            [&](int r, int c0, const float(&re)[16], const float(&im)[16]) {
+                                                const int i = i0 + r;
+                                                if (i >= m) return;
+                                                float2* dst[16];
+                                                float2 old[16];
+#pragma unroll
+                                                for (int c = 0; c < 16; ++c) {
+                                                    const int j = j0 + c0 + c;
+                                                    dst[c] = nullptr;
+                                                    if (j < m && i >= j)
+                                                        dst[c] = reinterpret_cast<float2*>(
+                                                            (j < w) ? Ls + i + static_cast<long long>(j) * m
+                                                                    : CBs + (i - w) + static_cast<long long>(j - w) * cs);
+                                                    if (dst[c]) old[c] = *dst[c];
+                                                }
+#pragma unroll
+                                                for (int c = 0; c < 16; ++c)
+                                                    if (dst[c]) *dst[c] = make_float2(old[c].x - re[c], old[c].y - im[c]);
+                                            });
+    if (!ok && threadIdx.x == 0) atomicExch(err, 1);
+}
+
 // ---------------------------------------------------------------- solves
 // y, U: per batch entry, nrhs vectors of length n (post-ordered numbering) and
 // upool (update vectors, one segment of m - w entries per supernode). A

@@ -13,6 +13,7 @@ constexpr int kTcGroup = 2;      // stages per fresh main accumulator (then drai
 constexpr int kTcSplit = 3;      // default: x = hi + mid + lo, each TF32 (2: x ~ hi + lo)
 constexpr int kTcPanel = 128;    // panel width whose trailing update goes to the tensor cores
 constexpr int kTcThreads = 128;
+constexpr int kTcPlanes = 10;    // pre-split operand planes per stage: A re/im x hi/lo, B (-Bi, Br, Bi) x hi/lo
 constexpr int kTcPlaneA = kTcM * kTcK * 4;      // bytes of one A plane in one stage
 constexpr int kTcPlaneB = kTcN * kTcK * 4;      // bytes of one B plane in one stage
 // Bytes of one split-operand stage, and the dynamic shared memory of a tile,

@@ -418,3 +418,172 @@ __device__ bool tc_tile(unsigned char* smem, const float2* P, long long ldp, int
 }
 
 }  // namespace aphi_b200
+
+// ---------------------------------------------------------------- pre-split operands
+// The two-piece tile with its operands split once per panel group instead of
+// once per tile: k_tc_split writes each front's trailing rows as the tile's
+// canonical planes (A = L D and B = L, hi and lo pieces, the stacked B form),
+// stage by stage, into a workspace region; the tile then only moves bytes
+// and issues MMAs. One thread stages each 8-column stage of the tile with ten
+// bulk asynchronous copies (cp.async.bulk, the copy engine, no threads moving
+// data) into one of kTcPreStages plane buffers, each completing on the
+// buffer's mbarrier by transaction count; the same thread issues the stage's
+// six MMAs once the buffer is full and commits them to the buffer's "empty"
+// mbarrier, which gates the buffer's next refill. All threads drain the main
+// accumulator every Group stages, as in tc_tile. Every wait is bounded.
+namespace aphi_b200 {
+
+// Dynamic shared memory of the pre-split tile with `Stages` plane buffers
+// (three fit two CTAs per SM comfortably, four just).
+template <int Stages>
+struct TcPreSmem {
+    static constexpr int bytes = Stages * TcBytes<2>::stage + 2 * Stages * 8 + 64;
+};
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(mbar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+// region: the front's planes for this entry (stage c, plane q at
+// region + (c * kTcPlanes + q) * (R / 8) * 256); R: the front's padded
+// trailing rows; nst: stages; ia, jb: the tile's first A and B row groups
+// (8 rows) within the region. Same result contract as tc_tile.
+template <int Group, int Stages, class Store>
+__device__ bool tc_tile_presplit(unsigned char* smem, const unsigned char* region, int R, int nst, int ia, int jb,
+                                 Store store) {
+    constexpr int P = Stages;
+    constexpr int kStage = TcBytes<2>::stage;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    unsigned char* planes = smem;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + P * kStage);
+    uint64_t* empty = full + P;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(empty + P);
+    volatile int* state = reinterpret_cast<volatile int*>(tmem_slot + 1);  // [0] failed, [1] stages committed, [2] stages loaded
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTcTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        for (int b = 0; b < P; ++b) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(full + b)));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(empty + b)));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;");
+        state[0] = 0;
+        state[1] = 0;
+        state[2] = 0;
+    }
+    const long long plane = static_cast<long long>(R / 8) * 256;  // bytes of one plane of one stage
+    auto load_stage = [&](int c) {                                 // thread 0
+        const int b = c % P;
+        const uint32_t dst = smem_u32(planes + b * kStage);
+        const uint32_t fb = smem_u32(full + b);
+        mbar_expect_tx(fb, kStage);
+        const unsigned char* st = region + static_cast<long long>(c) * kTcPlanes * plane;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) bulk_g2s(dst + q * kTcPlaneA, st + q * plane + ia * 256LL, kTcPlaneA, fb);
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+            bulk_g2s(dst + 4 * kTcPlaneA + q * kTcPlaneB, st + (4 + q) * plane + jb * 256LL, kTcPlaneB, fb);
+    };
+    __syncthreads();
+    if (tid == 0) {
+        const int pre = min(P - 1, nst);
+        for (int c = 0; c < pre; ++c) load_stage(c);
+        state[2] = pre;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = *tmem_slot;
+
+    float sr[kTcN], si[kTcN];
+#pragma unroll
+    for (int c = 0; c < kTcN; ++c) sr[c] = si[c] = 0.f;
+    bool ok = true;
+    for (int s = 0; s < nst; ++s) {
+        const int b = s % P;
+        const bool group_start = s % Group == 0;
+        if (group_start && s > 0) {
+            // The previous group's main products are complete once stage s - 1's
+            // commit has arrived: into the running sums before stage s
+            // restarts the main accumulator.
+            const int p = s - 1;
+            bool mine = !state[0] && mbar_wait(smem_u32(empty + p % P), (p / P) & 1);
+            mine = __all_sync(0xffffffffu, mine);  // the TMEM loads are warp-wide
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            if (mine) tc_drain(tmem, sr, si);
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            ok = __syncthreads_and(mine) != 0;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            if (!ok) break;
+        }
+        if (tid == 0 && !state[0]) {
+            bool good = mbar_wait(smem_u32(full + b), (s / P) & 1);
+            if (good) {
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                tc_issue<2>(smem_u32(planes + b * kStage), tmem, group_start, s == 0);
+                mma_commit(smem_u32(empty + b));
+                state[1] = s + 1;
+                const int t = s + P - 1;
+                if (t < nst) {
+                    // buffer t % P was stage s - 1's: refill once its MMAs are done
+                    if (s >= 1) good = mbar_wait(smem_u32(empty + (s - 1) % P), ((s - 1) / P) & 1);
+                    if (good) {
+                        load_stage(t);
+                        state[2] = t + 1;
+                    }
+                }
+            }
+            if (!good) state[0] = 1;
+        }
+    }
+    __syncthreads();
+    const int committed = state[1], loaded = state[2];
+    ok = ok && !state[0];
+    // Drain: the last committed stage's MMAs (all earlier ones complete before
+    // it), and any copies issued but never consumed (only after a failure).
+    bool drained = true;
+    if (committed > 0)
+        drained = mbar_wait(smem_u32(empty + (committed - 1) % P), ((committed - 1) / P) & 1);
+    if (tid == 0)
+        for (int c = committed; c < loaded; ++c) drained = mbar_wait(smem_u32(full + c % P), (c / P) & 1) && drained;
+    drained = __syncthreads_and(drained) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    ok = ok && drained && committed == nst;
+    if (ok) {
+        tc_drain(tmem, sr, si);  // the last group
+        const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
+        const int r = warp * 32 + lane;
+#pragma unroll
+        for (int c0 = 0; c0 < kTcN; c0 += 16) {
+            uint32_t cr[16], ci[16];
+            tmem_ld16(tmem + lane_base + 2 * kTcN + c0, cr);
+            tmem_ld16(tmem + lane_base + 3 * kTcN + c0, ci);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            float re[16], im[16];
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+                re[c] = sr[c0 + c] + __uint_as_float(cr[c]);
+                im[c] = si[c0 + c] + __uint_as_float(ci[c]);
+            }
+            store(r, c0, re, im);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols));
+    return ok;
+}
+
+}  // namespace aphi_b200

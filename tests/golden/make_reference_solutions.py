@@ -1,7 +1,9 @@
-"""Writes the reference's own solutions of the benchmarked cylinder sweep.
+"""Writes the reference's own solutions of the benchmarked cylinder sweep
+(and of the torus sweep of config 5).
 
     make -C oracle ref REF=<reference tree>
     python tests/golden/make_reference_solutions.py [--cells 24 32] [--jobs 6]
+    python tests/golden/make_reference_solutions.py --mesh torus --cells 24 32
 
 For each mesh (the Kuhn cylinder-in-box at 24^3 and 32^3 cells, reduced
 A-Phi, row-scaled, AMD) and each chosen member of the 16-frequency sweep
@@ -12,7 +14,9 @@ the reference's own pipeline runs through oracle/_ref/libaphi_ref.so
 with 10 Ruiz iterations. One process per (mesh, frequency); a 32^3 solve takes
 about 35 minutes of one core and 6.5 GB of host memory.
 
-Each fixture `reference_cylinder<cells>.npz` holds:
+The torus (the copper torus with its 1 A internal cut port, reduced A-Phi,
+row-scaled, AMD) uses members 0, 4 and 7 of its 8-point sweep (50 Hz .. 10
+kHz). Each fixture `reference_<mesh><cells>.npz` holds:
   omegas, sweep_index          the frequencies (rad/s) and their sweep index
   x_shuffled                   the reference's solutions, complex128 [f, n],
                                stored byte-shuffled (all first bytes of every
@@ -40,6 +44,8 @@ HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parent))
 
 SWEEP_INDEX = (0, 8, 15)
+# The torus (config 5): 8 log-spaced frequencies 50 Hz .. 10 kHz, members 0, 4, 7.
+TORUS_INDEX = (0, 4, 7)
 REPORT_KEYS = ("ok", "backward_error", "residual", "equilibration_min", "equilibration_max",
                "smallest_pivot", "largest_pivot", "largest_multiplier", "factor_nnz", "columns_done",
                "analyze_ms", "factorize_ms", "solve_ms")
@@ -47,6 +53,10 @@ REPORT_KEYS = ("ok", "backward_error", "residual", "equilibration_min", "equilib
 
 def sweep_omegas(nfreq=16, f_lo=50.0, f_hi=1.0e6):
     return 2 * np.pi * np.geomspace(f_lo, f_hi, nfreq)
+
+
+def torus_omegas():
+    return sweep_omegas(8, 50.0, 1.0e4)
 
 
 def sha(a) -> str:
@@ -59,17 +69,17 @@ def shuffle_bytes(x: np.ndarray) -> np.ndarray:
 
 
 def solve_one(task):
-    cells, k = task
+    mesh, cells, k = task
     import refbridge as rb
     t0 = time.time()
-    r = rb.RefProblem.cylinder(cells)
+    r = rb.RefProblem.cylinder(cells) if mesh == "cylinder" else rb.RefProblem.torus(cells)
     rp, ci = r.pattern()
     an = r.analysis()
-    om = float(sweep_omegas()[k])
+    om = float((sweep_omegas() if mesh == "cylinder" else torus_omegas())[k])
     v, b = r.refill(om)
     x, rep = r.solve_symmetric(b)
-    print(f"cells {cells} k {k}: {time.time() - t0:.0f} s, residual {rep['residual']:.2e}", flush=True)
-    return dict(cells=cells, k=k, omega=om, x=x, report=[rep[key] for key in REPORT_KEYS],
+    print(f"{mesh} {cells} k {k}: {time.time() - t0:.0f} s, residual {rep['residual']:.2e}", flush=True)
+    return dict(mesh=mesh, cells=cells, k=k, omega=om, x=x, report=[rep[key] for key in REPORT_KEYS],
                 sha_perm=sha(an["perm"]), sha_pattern=sha(np.concatenate([rp, ci])),
                 sha_values=sha(v), sha_rhs=sha(b), n=r.n, nnz=r.nnz, nnz_l=r.nnz_l)
 
@@ -77,12 +87,14 @@ def solve_one(task):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cells", type=int, nargs="+", default=[24, 32])
+    ap.add_argument("--mesh", default="cylinder", choices=["cylinder", "torus"])
     ap.add_argument("--jobs", type=int, default=6)
     args = ap.parse_args()
     import refbridge as rb
     if not rb.available():
         sys.exit("oracle/_ref/libaphi_ref.so is missing: run `make -C oracle ref REF=<reference tree>`")
-    tasks = [(c, k) for c in sorted(args.cells, reverse=True) for k in SWEEP_INDEX]
+    index = SWEEP_INDEX if args.mesh == "cylinder" else TORUS_INDEX
+    tasks = [(args.mesh, c, k) for c in sorted(args.cells, reverse=True) for k in index]
     with mp.get_context("spawn").Pool(min(args.jobs, len(tasks))) as pool:
         results = pool.map(solve_one, tasks, chunksize=1)
     for cells in args.cells:
@@ -97,7 +109,7 @@ def main():
                    sha_values=np.array([r["sha_values"] for r in rs]),
                    sha_rhs=np.array([r["sha_rhs"] for r in rs]),
                    n=np.array(rs[0]["n"]), nnz=np.array(rs[0]["nnz"]), nnz_l=np.array(rs[0]["nnz_l"]))
-        path = HERE / f"reference_cylinder{cells}.npz"
+        path = HERE / f"reference_{args.mesh}{cells}.npz"
         np.savez_compressed(path, **out)
         print(path.name, path.stat().st_size, "bytes")
 

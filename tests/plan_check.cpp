@@ -266,14 +266,29 @@ void update_tile(Fronts& F, int s, int c, int K, int i0, int j0, int tm, int tn,
     }
 }
 
+// The region a K_TC_SPLIT item writes (128 rows of every stage's ten planes)
+// lies inside the per-entry workspace, and the launch's regions are disjoint
+// per front (the items of one front share a region, distinct row blocks).
+long long g_tc_ws_units = 0;
+void tc_split_region(Fronts& F, const Launch& l, const Item& it, int w) {
+    const int m = F.rows(it.s);
+    const int K = std::min(l.kcap, w - it.a), pe = it.a + K;
+    const long long R = (m - pe + kTcM - 1) / kTcM * kTcM;
+    const long long units = ((K + kTcK - 1) / kTcK) * kTcPlanes * R / 8;
+    if (it.d < 0 || it.d + units > g_tc_ws_units || it.b < 0 || it.b >= R) {
+        ++F.ck.bounds;
+        F.ck.report("tc split region outside the workspace", "d", it.d);
+    }
+}
+
 void run_factor_plan(Fronts& F, const std::vector<Launch>& plan, const std::vector<Item>& items) {
     static const char* names[] = {"extend_add", "small", "diag", "trsm", "update_wide", "", "", "", "", "",
-                                  "update_panel", "update_tc"};
+                                  "update_panel", "update_tc", "tc_split"};
     Checker& ck = F.ck;
     for (const Launch& l : plan) {
         ++ck.launch;
         ++ck.launches;
-        ck.kind = l.kind >= 0 && l.kind < 12 ? names[l.kind] : "?";
+        ck.kind = l.kind >= 0 && l.kind < 13 ? names[l.kind] : "?";
         for (int q = 0; q < l.count; ++q) {
             ck.item = q;
             ++ck.items;
@@ -299,6 +314,12 @@ void run_factor_plan(Fronts& F, const std::vector<Launch>& plan, const std::vect
                     update_tile(F, it.s, it.a, K, it.b, it.c, kTcM, kTcN, F.rows(it.s));
                     break;
                 }
+                case K_TC_SPLIT:
+                    // A copy of the panel's operands into the split-plane workspace:
+                    // the arithmetic is the tiles' (update_tile). Its region must lie
+                    // inside the analysis's per-entry workspace.
+                    tc_split_region(F, l, it, w);
+                    break;
                 default:
                     ++ck.bounds;
                     ck.report("unexpected kind in a factor plan", "plan", l.kind);
@@ -581,6 +602,7 @@ int check_matrix(int n, const std::vector<int>& rp, const std::vector<int>& ci, 
         std::printf("cb_pool %lld bound %lld ", S.cb_pool, *std::max_element(live.begin(), live.end()));
     }
     int bad = 0;
+    g_tc_ws_units = A->tc_ws_units;
     const std::vector<Launch>* plans[2] = {&A->plan_factor, &A->plan_factor_tc};
     const char* pname[2] = {"dmma", "tc"};
     for (int p = 0; p < 2; ++p) {

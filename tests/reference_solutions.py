@@ -15,15 +15,15 @@ def sha(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
-def path(cells: int) -> Path:
-    return GOLDEN / f"reference_cylinder{cells}.npz"
+def path(cells: int, mesh: str = "cylinder") -> Path:
+    return GOLDEN / f"reference_{mesh}{cells}.npz"
 
 
-def load(cells: int) -> dict | None:
+def load(cells: int, mesh: str = "cylinder") -> dict | None:
     """{omegas, sweep_index, x [f, n] complex128, reports [dict per f],
     sha_perm, sha_pattern, sha_values [f], sha_rhs [f], n, nnz, nnz_l}, or
     None when no fixture exists for this mesh."""
-    p = path(cells)
+    p = path(cells, mesh)
     if not p.exists():
         return None
     z = np.load(p)

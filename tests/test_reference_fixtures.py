@@ -1,4 +1,4 @@
-"""The 24^3 and 32^3 reference fixtures (tests/golden/reference_cylinder*.npz,
+"""The 24^3 and 32^3 reference fixtures (tests/golden/reference_*.npz,
 written by the reference's own pipeline) against the host-side parts of this
 repository, on the CPU: the workload generator and the AMD restatement must
 give the reference's pattern and permutation bit for bit at the benchmarked
@@ -12,11 +12,11 @@ import oraclelib as orc
 import reference_solutions as refsol
 
 
-@pytest.mark.parametrize("cells", [24, 32])
-def test_pattern_permutation_and_oracle_refill_match_the_fixture(cells):
-    fx = refsol.load(cells)
-    assert fx is not None, f"{refsol.path(cells).name} is missing"
-    w = ab.Workload.cylinder(cells)
+@pytest.mark.parametrize("mesh,cells", [("cylinder", 24), ("cylinder", 32), ("torus", 24), ("torus", 32)])
+def test_pattern_permutation_and_oracle_refill_match_the_fixture(mesh, cells):
+    fx = refsol.load(cells, mesh)
+    assert fx is not None, f"{refsol.path(cells, mesh).name} is missing"
+    w = ab.Workload.cylinder(cells) if mesh == "cylinder" else ab.Workload.torus(cells)
     assert w.row_ptr.size - 1 == fx["n"] and w.col_idx.size == fx["nnz"]
     assert refsol.sha(np.concatenate([w.row_ptr, w.col_idx]).astype(np.int32)) == fx["sha_pattern"]
     perm = ab.amd_ordering(w.row_ptr, w.col_idx)
@@ -26,5 +26,6 @@ def test_pattern_permutation_and_oracle_refill_match_the_fixture(cells):
     assert refsol.sha(v) == fx["sha_values"][k] and refsol.sha(b) == fx["sha_rhs"][k]
     # the fixture's own solutions are solutions of those systems
     for j, rep in enumerate(fx["reports"]):
-        assert rep["ok"] == 1 and rep["residual"] < 1e-12
+        # the torus's only source is its 1 A port: no FP64 solve reaches 1e-12 there
+        assert rep["ok"] == 1 and rep["residual"] < (1e-12 if mesh == "cylinder" else 1e-3)
         assert np.isfinite(fx["x"][j]).all() and np.linalg.norm(fx["x"][j]) > 0
