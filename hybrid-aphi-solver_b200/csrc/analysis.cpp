@@ -152,6 +152,8 @@ void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing,
                             items[t].d = static_cast<int>(region);
                         split_fronts.push_back({s, p0, pe, static_cast<int>(region)});
                         region += units;
+                        if (region > 0x7fffffffLL)
+                            throw Error(APHI_ERR_BAD_SHAPE, "pre-split workspace of one launch exceeds 512 GiB");
                     }
                 }
                 if (trailing == K_UPDATE_TC && count_since(f0) > 0) {
@@ -160,7 +162,7 @@ void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing,
                     items.resize(f0);
                     for (const auto& sf : split_fronts) {
                         const int m = S.sn_rows[sf.s];
-                        for (int r0 = 0; r0 < m - sf.pe; r0 += kTcM) items.push_back({sf.s, sf.p0, r0, sf.d});
+                        for (int r0 = 0; r0 < m - sf.pe; r0 += kTcM) items.push_back({sf.s, sf.p0, r0, 0, sf.d});
                     }
                     push(K_TC_SPLIT, f0, cap_group * kTcPanel);
                     A.tc_ws_units = std::max(A.tc_ws_units, region);

@@ -30,6 +30,7 @@
 #include <complex>
 #include <cstdio>
 #include <cstdlib>
+#include <map>
 #include <random>
 #include <stdexcept>
 #include <string>
@@ -266,18 +267,69 @@ void update_tile(Fronts& F, int s, int c, int K, int i0, int j0, int tm, int tn,
     }
 }
 
-// The region a K_TC_SPLIT item writes (128 rows of every stage's ten planes)
-// lies inside the per-entry workspace, and the launch's regions are disjoint
-// per front (the items of one front share a region, distinct row blocks).
+// The pre-split workspace. A K_TC_SPLIT item writes 128 rows of every stage's
+// ten planes of its front's region: the region must lie inside the
+// per-entry workspace, the regions of different fronts in one launch must not
+// overlap, and one front's items must agree on it. The K_UPDATE_TC launch that
+// follows reads, per tile, A rows i0 - pe .. +127 and B rows j0 - pe .. +63 of
+// its front's region: the launch just before it must be a split launch that
+// wrote those rows of that region, for the same panel group.
 long long g_tc_ws_units = 0;
+struct SplitFront {
+    long long d, units;
+    int p0;
+    std::vector<char> rows;  // 128-row blocks written
+};
+std::map<int, SplitFront> g_split;
+int g_split_launch = -1;  // ck.launch of the last split launch
+
 void tc_split_region(Fronts& F, const Launch& l, const Item& it, int w) {
     const int m = F.rows(it.s);
     const int K = std::min(l.kcap, w - it.a), pe = it.a + K;
     const long long R = (m - pe + kTcM - 1) / kTcM * kTcM;
     const long long units = ((K + kTcK - 1) / kTcK) * kTcPlanes * R / 8;
-    if (it.d < 0 || it.d + units > g_tc_ws_units || it.b < 0 || it.b >= R) {
+    if (it.d < 0 || it.d + units > g_tc_ws_units || it.b < 0 || it.b >= R || it.b % kTcM) {
         ++F.ck.bounds;
         F.ck.report("tc split region outside the workspace", "d", it.d);
+        return;
+    }
+    auto found = g_split.find(it.s);
+    if (found == g_split.end()) {
+        for (const auto& kv : g_split)
+            if (it.d < kv.second.d + kv.second.units && kv.second.d < it.d + units) {
+                ++F.ck.ww;
+                F.ck.report("tc split regions of two fronts overlap", "d", it.d);
+            }
+        found = g_split.emplace(it.s, SplitFront{it.d, units, it.a, std::vector<char>(R / kTcM, 0)}).first;
+    } else if (found->second.d != it.d || found->second.p0 != it.a) {
+        ++F.ck.bounds;
+        F.ck.report("tc split items of one front disagree on the region", "d", it.d);
+        return;
+    }
+    char& blk = found->second.rows[it.b / kTcM];
+    if (blk) {
+        ++F.ck.ww;
+        F.ck.report("tc split row block written twice", "row", it.b);
+    }
+    blk = 1;
+}
+
+// A K_UPDATE_TC tile of a plan with split launches reads only planes that the
+// split launch just before it wrote.
+void tc_tile_region(Fronts& F, const Launch& l, const Item& it, int w) {
+    const int K = std::min(l.kcap, w - it.a), pe = it.a + K;
+    const auto found = g_split.find(it.s);
+    const bool fresh = g_split_launch == F.ck.launch - 1;
+    bool ok = fresh && found != g_split.end() && found->second.d == it.d && found->second.p0 == it.a;
+    if (ok) {
+        const std::vector<char>& rows = found->second.rows;
+        const int ia = (it.b - pe) / kTcM, jb = (it.c - pe) / kTcM;
+        ok = it.b >= pe && it.c >= pe && ia < static_cast<int>(rows.size()) && jb < static_cast<int>(rows.size()) &&
+             rows[ia] && rows[jb];
+    }
+    if (!ok) {
+        ++F.ck.rw;
+        F.ck.report("tc tile reads planes its split launch did not write", "row", it.b);
     }
 }
 
@@ -285,10 +337,17 @@ void run_factor_plan(Fronts& F, const std::vector<Launch>& plan, const std::vect
     static const char* names[] = {"extend_add", "small", "diag", "trsm", "update_wide", "", "", "", "", "",
                                   "update_panel", "update_tc", "tc_split"};
     Checker& ck = F.ck;
+    const bool presplit = std::any_of(plan.begin(), plan.end(), [](const Launch& l) { return l.kind == K_TC_SPLIT; });
+    g_split.clear();
+    g_split_launch = -1;
     for (const Launch& l : plan) {
         ++ck.launch;
         ++ck.launches;
         ck.kind = l.kind >= 0 && l.kind < 13 ? names[l.kind] : "?";
+        if (l.kind == K_TC_SPLIT) {
+            g_split.clear();
+            g_split_launch = ck.launch;
+        }
         for (int q = 0; q < l.count; ++q) {
             ck.item = q;
             ++ck.items;
@@ -311,6 +370,7 @@ void run_factor_plan(Fronts& F, const std::vector<Launch>& plan, const std::vect
                 case K_UPDATE_WIDE:
                 case K_UPDATE_TC: {
                     const int K = std::min(l.kcap, w - it.a);
+                    if (l.kind == K_UPDATE_TC && presplit) tc_tile_region(F, l, it, w);
                     update_tile(F, it.s, it.a, K, it.b, it.c, kTcM, kTcN, F.rows(it.s));
                     break;
                 }
