@@ -289,18 +289,24 @@ def test_cocg_refinement_converges(cuda):
 
 def test_factor_profile_counts_every_planned_launch(cuda):
     """aphi_factor_profile: one factorization with timing on records exactly
-    the launches its plan holds, per kind, with positive durations."""
+    the launches its plan holds, per kind, with positive durations. The
+    operand-split launches run only for the two-piece split (the three-piece
+    tile splits its operands itself)."""
     w = ab.Workload.cylinder(10)
     an = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx))
     asm = ab.Assembly(ab.workload_arrays(w))
     vals, _ = asm.refill(2 * np.pi * np.array([50.0, 1e3]))
-    for prec, plan in ((ab.PREC_FP64, 0), (ab.PREC_FP32, 1)):
+    for prec, plan, split in ((ab.PREC_FP64, 0, None), (ab.PREC_FP32, 1, 3), (ab.PREC_FP32, 1, 2)):
         f = ab.Factor(an, precision=prec, batch=2)
+        if split:
+            f.set_tc_split(split)
         f.profile(True)
         assert f.factorize(vals)
         got = f.profile_read()
-        want = an.plan_stats(plan)
-        assert {k: v[0] for k, v in got.items()} == {k: v[0] for k, v in want.items()}
+        want = {k: v[0] for k, v in an.plan_stats(plan).items() if split != 3 or k != "tc_split"}
+        if split == 2:
+            assert want.get("tc_split", 0) > 0
+        assert {k: v[0] for k, v in got.items()} == want
         assert all(ms > 0 for _, ms in got.values())
         f.profile(False)
 
