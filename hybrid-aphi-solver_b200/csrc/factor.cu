@@ -304,13 +304,10 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
                             kern<<<grid, kTcThreads, smem, st>>>(S, l.first, L, CB, ls, cs, l.kcap, f->tcws,
                                                                  f->tcws_stride, f->err);
                         };
-                        if (f->pre_stages == 4) {
-                            if (f->tc_group == 4) go(k_update_tc_presplit<4, 4>, TcPreSmem<4>::bytes);
-                            else go(k_update_tc_presplit<2, 4>, TcPreSmem<4>::bytes);
-                        } else {
-                            if (f->tc_group == 4) go(k_update_tc_presplit<4, 3>, TcPreSmem<3>::bytes);
-                            else go(k_update_tc_presplit<2, 3>, TcPreSmem<3>::bytes);
-                        }
+                        // A 4-stage accumulator group needs 4 plane buffers.
+                        if (f->tc_group == 4) go(k_update_tc_presplit<4, 4>, TcPreSmem<4>::bytes);
+                        else if (f->pre_stages == 4) go(k_update_tc_presplit<2, 4>, TcPreSmem<4>::bytes);
+                        else go(k_update_tc_presplit<2, 3>, TcPreSmem<3>::bytes);
                         break;
                     }
                     // split 3: two plane stages (3 would leave one CTA per SM);
@@ -382,8 +379,6 @@ void set_smem_limits(int small_front) {
         APHI_CUDA(cudaFuncSetAttribute(k_update_tc<2, 3, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        TcSmem<2, 3>::bytes));
         APHI_CUDA(cudaFuncSetAttribute(k_update_tc_presplit<2, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       TcPreSmem<3>::bytes));
-        APHI_CUDA(cudaFuncSetAttribute(k_update_tc_presplit<4, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        TcPreSmem<3>::bytes));
         APHI_CUDA(cudaFuncSetAttribute(k_update_tc_presplit<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        TcPreSmem<4>::bytes));

@@ -652,10 +652,11 @@ __global__ void __launch_bounds__(kTcThreads) k_update_tc(Sched S, long long ite
 // trailing part (pe = p0 + K, the group's K columns from p0) split into the
 // pre-split tile's planes, stage by stage: A = L D (the pivots on the panel
 // diagonal, the same product tc_split forms) and B = L, each as hi + lo TF32
-// pieces (hi = round(x), lo = round(x - hi)); B also as -Bi. Plane q of stage
-// c starts at region + (c * kTcPlanes + q) * (R / 8) * 256 and holds the rows in
-// the canonical K-major core-matrix layout; rows past the front and columns
-// past K are zeros. One thread per row.
+// pieces (hi = round(x), lo = round(x - hi)); B also as -Bi. The region
+// (workspace offset d) holds the A blocks (128 rows) and the B blocks (64
+// rows) in the layout tc_tile_presplit reads (pre_a_off, pre_b_off), each
+// plane in the canonical K-major core-matrix layout; rows past the front and
+// columns past K are zeros. One thread per row.
 __global__ void __launch_bounds__(kTcThreads) k_tc_split(Sched S, long long item0, const cx<float>* Lb,
                                                          long long lstride, unsigned char* ws, long long ws_stride,
                                                          int kcap) {
@@ -666,15 +667,15 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_split(Sched S, long long item
     const int K = min(kcap, w - p0), pe = p0 + K;
     const int R = (m - pe + kTcM - 1) / kTcM * kTcM;
     const int nst = (K + kTcK - 1) / kTcK;
-    const long long plane = static_cast<long long>(R / 8) * 256;
     unsigned char* region = ws + ws_stride * blockIdx.y + static_cast<long long>(it.d) * 256;
     const cx<float>* P = Lb + lstride * blockIdx.y + S.loff[s];
     const int r = r0 + threadIdx.x;  // row within the trailing part
     const int row = pe + r;
     const bool in = row < m;
-    const uint32_t o = (r >> 3) * 256 + (r & 7) * 16;
+    const uint32_t oa = plane_off(r & 127, 0), ob = plane_off(r & 63, 0);
     for (int c = 0; c < nst; ++c) {
-        unsigned char* st = region + static_cast<long long>(c) * kTcPlanes * plane;
+        unsigned char* A = region + pre_a_off(R, nst, r, c);
+        unsigned char* B = region + pre_b_off(R, nst, r, c);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             float ar[4], ai[4], br[4], bi[4];
@@ -692,12 +693,11 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_split(Sched S, long long item
                     bi[q] = v.im;
                 }
             }
-            const uint32_t off = o + h * 128;
             // A: re hi, re lo, im hi, im lo; B per piece: -Bi, Br, Bi
-            split_store4<2>(st, static_cast<int>(plane), off, ar);
-            split_store4<2>(st + 2 * plane, static_cast<int>(plane), off, ai);
-            split_store4<2>(st + 5 * plane, static_cast<int>(3 * plane), off, br);
-            split_store4<2, true>(st + 6 * plane, static_cast<int>(3 * plane), off, bi, st + 4 * plane);
+            split_store4<2>(A, kTcPlaneA, oa + h * 128, ar);
+            split_store4<2>(A + 2 * kTcPlaneA, kTcPlaneA, oa + h * 128, ai);
+            split_store4<2>(B + kTcPlaneB, 3 * kTcPlaneB, ob + h * 128, br);
+            split_store4<2, true>(B + 2 * kTcPlaneB, 3 * kTcPlaneB, ob + h * 128, bi, B);
         }
     }
 }
@@ -726,7 +726,7 @@ __global__ void __launch_bounds__(kTcThreads) k_update_tc_presplit(Sched S, long
     cx<float>* Ls = L + S.loff[s];
     cx<float>* CBs = CB + (cs > 0 ? S.cboff[s] : 0);
     const unsigned char* region = ws + ws_stride * blockIdx.y + static_cast<long long>(it.d) * 256;
-    const bool ok = tc_tile_presplit<Group, Stages>(smem_raw, region, R, nst, (i0 - pe) / 8, (j0 - pe) / 8,
+    const bool ok = tc_tile_presplit<Group, Stages>(smem_raw, region, R, nst, i0 - pe, j0 - pe,
                                             [&](int r, int c0, const float(&re)[16], const float(&im)[16]) {
                                                 const int i = i0 + r;
                                                 if (i >= m) return;

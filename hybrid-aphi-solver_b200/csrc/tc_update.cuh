@@ -97,17 +97,31 @@ __device__ __forceinline__ void mma_commit(uint32_t mbar) {
                  : "memory");
 }
 
+__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t phase) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    return done != 0;
+}
+
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase, long long limit = kTcSpinLimit) {
-    for (long long i = 0; i < limit; ++i) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(mbar), "r"(phase)
-            : "memory");
-        if (done) return true;
+    for (long long i = 0; i < limit; ++i)
+        if (mbar_try(mbar, phase)) return true;
+    return false;
+}
+
+// A bounded wait that also gives up as soon as another thread of the CTA
+// has recorded a failure (*failed != 0): what it waits for may then never
+// come.
+__device__ __forceinline__ bool mbar_wait_live(uint32_t mbar, uint32_t phase, const volatile int* failed) {
+    for (long long i = 0; i < kTcSpinLimit; ++i) {
+        if (mbar_try(mbar, phase)) return true;
+        if (*failed) return false;
     }
     return false;
 }
@@ -422,16 +436,38 @@ __device__ bool tc_tile(unsigned char* smem, const float2* P, long long ldp, int
 // ---------------------------------------------------------------- pre-split operands
 // The two-piece tile with its operands split once per panel group instead of
 // once per tile: k_tc_split writes each front's trailing rows as the tile's
-// canonical planes (A = L D and B = L, hi and lo pieces, the stacked B form),
-// stage by stage, into a workspace region; the tile then only moves bytes
-// and issues MMAs. One thread stages each 8-column stage of the tile with ten
-// bulk asynchronous copies (cp.async.bulk, the copy engine, no threads moving
-// data) into one of kTcPreStages plane buffers, each completing on the
-// buffer's mbarrier by transaction count; the same thread issues the stage's
-// six MMAs once the buffer is full and commits them to the buffer's "empty"
-// mbarrier, which gates the buffer's next refill. All threads drain the main
-// accumulator every Group stages, as in tc_tile. Every wait is bounded.
+// canonical planes (A = L D and B = L, hi and lo pieces, the stacked B form)
+// into a workspace region, laid out so that one stage of one tile's A rows
+// (four 128-row planes, 16 KB) and of its B rows (six 64-row planes, 12 KB)
+// are each one contiguous block:
+//   A part: [128-row block][stage][Ar hi, Ar lo, Ai hi, Ai lo]
+//   B part: [64-row block][stage][-Bi hi, Br hi, Bi hi, -Bi lo, Br lo, Bi lo]
+// (the B part follows the A part). The tile then only moves bytes and issues
+// MMAs, in two roles that run side by side: a producer thread (warp 0, lane
+// 0) stages each 8-column stage with two bulk asynchronous copies
+// (cp.async.bulk, no threads moving data) into one of Stages plane buffers,
+// completing on the buffer's "full" mbarrier by transaction count, as soon as
+// the buffer's previous MMAs are done; an issuer thread (warp 1, lane 0)
+// issues each stage's six MMAs once its buffer is full and commits them to
+// the buffer's "empty" mbarrier. All threads drain the main accumulator every
+// Group stages, as in tc_tile. Every wait is bounded, and gives up early once
+// the other role has failed.
 namespace aphi_b200 {
+
+constexpr int kTcPreA = 2 * 2 * kTcPlaneA;  // one stage of a 128-row A block
+constexpr int kTcPreB = 3 * 2 * kTcPlaneB;  // one stage of a 64-row B block
+static_assert(kTcPreA + kTcPreB == TcBytes<2>::stage, "pre-split stage = the two-piece tile's plane stage");
+
+// Byte offsets, inside a front's region (R padded trailing rows, nst stages),
+// of stage c of the A block holding trailing row r (r / 128) and of the B
+// block holding it (r / 64).
+__device__ __forceinline__ long long pre_a_off(int R, int nst, int r, int c) {
+    (void)R;
+    return (static_cast<long long>(r >> 7) * nst + c) * kTcPreA;
+}
+__device__ __forceinline__ long long pre_b_off(int R, int nst, int r, int c) {
+    return static_cast<long long>(R >> 7) * nst * kTcPreA + (static_cast<long long>(r >> 6) * nst + c) * kTcPreB;
+}
 
 // Dynamic shared memory of the pre-split tile with `Stages` plane buffers
 // (three fit two CTAs per SM comfortably, four just).
@@ -450,15 +486,20 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
 }
 
-// region: the front's planes for this entry (stage c, plane q at
-// region + (c * kTcPlanes + q) * (R / 8) * 256); R: the front's padded
-// trailing rows; nst: stages; ia, jb: the tile's first A and B row groups
-// (8 rows) within the region. Same result contract as tc_tile.
+// region: the front's planes for this entry (layout above); R: the front's
+// padded trailing rows; nst: stages; ra, rb: the tile's first A and B rows
+// within the trailing part (ra a multiple of 128, rb of 64). Same result
+// contract as tc_tile; requires kTcThreads threads.
 template <int Group, int Stages, class Store>
-__device__ bool tc_tile_presplit(unsigned char* smem, const unsigned char* region, int R, int nst, int ia, int jb,
+__device__ bool tc_tile_presplit(unsigned char* smem, const unsigned char* region, int R, int nst, int ra, int rb,
                                  Store store) {
     constexpr int P = Stages;
     constexpr int kStage = TcBytes<2>::stage;
+    constexpr int kProducer = 0, kIssuer = 32;
+    // A group's drain waits for each of its stages' commits in turn; each
+    // buffer then holds at most one commit that no thread has waited for yet,
+    // so a parity wait cannot match a phase one round early.
+    static_assert(Group <= Stages, "an accumulator group must not span more stages than there are buffers");
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     unsigned char* planes = smem;
@@ -482,21 +523,16 @@ __device__ bool tc_tile_presplit(unsigned char* smem, const unsigned char* regio
         state[1] = 0;
         state[2] = 0;
     }
-    const long long plane = static_cast<long long>(R / 8) * 256;  // bytes of one plane of one stage
-    auto load_stage = [&](int c) {                                 // thread 0
+    auto load_stage = [&](int c) {  // producer
         const int b = c % P;
         const uint32_t dst = smem_u32(planes + b * kStage);
         const uint32_t fb = smem_u32(full + b);
         mbar_expect_tx(fb, kStage);
-        const unsigned char* st = region + static_cast<long long>(c) * kTcPlanes * plane;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) bulk_g2s(dst + q * kTcPlaneA, st + q * plane + ia * 256LL, kTcPlaneA, fb);
-#pragma unroll
-        for (int q = 0; q < 6; ++q)
-            bulk_g2s(dst + 4 * kTcPlaneA + q * kTcPlaneB, st + (4 + q) * plane + jb * 256LL, kTcPlaneB, fb);
+        bulk_g2s(dst, region + pre_a_off(R, nst, ra, c), kTcPreA, fb);
+        bulk_g2s(dst + kTcPreA, region + pre_b_off(R, nst, rb, c), kTcPreB, fb);
     };
     __syncthreads();
-    if (tid == 0) {
+    if (tid == kProducer) {
         const int pre = min(P - 1, nst);
         for (int c = 0; c < pre; ++c) load_stage(c);
         state[2] = pre;
@@ -514,11 +550,12 @@ __device__ bool tc_tile_presplit(unsigned char* smem, const unsigned char* regio
         const int b = s % P;
         const bool group_start = s % Group == 0;
         if (group_start && s > 0) {
-            // The previous group's main products are complete once stage s - 1's
-            // commit has arrived: into the running sums before stage s
-            // restarts the main accumulator.
-            const int p = s - 1;
-            bool mine = !state[0] && mbar_wait(smem_u32(empty + p % P), (p / P) & 1);
+            // The previous group's main products are complete once its stages'
+            // commits have arrived (waited for in order, the last being s - 1's):
+            // into the running sums before stage s restarts the main accumulator.
+            bool mine = true;
+            for (int p = s - Group; p < s && mine; ++p)
+                mine = mbar_wait_live(smem_u32(empty + p % P), (p / P) & 1, state);
             mine = __all_sync(0xffffffffu, mine);  // the TMEM loads are warp-wide
             asm volatile("tcgen05.fence::after_thread_sync;");
             if (mine) tc_drain(tmem, sr, si);
@@ -527,24 +564,27 @@ __device__ bool tc_tile_presplit(unsigned char* smem, const unsigned char* regio
             asm volatile("tcgen05.fence::after_thread_sync;");
             if (!ok) break;
         }
-        if (tid == 0 && !state[0]) {
-            bool good = mbar_wait(smem_u32(full + b), (s / P) & 1);
-            if (good) {
+        if (tid == kIssuer && !state[0]) {
+            if (mbar_wait_live(smem_u32(full + b), (s / P) & 1, state)) {
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 tc_issue<2>(smem_u32(planes + b * kStage), tmem, group_start, s == 0);
                 mma_commit(smem_u32(empty + b));
                 state[1] = s + 1;
-                const int t = s + P - 1;
-                if (t < nst) {
-                    // buffer t % P was stage s - 1's: refill once its MMAs are done
-                    if (s >= 1) good = mbar_wait(smem_u32(empty + (s - 1) % P), ((s - 1) / P) & 1);
-                    if (good) {
-                        load_stage(t);
-                        state[2] = t + 1;
-                    }
+            } else {
+                state[0] = 1;
+            }
+        }
+        if (tid == kProducer && !state[0]) {
+            // buffer (s + P - 1) % P was stage s - 1's: refill it once those MMAs are done
+            const int t = s + P - 1;
+            if (t < nst) {
+                if (s == 0 || mbar_wait_live(smem_u32(empty + (s - 1) % P), ((s - 1) / P) & 1, state)) {
+                    load_stage(t);
+                    state[2] = t + 1;
+                } else {
+                    state[0] = 1;
                 }
             }
-            if (!good) state[0] = 1;
         }
     }
     __syncthreads();
@@ -555,7 +595,7 @@ __device__ bool tc_tile_presplit(unsigned char* smem, const unsigned char* regio
     bool drained = true;
     if (committed > 0)
         drained = mbar_wait(smem_u32(empty + (committed - 1) % P), ((committed - 1) / P) & 1);
-    if (tid == 0)
+    if (tid == kProducer)
         for (int c = committed; c < loaded; ++c) drained = mbar_wait(smem_u32(full + c % P), (c / P) & 1) && drained;
     drained = __syncthreads_and(drained) != 0;
     asm volatile("tcgen05.fence::after_thread_sync;");
