@@ -761,8 +761,8 @@ class Factor:
         self.batch = batch
 
     def profile(self, enable: bool = True, kinds=None) -> None:
-        """Per-kind device timing of later factorizations (clears the totals);
-        kinds: names of the kinds to time (all when None)."""
+        """Per-kind device timing of later factorizations and solves (clears
+        the totals); kinds: names of the kinds to time (all when None)."""
         if enable and kinds:
             mask = 0
             for k in kinds:

@@ -180,10 +180,6 @@ void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing,
 // The solve plans and the statistics pass.
 void build_plans(aphi_analysis& A, std::vector<Item>& items) {
     const Symbolic& S = A.S;
-    auto push = [&](std::vector<Launch>& plan, int kind, long long first) {
-        const int count = static_cast<int>(items.size() - first);
-        if (count > 0) plan.push_back({kind, first, count});
-    };
     build_factor_plan(A, items, K_UPDATE_WIDE, A.plan_factor);
     build_factor_plan(A, items, K_UPDATE_TC, A.plan_factor_tc);
     // Statistics pass over the panels: 32 columns per item.
@@ -197,62 +193,85 @@ void build_plans(aphi_analysis& A, std::vector<Item>& items) {
     // Solves. Forward, levels bottom-up: gather, then per 64-column block the
     // triangle and the rows below. Backward, levels top-down, blocks last to
     // first: partial sums over row chunks, then the triangle.
+    //
+    // Two forms of each. The split plans give every triangle a launch of its
+    // own. The fused plans (wide = 1, the ones the solves run) fold each
+    // triangle into the launch before it: the gather's CTA solves its
+    // supernode's first block; of the CTAs updating the rows below block blk
+    // (forward), the last to finish (a per-supernode arrival counter) solves
+    // block blk + 1, whose rows they have just updated; of the CTAs forming
+    // block blk's backward partial sums, the last reduces them and solves
+    // block blk. A backward block with no rows below gets one empty chunk, so
+    // that a CTA exists to solve it. Fused backward items carry the block's
+    // first partial slot in d; the chunk count follows from the shape.
     auto nblocks = [&](int s) { return (S.sn_first[s + 1] - S.sn_first[s] + kSolveBlock - 1) / kSolveBlock; };
-    for (int L = 0; L < S.num_levels; ++L) {
-        const int* lb = S.level_list.data() + S.level_ptr[L];
-        const int* le = S.level_list.data() + S.level_ptr[L + 1];
-        long long f0 = static_cast<long long>(items.size());
-        int maxb = 0;
-        for (const int* p = lb; p < le; ++p) {
-            items.push_back({*p, 0, 0, 0});
-            maxb = std::max(maxb, nblocks(*p));
-        }
-        push(A.plan_fwd, K_FWD_GATHER, f0);
-        for (int blk = 0; blk < maxb; ++blk) {
-            f0 = static_cast<long long>(items.size());
-            for (const int* p = lb; p < le; ++p)
-                if (blk < nblocks(*p)) items.push_back({*p, blk, 0, 0});
-            push(A.plan_fwd, K_FWD_DIAG, f0);
-            f0 = static_cast<long long>(items.size());
+    auto below_of = [&](int s, int blk) { return std::min(S.sn_first[s + 1] - S.sn_first[s], (blk + 1) * kSolveBlock); };
+    auto pushw = [&](std::vector<Launch>& plan, int kind, long long first, int wide) {
+        const int count = static_cast<int>(items.size() - first);
+        if (count > 0) plan.push_back({kind, first, count, kTcPanel, wide});
+    };
+    for (int fused = 0; fused < 2; ++fused) {
+        std::vector<Launch>& fwd = fused ? A.plan_fwd : A.plan_fwd_split;
+        for (int L = 0; L < S.num_levels; ++L) {
+            const int* lb = S.level_list.data() + S.level_ptr[L];
+            const int* le = S.level_list.data() + S.level_ptr[L + 1];
+            long long f0 = static_cast<long long>(items.size());
+            int maxb = 0;
             for (const int* p = lb; p < le; ++p) {
-                const int s = *p;
-                if (blk >= nblocks(s)) continue;
-                const int w = S.sn_first[s + 1] - S.sn_first[s];
-                const int below = std::min(w, (blk + 1) * kSolveBlock);
-                for (int r = below; r < S.sn_rows[s]; r += kSolveRows) items.push_back({s, blk, r, 0});
+                items.push_back({*p, 0, 0, 0});
+                maxb = std::max(maxb, nblocks(*p));
             }
-            push(A.plan_fwd, K_FWD_UPDATE, f0);
+            pushw(fwd, K_FWD_GATHER, f0, fused);
+            for (int blk = 0; blk < maxb; ++blk) {
+                if (!fused) {
+                    f0 = static_cast<long long>(items.size());
+                    for (const int* p = lb; p < le; ++p)
+                        if (blk < nblocks(*p)) items.push_back({*p, blk, 0, 0});
+                    pushw(fwd, K_FWD_DIAG, f0, 0);
+                }
+                f0 = static_cast<long long>(items.size());
+                for (const int* p = lb; p < le; ++p) {
+                    const int s = *p;
+                    if (blk >= nblocks(s)) continue;
+                    for (int r = below_of(s, blk); r < S.sn_rows[s]; r += kSolveRows) items.push_back({s, blk, r, 0});
+                }
+                pushw(fwd, K_FWD_UPDATE, f0, fused);
+            }
         }
     }
     A.max_parts = 1;
-    for (int L = S.num_levels - 1; L >= 0; --L) {
-        const int* lb = S.level_list.data() + S.level_ptr[L];
-        const int* le = S.level_list.data() + S.level_ptr[L + 1];
-        int maxb = 0;
-        for (const int* p = lb; p < le; ++p) maxb = std::max(maxb, nblocks(*p));
-        for (int blk = maxb - 1; blk >= 0; --blk) {
-            long long f0 = static_cast<long long>(items.size());
-            std::vector<std::pair<int, int>> slots;  // per supernode of this launch: first slot, count
-            int slot = 0;
-            for (const int* p = lb; p < le; ++p) {
-                const int s = *p;
-                if (blk >= nblocks(s)) continue;
-                const int w = S.sn_first[s + 1] - S.sn_first[s];
-                const int below = std::min(w, (blk + 1) * kSolveBlock);
-                const int first = slot;
-                for (int r = below; r < S.sn_rows[s]; r += kSolveRows) items.push_back({s, blk, r, slot++});
-                slots.push_back({first, slot - first});
+    for (int fused = 0; fused < 2; ++fused) {
+        std::vector<Launch>& bwd = fused ? A.plan_bwd : A.plan_bwd_split;
+        for (int L = S.num_levels - 1; L >= 0; --L) {
+            const int* lb = S.level_list.data() + S.level_ptr[L];
+            const int* le = S.level_list.data() + S.level_ptr[L + 1];
+            int maxb = 0;
+            for (const int* p = lb; p < le; ++p) maxb = std::max(maxb, nblocks(*p));
+            for (int blk = maxb - 1; blk >= 0; --blk) {
+                long long f0 = static_cast<long long>(items.size());
+                std::vector<std::pair<int, int>> slots;  // per supernode of this launch: first slot, count
+                int slot = 0;
+                for (const int* p = lb; p < le; ++p) {
+                    const int s = *p;
+                    if (blk >= nblocks(s)) continue;
+                    const int first = slot;
+                    for (int r = below_of(s, blk); r < S.sn_rows[s]; r += kSolveRows)
+                        items.push_back({s, blk, r, slot++, first});
+                    if (fused && slot == first) items.push_back({s, blk, S.sn_rows[s], slot++, first});
+                    slots.push_back({first, slot - first});
+                }
+                A.max_parts = std::max(A.max_parts, slot);
+                pushw(bwd, K_BWD_UPDATE, f0, fused);
+                if (fused) continue;
+                f0 = static_cast<long long>(items.size());
+                int q = 0;
+                for (const int* p = lb; p < le; ++p) {
+                    if (blk >= nblocks(*p)) continue;
+                    items.push_back({*p, blk, slots[q].first, slots[q].second});
+                    ++q;
+                }
+                pushw(bwd, K_BWD_DIAG, f0, 0);
             }
-            A.max_parts = std::max(A.max_parts, slot);
-            push(A.plan_bwd, K_BWD_UPDATE, f0);
-            f0 = static_cast<long long>(items.size());
-            int q = 0;
-            for (const int* p = lb; p < le; ++p) {
-                if (blk >= nblocks(*p)) continue;
-                items.push_back({*p, blk, slots[q].first, slots[q].second});
-                ++q;
-            }
-            push(A.plan_bwd, K_BWD_DIAG, f0);
         }
     }
 }

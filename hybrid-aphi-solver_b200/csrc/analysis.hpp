@@ -37,7 +37,8 @@ struct Launch {
     long long first;  // offset into the item array
     int count;
     int kcap = kTcPanel;  // trailing updates: panel columns applied at once (K = min(kcap, w - p0))
-    int wide = 0;         // K_UPDATE_PANEL: 128 x 64 tiles on the trailing-update kernels (column cap at the panel's end)
+    int wide = 0;         // K_UPDATE_PANEL: 128 x 64 tiles on the trailing-update kernels (column cap at the panel's end);
+                          // K_FWD_GATHER / K_FWD_UPDATE / K_BWD_UPDATE: fused with the triangle solve (see build_plans)
 };
 
 struct Item {
@@ -59,7 +60,7 @@ constexpr int kWidePair = kPanelGroup * kTcPanel;  // the most panel columns one
 constexpr int kGroup4Rows = APHI_GROUP4_ROWS;
 constexpr int kEaCols = 32;      // front columns per extend-add item
 constexpr int kSolveBlock = 64;  // columns per triangular-solve block
-constexpr int kSolveRows = 256;  // rows per solve update item
+constexpr int kSolveRows = 64;   // rows per solve update item
 
 struct DeviceSchedule {
     int* first = nullptr;
@@ -92,6 +93,7 @@ struct aphi_analysis {
     aphi_analysis_options opt{};
     aphi_b200::DeviceSchedule d;
     std::vector<aphi_b200::Launch> plan_factor, plan_factor_tc, plan_fwd, plan_bwd;
+    std::vector<aphi_b200::Launch> plan_fwd_split, plan_bwd_split;  // the same solves, triangles as launches of their own
     std::vector<aphi_b200::Item> h_items;
     std::vector<long long> h_uoff;
     std::vector<int> h_row_ptr, h_col_idx;

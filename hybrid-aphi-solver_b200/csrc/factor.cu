@@ -257,8 +257,10 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
     const long long ls = A->S.stored, cs = A->S.cb_pool;
     const int smallsm = A->opt.small_front * A->opt.small_front * static_cast<int>(sizeof(cx<R>));
     aphi_factor* fm = const_cast<aphi_factor*>(f);
-    const bool prof = f->profile && !sa;
+    const bool prof = f->profile;
     const bool presplit = sizeof(R) == 4 && f->tc_split == 2 && f->presplit && f->tcws;
+    const size_t tri_smem = kTriSmem * sizeof(cx<R>);               // forward triangles
+    const size_t bwd_smem = (kTriSmem + kRedSmem) * sizeof(cx<R>);  // backward triangles
     for (const Launch& l : plan) {
         // Without pre-split operands the tile splits them itself: no split launch.
         if (l.kind == K_TC_SPLIT && !presplit) continue;
@@ -323,15 +325,26 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
                 } else
                     throw Error(APHI_ERR_INVALID, "tensor-core update planned for an FP64 factor");
                 break;
-            case K_FWD_GATHER: k_fwd_gather<R><<<grid, 256, 0, st>>>(S, l.first, *sa, y, U); break;
-            case K_FWD_DIAG:
-                k_fwd_diag<R><<<grid, 256, kSolveDiagSmem * sizeof(cx<R>), st>>>(S, l.first, *sa, L, ls, y);
+            case K_FWD_GATHER:
+                if (l.wide)
+                    k_fwd_gather<R, true><<<grid, 256, tri_smem, st>>>(S, l.first, *sa, L, ls, y, U);
+                else
+                    k_fwd_gather<R, false><<<grid, 256, 0, st>>>(S, l.first, *sa, L, ls, y, U);
                 break;
-            case K_FWD_UPDATE: k_fwd_update<R><<<grid, 256, 0, st>>>(S, l.first, *sa, L, ls, y, U); break;
-            case K_BWD_UPDATE: k_bwd_update<R><<<grid, 256, 0, st>>>(S, l.first, *sa, L, ls, y, part); break;
-            case K_BWD_DIAG:
-                k_bwd_diag<R><<<grid, 256, kSolveDiagSmem * sizeof(cx<R>), st>>>(S, l.first, *sa, L, ls, y, part);
+            case K_FWD_DIAG: k_fwd_diag<R><<<grid, 256, tri_smem, st>>>(S, l.first, *sa, L, ls, y); break;
+            case K_FWD_UPDATE:
+                if (l.wide)
+                    k_fwd_update<R, true><<<grid, 256, tri_smem, st>>>(S, l.first, *sa, L, ls, y, U);
+                else
+                    k_fwd_update<R, false><<<grid, 256, 0, st>>>(S, l.first, *sa, L, ls, y, U);
                 break;
+            case K_BWD_UPDATE:
+                if (l.wide)
+                    k_bwd_update<R, true><<<grid, 256, bwd_smem, st>>>(S, l.first, *sa, L, ls, y, part);
+                else
+                    k_bwd_update<R, false><<<grid, 256, 0, st>>>(S, l.first, *sa, L, ls, y, part);
+                break;
+            case K_BWD_DIAG: k_bwd_diag<R><<<grid, 256, bwd_smem, st>>>(S, l.first, *sa, L, ls, y, part); break;
         }
         APHI_CHECK_LAUNCH();
         if (timed) APHI_CUDA(cudaEventRecord(fm->prof_events.back(), st));
@@ -384,10 +397,12 @@ void set_smem_limits(int small_front) {
                                        TcPreSmem<4>::bytes));
         APHI_CUDA(cudaFuncSetAttribute(k_update_tc_presplit<4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        TcPreSmem<4>::bytes));
-    APHI_CUDA(cudaFuncSetAttribute(k_fwd_diag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   kSolveDiagSmem * static_cast<int>(sizeof(cx<R>))));
-    APHI_CUDA(cudaFuncSetAttribute(k_bwd_diag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   kSolveDiagSmem * static_cast<int>(sizeof(cx<R>))));
+    const int tri = kTriSmem * static_cast<int>(sizeof(cx<R>)), bwd = (kTriSmem + kRedSmem) * static_cast<int>(sizeof(cx<R>));
+    APHI_CUDA(cudaFuncSetAttribute(k_fwd_diag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
+    APHI_CUDA(cudaFuncSetAttribute(k_fwd_gather<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
+    APHI_CUDA(cudaFuncSetAttribute(k_fwd_update<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
+    APHI_CUDA(cudaFuncSetAttribute(k_bwd_diag<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd));
+    APHI_CUDA(cudaFuncSetAttribute(k_bwd_update<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd));
     (void)small_front;
     done = true;
 }
@@ -458,13 +473,17 @@ void solve_numeric(aphi_factor* f, int nrhs, const double* b, double* x, cudaStr
     k_permute_in<R><<<g, 256, 0, st>>>(n, nrhs, A->d.orig_of_new, f->dscale, b, y);
     APHI_CHECK_LAUNCH();
     for (int k0 = 0; k0 < nrhs; k0 += 8) {
-        const SolveArgs sa{n, nrhs, k0, std::min(8, nrhs - k0), A->upool, A->max_parts, entries,
-                           entries ? nentries : 0};
-        run_plan<R>(f, A->plan_fwd, st, &sa, y, U, part);
-        run_plan<R>(f, A->plan_bwd, st, &sa, y, U, part);
+        const SolveArgs sa{n,       nrhs, k0, std::min(8, nrhs - k0), A->upool, A->max_parts, entries,
+                           entries ? nentries : 0, f->counters, A->S.ns};
+        run_plan<R>(f, f->solve_split ? A->plan_fwd_split : A->plan_fwd, st, &sa, y, U, part);
+        run_plan<R>(f, f->solve_split ? A->plan_bwd_split : A->plan_bwd, st, &sa, y, U, part);
     }
     k_permute_out<R><<<g, 256, 0, st>>>(n, nrhs, A->d.new_of_orig, f->dscale, y, x);
     APHI_CHECK_LAUNCH();
+    if (f->profile && !f->prof_kinds.empty()) {
+        APHI_CUDA(cudaStreamSynchronize(st));
+        collect_profile(f);
+    }
 }
 
 }  // namespace
@@ -506,6 +525,10 @@ aphi_factor* factor_create(aphi_analysis* an, int precision, int batch) {
         f->err = dalloc<int>(4);
         f->kmax = dalloc<int>(batch);
         APHI_CUDA(cudaMemset(f->err, 0, 4 * sizeof(int)));
+        f->counters = dalloc<int>(static_cast<size_t>(std::max(S.ns, 1)) * batch);
+        APHI_CUDA(cudaMemset(f->counters, 0, sizeof(int) * std::max(S.ns, 1) * batch));
+        const char* split_solve = std::getenv("APHI_SOLVE_SPLIT");
+        f->solve_split = split_solve && split_solve[0] == '1';
         f->host_stats.assign(batch, aphi_factor_stats{});
     } catch (...) {
         delete f;
@@ -1341,7 +1364,8 @@ void factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, do
 
 aphi_factor::~aphi_factor() {
     for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
-    void* ptrs[] = {L, dscale, rowmax, stats, dref, y, U, part, ir, red, norms, kr, err, kmax, hvals, hvec, tcws};
+    void* ptrs[] = {L, dscale, rowmax, stats, dref, y, U, part, ir, red, norms, kr, err, kmax, hvals, hvec, tcws,
+                    counters};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }

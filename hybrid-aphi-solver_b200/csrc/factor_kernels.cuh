@@ -760,7 +760,7 @@ __global__ void __launch_bounds__(kTcThreads) k_update_tc_presplit(Sched S, long
 // Backward (L^T x = D^-1 y), per level top-down, blocks last to first: partial
 // sums of L[rows below, block]^T x over 256-row chunks, then one CTA adds them
 // in chunk order, scales by D^-1 and solves the block's triangle.
-constexpr int kSolveDiagSmem = (kSolveBlock * kSolveBlock + 8 * kSolveBlock);  // complex entries
+
 
 struct SolveArgs {
     int n;
@@ -770,6 +770,8 @@ struct SolveArgs {
     int max_parts;
     const int* entries;  // grid.y -> batch entry (the entries still being solved); null: grid.y is the entry
     int ny;              // grid.y of the solve launches (0: the factor's batch)
+    int* counters;       // fused plans: arrival counters, ns per grid row, zero between launches
+    int ns;              // supernodes
 };
 
 __device__ __forceinline__ int solve_entry(const SolveArgs& a) {
@@ -780,14 +782,141 @@ __device__ __forceinline__ long long vec_at(const SolveArgs& a, int b, int k) {
     return static_cast<long long>(b) * a.nrhs + (a.k0 + k);
 }
 
+// Loads of values that other CTAs of the same launch wrote (through L2, not
+// a possibly stale L1 line).
+__device__ __forceinline__ cx<double> ld_l2(const cx<double>* p) {
+    const double2 v = __ldcg(reinterpret_cast<const double2*>(p));
+    return cx<double>{v.x, v.y};
+}
+__device__ __forceinline__ cx<float> ld_l2(const cx<float>* p) {
+    const float2 v = __ldcg(reinterpret_cast<const float2*>(p));
+    return cx<float>{v.x, v.y};
+}
+
+// The fused solve kernels' hand-over: every CTA working on supernode s in
+// this launch counts itself in, after a fence that publishes its writes; the
+// one that arrives last (count == expected) resets the counter for the next
+// launch and returns true. No CTA waits for another.
+__device__ __forceinline__ bool last_to_arrive(int* counter, int expected) {
+    __shared__ int last;
+    __syncthreads();  // the CTA's writes ordered before thread 0's fence
+    if (threadIdx.x == 0) {
+        __threadfence();  // ... which publishes them before the arrival
+        const int prev = atomicAdd(counter, 1);
+        last = prev == expected - 1;
+        if (last) {
+            *counter = 0;
+            __threadfence();  // the other CTAs' published writes before this CTA reads them
+        }
+    }
+    __syncthreads();
+    return last;
+}
+
+// A triangle's panel entries (jb x jb at P, leading dimension m) towards L2,
+// ahead of the CTA that will stage them: one prefetch per 128-byte line.
 template <class R>
-__global__ void __launch_bounds__(256) k_fwd_gather(Sched S, long long item0, SolveArgs a, cx<R>* yb, cx<R>* Ub) {
+__device__ __forceinline__ void prefetch_triangle(const cx<R>* P, long long m, int jb) {
+    constexpr int kPerLine = 128 / sizeof(cx<R>);
+    const int lines = (jb + kPerLine - 1) / kPerLine;
+    for (int e = threadIdx.x; e < lines * jb; e += blockDim.x) {
+        const int i = (e % lines) * kPerLine, j = e / lines;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(P + i + static_cast<long long>(j) * m));
+    }
+}
+
+__device__ __forceinline__ int solve_nblocks(const Sched& S, int s) {
+    return (S.first[s + 1] - S.first[s] + kSolveBlock - 1) / kSolveBlock;
+}
+
+// Shared memory of the solve kernels that hold a triangle: L_bb with leading
+// dimension kTriLd (65: a lane's column-strided reads of the backward solve
+// fall in distinct banks), and for the backward solve the partial-sum
+// reduction's four sub-sums per (column, rhs).
+constexpr int kTriLd = kSolveBlock + 1;
+constexpr int kTriSmem = kSolveBlock * kTriLd;     // complex entries
+constexpr int kRedSmem = 4 * kSolveBlock * 8;      // complex entries
+
+// L_bb (jb x jb, leading dimension m in the panel) into shared memory T
+// (leading dimension kTriLd, zeros outside the jb x jb block) by
+// asynchronous copies (cp.async, zero-filled where the source size is 0), so
+// the caller's own loads overlap them; the caller waits with
+// triangle_wait() and a __syncthreads() before reading T.
+__device__ __forceinline__ void cp_async_entry(uint32_t dst, const cx<double>* src, bool in) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(in ? 16u : 0u) : "memory");
+}
+__device__ __forceinline__ void cp_async_entry(uint32_t dst, const cx<float>* src, bool in) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(in ? 8u : 0u) : "memory");
+}
+template <class R>
+__device__ __forceinline__ void stage_triangle(cx<R>* T, const cx<R>* P, long long m, int jb) {
+    static_assert(kSolveBlock * kSolveBlock % 256 == 0, "the block splits evenly over 256 threads");
+#pragma unroll 4
+    for (int e = threadIdx.x; e < kSolveBlock * kSolveBlock; e += 256) {
+        const int i = e % kSolveBlock, j = e / kSolveBlock;
+        const bool in = i < jb && j < jb;
+        cp_async_entry(smem_u32(T + i + j * kTriLd), in ? P + i + static_cast<long long>(j) * m : P, in);
+    }
+    cp_async_commit();
+}
+__device__ __forceinline__ void triangle_wait() { cp_async_wait<0>(); }
+
+// Forward triangle of block blk of supernode s: y[blk] = L_bb^-1 y[blk] for
+// the pass's rhs, one warp per rhs, L_bb staged in shared memory (smem:
+// kTriSmem entries). Lane l holds rows l and l + 32 in registers;
+// step j broadcasts y_j from its owner lane and every lane below updates
+// its rows, y_i = y_i - L_ij y_j, in ascending j. Every thread of the CTA
+// calls it (256 threads).
+template <class R>
+__device__ void fwd_triangle(const Sched& S, const SolveArgs& a, int eb, const cx<R>* Lb, long long lstride,
+                             cx<R>* yb, int s, int blk, unsigned char* smem) {
+    static_assert(kSolveBlock == 64, "two rows per lane");
+    cx<R>* T = reinterpret_cast<cx<R>*>(smem);
+    const int j0 = blk * kSolveBlock;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int f = S.first[s];
+    const int jb = min(kSolveBlock, w - j0);
+    stage_triangle(T, Lb + lstride * eb + S.loff[s] + j0 + static_cast<long long>(j0) * m, m, jb);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    cx<R>* y = yb + vec_at(a, eb, warp) * a.n + f + j0;
+    cx<R> y0{0, 0}, y1{0, 0};
+    if (warp < a.nr) {
+        if (lane < jb) y0 = ld_l2(y + lane);
+        if (lane + 32 < jb) y1 = ld_l2(y + lane + 32);
+    }
+    triangle_wait();
+    __syncthreads();
+    if (warp < a.nr) {
+        for (int j = 0; j < jb; ++j) {
+            const cx<R> src = j < 32 ? y0 : y1;
+            cx<R> yj;
+            yj.re = __shfl_sync(0xffffffffu, src.re, j & 31);
+            yj.im = __shfl_sync(0xffffffffu, src.im, j & 31);
+            if (lane > j) y0 = fms(y0, T[lane + j * kTriLd], yj);
+            if (lane + 32 > j && lane + 32 < jb) y1 = fms(y1, T[lane + 32 + j * kTriLd], yj);
+        }
+        if (lane < jb) y[lane] = y0;
+        if (lane + 32 < jb) y[lane + 32] = y1;
+    }
+}
+
+// Item (s): the children's update vectors added into supernode s's front
+// vector (y at its pivot rows, its own update segment U_s below). Fused: the
+// same CTA then solves the supernode's first block (dynamic shared memory
+// kTriSmem entries).
+template <class R, bool Fused>
+__global__ void __launch_bounds__(256) k_fwd_gather(Sched S, long long item0, SolveArgs a, const cx<R>* Lb,
+                                                    long long lstride, cx<R>* yb, cx<R>* Ub) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int eb = solve_entry(a);
     const int s = S.items[item0 + blockIdx.x].s;
     const int w = S.first[s + 1] - S.first[s];
     const int m = S.rows[s];
     const int cs = m - w;
     const int f = S.first[s];
+    if constexpr (Fused)  // the first block's triangle, staged after the gather
+        prefetch_triangle(Lb + lstride * eb + S.loff[s], m, min(kSolveBlock, w));
     for (int k = 0; k < a.nr; ++k) {
         cx<R>* y = yb + vec_at(a, eb, k) * a.n;
         cx<R>* U = Ub + vec_at(a, eb, k) * a.upool;
@@ -807,93 +936,187 @@ __global__ void __launch_bounds__(256) k_fwd_gather(Sched S, long long item0, So
             __syncthreads();
         }
     }
+    if constexpr (Fused) {
+        __threadfence();
+        __syncthreads();
+        if (w > 0) fwd_triangle<R>(S, a, eb, Lb, lstride, yb, s, 0, smem_raw);
+    }
 }
 
-// Item (s, blk): y[blk] = L_bb^-1 y[blk], one warp per rhs.
+// Item (s, blk): y[blk] = L_bb^-1 y[blk] (the split plan's triangle launch).
 template <class R>
 __global__ void __launch_bounds__(256) k_fwd_diag(Sched S, long long item0, SolveArgs a, const cx<R>* Lb,
                                                   long long lstride, cx<R>* yb) {
-    const int eb = solve_entry(a);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cx<R>* T = reinterpret_cast<cx<R>*>(smem_raw);
-    cx<R>(*ys)[kSolveBlock] = reinterpret_cast<cx<R>(*)[kSolveBlock]>(T + kSolveBlock * kSolveBlock);
     const Item it = S.items[item0 + blockIdx.x];
-    const int s = it.s, j0 = it.a * kSolveBlock;
-    const int w = S.first[s + 1] - S.first[s];
-    const int m = S.rows[s];
-    const int f = S.first[s];
-    const int jb = min(kSolveBlock, w - j0);
-    const cx<R>* P = Lb + lstride * eb + S.loff[s] + j0 + static_cast<long long>(j0) * m;
-#pragma unroll 4
-    for (int e = threadIdx.x; e < jb * jb; e += blockDim.x) {
-        const int i = e % jb, j = e / jb;
-        T[i + j * kSolveBlock] = P[i + static_cast<long long>(j) * m];
-    }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    cx<R>* y = yb + vec_at(a, eb, warp) * a.n + f + j0;
-    if (warp < a.nr)
-        for (int i = lane; i < jb; i += 32) ys[warp][i] = y[i];
-    __syncthreads();
-    if (warp >= a.nr) return;
-    for (int j = 0; j < jb; ++j) {
-        const cx<R> yj = ys[warp][j];
-        for (int i = j + 1 + lane; i < jb; i += 32) ys[warp][i] = fms(ys[warp][i], T[i + j * kSolveBlock], yj);
-        __syncwarp();
-    }
-    for (int i = lane; i < jb; i += 32) y[i] = ys[warp][i];
+    fwd_triangle<R>(S, a, solve_entry(a), Lb, lstride, yb, it.s, it.a, smem_raw);
 }
 
-// Item (s, blk, row0): rows row0.. of the supernode minus L[rows, blk] y[blk].
-template <class R>
+// Item (s, blk, row0): rows row0 .. row0 + kSolveRows - 1 of the supernode
+// minus L[rows, blk] y[blk]. Four threads per row, each over 16 of the
+// block's columns with all 16 loads in flight (one round trip); the four
+// column-ordered sub-sums are added in order. Fused: the last of the
+// block's CTAs then solves block blk + 1 (counters: one per supernode and
+// grid row; dynamic shared memory kTriSmem entries).
+template <class R, bool Fused>
 __global__ void __launch_bounds__(256) k_fwd_update(Sched S, long long item0, SolveArgs a, const cx<R>* Lb,
                                                     long long lstride, cx<R>* yb, cx<R>* Ub) {
+    static_assert(kSolveRows * 4 == 256 && kSolveBlock == 64, "four 16-column quarters per row");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int eb = solve_entry(a);
     __shared__ cx<R> ys[8][kSolveBlock];
+    __shared__ cx<R> red[3][8][kSolveRows];  // quarters 1..3's sub-sums
     const Item it = S.items[item0 + blockIdx.x];
     const int s = it.s, j0 = it.a * kSolveBlock, row0 = it.b;
     const int w = S.first[s + 1] - S.first[s];
     const int m = S.rows[s];
     const int f = S.first[s];
     const int jb = min(kSolveBlock, w - j0);
+    const int t = threadIdx.x % kSolveRows, qt = threadIdx.x / kSolveRows;
+    const int r = row0 + t;
+    const int c0 = 16 * qt, nc = min(16, jb - c0);
+    // The panel entries first (they depend on the item only), so their round
+    // trip overlaps the block's y values'.
+    cx<R> l[16];
+    {
+        const bool live = r < m && nc > 0;
+        const cx<R>* P = Lb + lstride * eb + S.loff[s] + (live ? r : 0) + static_cast<long long>(j0 + c0) * m;
+#pragma unroll
+        for (int u = 0; u < 16; ++u) l[u] = live && u < nc ? P[static_cast<long long>(u) * m] : cx<R>{0, 0};
+    }
+    // The first rhs's destination, read now (only this CTA writes these rows
+    // in this launch).
+    cx<R>* dst0 = r < w ? yb + vec_at(a, eb, 0) * a.n + f + r : Ub + vec_at(a, eb, 0) * a.upool + S.uoff[s] + (r - w);
+    const cx<R> old0 = qt == 0 && r < m ? *dst0 : cx<R>{0, 0};
+    if constexpr (Fused) {
+        const int jn = j0 + kSolveBlock;  // the next block, which this launch's last CTA solves
+        if (row0 == j0 + jb && jn < w)
+            prefetch_triangle(Lb + lstride * eb + S.loff[s] + jn + static_cast<long long>(jn) * m, m,
+                              min(kSolveBlock, w - jn));
+    }
     for (int e = threadIdx.x; e < jb * a.nr; e += blockDim.x) {
         const int j = e % jb, k = e / jb;
         ys[k][j] = yb[vec_at(a, eb, k) * a.n + f + j0 + j];
     }
     __syncthreads();
-    const int r = row0 + threadIdx.x;
-    if (r >= m) return;
-    const cx<R>* P = Lb + lstride * eb + S.loff[s] + r + static_cast<long long>(j0) * m;
     cx<R> acc[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) acc[k] = cx<R>{0, 0};
-    // Eight columns' loads in flight before they are used (one round trip per
-    // eight columns, not per column); the sums keep their column order.
-    for (int j = 0; j < jb; j += 8) {
-        cx<R> l[8];
+    if (r < m && nc > 0) {
 #pragma unroll
-        for (int u = 0; u < 8; ++u) l[u] = j + u < jb ? P[static_cast<long long>(j + u) * m] : cx<R>{0, 0};
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            if (j + u >= jb) break;
+        for (int u = 0; u < 16; ++u) {
+            if (u >= nc) break;
 #pragma unroll
             for (int k = 0; k < 8; ++k)
-                if (k < a.nr) acc[k] = acc[k] + l[u] * ys[k][j + u];
+                if (k < a.nr) acc[k] = acc[k] + l[u] * ys[k][c0 + u];
         }
     }
+    if (qt > 0) {
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        if (k >= a.nr) break;
-        cx<R>* dst = r < w ? yb + vec_at(a, eb, k) * a.n + f + r
-                           : Ub + vec_at(a, eb, k) * a.upool + S.uoff[s] + (r - w);
-        *dst = *dst - acc[k];
+        for (int k = 0; k < 8; ++k)
+            if (k < a.nr) red[qt - 1][k][t] = acc[k];
+    }
+    __syncthreads();
+    if (qt == 0 && r < m) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k >= a.nr) break;
+            const cx<R> sum = ((acc[k] + red[0][k][t]) + red[1][k][t]) + red[2][k][t];
+            cx<R>* dst = r < w ? yb + vec_at(a, eb, k) * a.n + f + r
+                               : Ub + vec_at(a, eb, k) * a.upool + S.uoff[s] + (r - w);
+            *dst = (k == 0 ? old0 : *dst) - sum;
+        }
+    }
+    if constexpr (Fused) {
+        const int below = j0 + jb;
+        const int chunks = (m - below + kSolveRows - 1) / kSolveRows;
+        if (last_to_arrive(a.counters + static_cast<long long>(blockIdx.y) * a.ns + s, chunks) &&
+            it.a + 1 < solve_nblocks(S, s))
+            fwd_triangle<R>(S, a, eb, Lb, lstride, yb, s, it.a + 1, smem_raw);
     }
 }
 
-// Item (s, blk, row0, slot): partial[slot][j][k] = sum over rows row0..row0+255
-// (below the block) of L[row, j0 + j] x_k[row].
+// Backward triangle of block blk of supernode s: x[blk] = L_bb^-T (D^-1
+// y[blk] - sum of the partials in slots p0 .. p0 + np - 1) for the pass's
+// rhs (smem: kTriSmem + kRedSmem entries). The partials are summed by four
+// threads per (column, rhs), each over every fourth slot in slot order, the
+// four sub-sums then added in order. The triangle: one warp per rhs, lane l
+// holding rows l and l + 32; step j (descending) broadcasts x_j from its
+// owner lane and every lane above updates its rows, z_t = z_t - L_jt x_j.
+// Every thread of the CTA calls it (256 threads).
 template <class R>
+__device__ void bwd_triangle(const Sched& S, const SolveArgs& a, int eb, const cx<R>* Lb, long long lstride,
+                             cx<R>* yb, const cx<R>* partb, int s, int blk, int p0, int np, unsigned char* smem) {
+    static_assert(kSolveBlock == 64, "two rows per lane");
+    cx<R>* T = reinterpret_cast<cx<R>*>(smem);
+    cx<R>* red = T + kTriSmem;  // [4][8][kSolveBlock]
+    const int j0 = blk * kSolveBlock;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int f = S.first[s];
+    const int jb = min(kSolveBlock, w - j0);
+    stage_triangle(T, Lb + lstride * eb + S.loff[s] + j0 + static_cast<long long>(j0) * m, m, jb);
+    const cx<R>* part = partb + static_cast<long long>(eb) * a.max_parts * kSolveBlock * 8;
+    for (int e = threadIdx.x; e < 4 * kSolveBlock * a.nr; e += blockDim.x) {
+        const int g = e & 3, j = (e >> 2) % kSolveBlock, k = (e >> 2) / kSolveBlock;
+        cx<R> sum{0, 0};
+        if (j < jb) {
+            constexpr int kU = 16;  // loads in flight per thread
+            int q = g;
+            for (; q + 4 * (kU - 1) < np; q += 4 * kU) {
+                cx<R> v[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u)
+                    v[u] = ld_l2(part + (static_cast<long long>(p0 + q + 4 * u) * kSolveBlock + j) * 8 + k);
+#pragma unroll
+                for (int u = 0; u < kU; ++u) sum = sum + v[u];
+            }
+            for (; q < np; q += 4) sum = sum + ld_l2(part + (static_cast<long long>(p0 + q) * kSolveBlock + j) * 8 + k);
+        }
+        red[(g * 8 + k) * kSolveBlock + j] = sum;
+    }
+    triangle_wait();
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < a.nr) {
+        cx<R>* y = yb + vec_at(a, eb, warp) * a.n + f + j0;
+        cx<R> z[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int j = lane + 32 * h;
+            z[h] = cx<R>{0, 0};
+            if (j < jb) {
+                const cx<R>* rj = red + warp * kSolveBlock + j;
+                const cx<R> sum = ((rj[0] + rj[8 * kSolveBlock]) + rj[16 * kSolveBlock]) + rj[24 * kSolveBlock];
+                z[h] = ld_l2(y + j) * crecip(T[j * (kTriLd + 1)]) - sum;
+            }
+        }
+        for (int j = jb - 1; j >= 0; --j) {
+            const cx<R> src = j < 32 ? z[0] : z[1];
+            cx<R> xj;
+            xj.re = __shfl_sync(0xffffffffu, src.re, j & 31);
+            xj.im = __shfl_sync(0xffffffffu, src.im, j & 31);
+            if (lane < j) z[0] = fms(z[0], T[j + lane * kTriLd], xj);
+            if (lane + 32 < j) z[1] = fms(z[1], T[j + (lane + 32) * kTriLd], xj);
+        }
+        if (lane < jb) y[lane] = z[0];
+        if (lane + 32 < jb) y[lane + 32] = z[1];
+    }
+}
+
+// Item (s, blk, row0, slot[, p0]): partial[slot][j][k] = sum over rows
+// row0 .. row0 + kSolveRows - 1 (below the block) of L[row, j0 + j] x_k[row]
+// (an empty chunk, row0 = m, gives zeros). Warp v takes columns 8v .. 8v + 7,
+// lane l rows l and l + 32: all 16 loads in flight (one round trip); per
+// column the lane's two rows in order, then a butterfly over the warp.
+// Fused: the last of the block's CTAs then reduces the block's partials
+// (slots p0 ..) and solves the block (counters: one per supernode and grid
+// row; dynamic shared memory kTriSmem + kRedSmem entries).
+template <class R, bool Fused>
 __global__ void __launch_bounds__(256) k_bwd_update(Sched S, long long item0, SolveArgs a, const cx<R>* Lb,
-                                                    long long lstride, const cx<R>* yb, cx<R>* partb) {
+                                                    long long lstride, cx<R>* yb, cx<R>* partb) {
+    static_assert(kSolveRows == 64 && kSolveBlock == 64, "two rows per lane, eight columns per warp");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int eb = solve_entry(a);
     __shared__ cx<R> xs[8][kSolveRows];
     const Item it = S.items[item0 + blockIdx.x];
@@ -902,8 +1125,26 @@ __global__ void __launch_bounds__(256) k_bwd_update(Sched S, long long item0, So
     const int m = S.rows[s];
     const int f = S.first[s];
     const int jb = min(kSolveBlock, w - j0);
-    const int nrows = min(kSolveRows, m - row0);
+    const int nrows = max(0, min(kSolveRows, m - row0));
     const int* st = S.structs + S.soff[s];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // The panel entries first (they depend on the item only), so their round
+    // trip overlaps the gather of x.
+    if constexpr (Fused) {
+        if (row0 == j0 + jb)  // the block's triangle, which this launch's last CTA stages
+            prefetch_triangle(Lb + lstride * eb + S.loff[s] + j0 + static_cast<long long>(j0) * m, m, jb);
+    }
+    cx<R> l[8][2];
+    {
+        const cx<R>* P = Lb + lstride * eb + S.loff[s] + static_cast<long long>(j0) * m;
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int j = 8 * warp + c, t = lane + 32 * h;
+                l[c][h] = j < jb && t < nrows ? P[row0 + t + static_cast<long long>(j) * m] : cx<R>{0, 0};
+            }
+    }
     for (int e = threadIdx.x; e < nrows * a.nr; e += blockDim.x) {
         const int t = e % nrows, k = e / nrows;
         const int r = row0 + t;
@@ -911,33 +1152,19 @@ __global__ void __launch_bounds__(256) k_bwd_update(Sched S, long long item0, So
         xs[k][t] = yb[vec_at(a, eb, k) * a.n + g];
     }
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const cx<R>* P = Lb + lstride * eb + S.loff[s] + row0 + static_cast<long long>(j0) * m;
     cx<R>* part = partb + static_cast<long long>(eb) * a.max_parts * kSolveBlock * 8 +
                   static_cast<long long>(slot) * kSolveBlock * 8;
-    for (int j = warp; j < jb; j += 8) {
-        const cx<R>* col = P + static_cast<long long>(j) * m;
-        cx<R> acc[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) acc[k] = cx<R>{0, 0};
-        // All of a lane's rows (at most 8: kSolveRows = 256) loaded before
-        // use; the sums keep their row order.
-        static_assert(kSolveRows <= 32 * 8, "one pass of 8 loads per lane covers the chunk");
-        cx<R> l[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) l[u] = lane + 32 * u < nrows ? col[lane + 32 * u] : cx<R>{0, 0};
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int t = lane + 32 * u;
-            if (t >= nrows) break;
-#pragma unroll
-            for (int k = 0; k < 8; ++k)
-                if (k < a.nr) acc[k] = acc[k] + l[u] * xs[k][t];
-        }
+    for (int c = 0; c < 8; ++c) {
+        const int j = 8 * warp + c;
+        if (j >= jb) break;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             if (k >= a.nr) break;
-            cx<R> v = acc[k];
+            cx<R> v{0, 0};
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                if (lane + 32 * h < nrows) v = v + l[c][h] * xs[k][lane + 32 * h];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
                 v.re += __shfl_xor_sync(0xffffffffu, v.re, o);
@@ -946,47 +1173,22 @@ __global__ void __launch_bounds__(256) k_bwd_update(Sched S, long long item0, So
             if (lane == 0) part[j * 8 + k] = v;
         }
     }
+    if constexpr (Fused) {
+        const int below = j0 + jb;
+        const int chunks = max(1, (m - below + kSolveRows - 1) / kSolveRows);
+        if (last_to_arrive(a.counters + static_cast<long long>(blockIdx.y) * a.ns + s, chunks))
+            bwd_triangle<R>(S, a, eb, Lb, lstride, yb, partb, s, it.a, it.d, chunks, smem_raw);
+    }
 }
 
-// Item (s, blk, first_slot, nslots): x[blk] = L_bb^-T (D^-1 y[blk] - sum of partials).
+// Item (s, blk, first_slot, nslots): x[blk] = L_bb^-T (D^-1 y[blk] - sum of
+// partials) (the split plan's triangle launch).
 template <class R>
 __global__ void __launch_bounds__(256) k_bwd_diag(Sched S, long long item0, SolveArgs a, const cx<R>* Lb,
                                                   long long lstride, cx<R>* yb, const cx<R>* partb) {
-    const int eb = solve_entry(a);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cx<R>* T = reinterpret_cast<cx<R>*>(smem_raw);
-    cx<R>(*zs)[kSolveBlock] = reinterpret_cast<cx<R>(*)[kSolveBlock]>(T + kSolveBlock * kSolveBlock);
     const Item it = S.items[item0 + blockIdx.x];
-    const int s = it.s, j0 = it.a * kSolveBlock, p0 = it.b, np = it.c;
-    const int w = S.first[s + 1] - S.first[s];
-    const int m = S.rows[s];
-    const int f = S.first[s];
-    const int jb = min(kSolveBlock, w - j0);
-    const cx<R>* P = Lb + lstride * eb + S.loff[s] + j0 + static_cast<long long>(j0) * m;
-#pragma unroll 4
-    for (int e = threadIdx.x; e < jb * jb; e += blockDim.x) {
-        const int i = e % jb, j = e / jb;
-        T[i + j * kSolveBlock] = P[i + static_cast<long long>(j) * m];
-    }
-    __syncthreads();
-    const cx<R>* part = partb + static_cast<long long>(eb) * a.max_parts * kSolveBlock * 8;
-    for (int e = threadIdx.x; e < jb * a.nr; e += blockDim.x) {
-        const int j = e % jb, k = e / jb;
-        cx<R> sum{0, 0};
-        for (int q = 0; q < np; ++q) sum = sum + part[(static_cast<long long>(p0 + q) * kSolveBlock + j) * 8 + k];
-        const cx<R> yv = yb[vec_at(a, eb, k) * a.n + f + j0 + j];
-        zs[k][j] = yv * crecip(T[j * (kSolveBlock + 1)]) - sum;
-    }
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp >= a.nr) return;
-    for (int j = jb - 1; j >= 0; --j) {
-        const cx<R> xj = zs[warp][j];
-        for (int t = lane; t < j; t += 32) zs[warp][t] = fms(zs[warp][t], T[j + t * kSolveBlock], xj);
-        __syncwarp();
-    }
-    cx<R>* y = yb + vec_at(a, eb, warp) * a.n + f + j0;
-    for (int i = lane; i < jb; i += 32) y[i] = zs[warp][i];
+    bwd_triangle<R>(S, a, solve_entry(a), Lb, lstride, yb, partb, it.s, it.a, it.b, it.c, smem_raw);
 }
 
 }  // namespace aphi_b200

@@ -442,9 +442,10 @@ int aphi_fronts_read(const aphi_factor* f, int k, double* panels_dev, double* cb
 int aphi_analysis_plan_stats(const aphi_analysis* a, int plan, int64_t* launches, int64_t* items, double* useful,
                              double* executed);
 
-/* Per-kind device time of a factor's factorizations: while enabled, every
- * launch of the factorization plan is bracketed by CUDA events on its stream
- * and its duration added to ms[kind] (launch counts in launches[kind]).
+/* Per-kind device time of a factor's factorizations and solves: while
+ * enabled, every launch of the factorization and solve plans is bracketed by
+ * CUDA events on its stream and its duration added to ms[kind] (launch
+ * counts in launches[kind]; the solve kinds are 5..9).
  * Enabling clears the totals. Costs two events per launch: for measurement
  * runs, not for timed ones. */
 int aphi_factor_profile(aphi_factor* f, int enable);

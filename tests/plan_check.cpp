@@ -402,88 +402,151 @@ void run_solve_plan(const aphi_analysis& A, Fronts& F, SolveMem& V, const std::v
     Checker& ck = F.ck;
     const long long n = S.n;
     auto Lv = [&](int s, int i, int j) { return F.L.v[S.sn_loff[s] + i + static_cast<long long>(j) * S.sn_rows[s]]; };
+    auto nblocks = [&](int s) { return (F.width(s) + kSolveBlock - 1) / kSolveBlock; };
+    auto gather = [&](int s) {
+        const int w = F.width(s), f = S.sn_first[s];
+        const long long us = A.h_uoff[s], ue = A.h_uoff[s + 1];
+        for (long long i = us; i < ue; ++i) ck.wr(V.U, i, 0.0, us, ue);
+        for (int t = S.child_ptr[s]; t < S.child_ptr[s + 1]; ++t) {
+            const int c = S.child_list[t];
+            const int cc = F.rows(c) - F.width(c);
+            const int* rel = S.rel.data() + S.rel_off[c];
+            const long long uc = A.h_uoff[c];
+            for (int i = 0; i < cc; ++i) {
+                const C v = ck.rd(V.U, uc + i, uc, uc + cc);
+                if (rel[i] < w) ck.wr(V.y, f + rel[i], ck.rd(V.y, f + rel[i], f, f + w) + v, f, f + w);
+                else ck.wr(V.U, us + rel[i] - w, ck.rd(V.U, us + rel[i] - w, us, ue) + v, us, ue);
+            }
+        }
+    };
+    auto fdiag = [&](int s, int blk) {
+        const int w = F.width(s), f = S.sn_first[s];
+        const int j0 = blk * kSolveBlock, jb = std::min(kSolveBlock, w - j0);
+        std::vector<C> ys(jb);
+        for (int i = 0; i < jb; ++i) ys[i] = ck.rd(V.y, f + j0 + i, f, f + w);
+        for (int j = 0; j < jb; ++j)
+            for (int i = j + 1; i < jb; ++i) ys[i] -= Lv(s, j0 + i, j0 + j) * ys[j];
+        for (int i = 0; i < jb; ++i) ck.wr(V.y, f + j0 + i, ys[i], f, f + w);
+    };
+    auto fupd = [&](const Item& it) {
+        const int s = it.s, w = F.width(s), m = F.rows(s), f = S.sn_first[s];
+        const long long us = A.h_uoff[s], ue = A.h_uoff[s + 1];
+        const int j0 = it.a * kSolveBlock, jb = std::min(kSolveBlock, w - j0);
+        std::vector<C> ys(jb);
+        for (int j = 0; j < jb; ++j) ys[j] = ck.rd(V.y, f + j0 + j, f, f + w);
+        const int r0 = it.b, r1 = std::min(it.b + kSolveRows, m);
+        std::vector<C> acc(std::max(r1 - r0, 0), 0.0);  // each row's sum in column order
+        for (int j = 0; j < jb; ++j)
+            for (int r = r0; r < r1; ++r) acc[r - r0] += Lv(s, r, j0 + j) * ys[j];
+        for (int r = r0; r < r1; ++r) {
+            if (r < w) ck.wr(V.y, f + r, ck.rd(V.y, f + r, f, f + w) - acc[r - r0], f, f + w);
+            else ck.wr(V.U, us + r - w, ck.rd(V.U, us + r - w, us, ue) - acc[r - r0], us, ue);
+        }
+    };
+    auto bupd = [&](const Item& it) {
+        const int s = it.s, w = F.width(s), m = F.rows(s), f = S.sn_first[s];
+        const int j0 = it.a * kSolveBlock, jb = std::min(kSolveBlock, w - j0);
+        const int row0 = it.b, slot = it.c, nrows = std::max(0, std::min(kSolveRows, m - row0));
+        const int* st = S.structs.data() + S.sn_struct_off[s];
+        std::vector<C> xs(nrows);
+        for (int t = 0; t < nrows; ++t) {
+            const int r = row0 + t;
+            xs[t] = ck.rd(V.y, r < w ? f + r : st[r], 0, n);
+        }
+        const long long pb = static_cast<long long>(slot) * kSolveBlock * 8;
+        for (int j = 0; j < jb; ++j) {
+            C acc = 0.0;
+            for (int t = 0; t < nrows; ++t) acc += Lv(s, row0 + t, j0 + j) * xs[t];
+            ck.wr(V.part, pb + j * 8, acc, pb, pb + kSolveBlock * 8);
+        }
+    };
+    auto bdiag = [&](int s, int blk, int p0, int np) {
+        const int w = F.width(s), f = S.sn_first[s];
+        const int j0 = blk * kSolveBlock, jb = std::min(kSolveBlock, w - j0);
+        std::vector<C> z(jb);
+        for (int j = 0; j < jb; ++j) {
+            C sum = 0.0;
+            for (int qq = 0; qq < np; ++qq) {
+                const long long pb = static_cast<long long>(p0 + qq) * kSolveBlock * 8;
+                sum += ck.rd(V.part, pb + j * 8, pb, pb + kSolveBlock * 8);
+            }
+            z[j] = ck.rd(V.y, f + j0 + j, f, f + w) / Lv(s, j0 + j, j0 + j) - sum;
+        }
+        for (int j = jb - 1; j >= 0; --j)
+            for (int t = 0; t < j; ++t) z[t] -= Lv(s, j0 + j, j0 + t) * z[j];
+        for (int j = 0; j < jb; ++j) ck.wr(V.y, f + j0 + j, z[j], f, f + w);
+    };
+    // The chunk count a fused kernel expects for (s, blk): its CTAs' arrivals.
+    auto chunks = [&](int s, int blk, bool backward) {
+        const int below = std::min(F.width(s), (blk + 1) * kSolveBlock);
+        const int c = (F.rows(s) - below + kSolveRows - 1) / kSolveRows;
+        return backward ? std::max(1, c) : c;
+    };
     for (const Launch& l : plan) {
         ++ck.launch;
         ++ck.launches;
-        ck.kind = "solve";
+        ck.kind = l.wide ? "solve (fused)" : "solve";
+        struct Arrivals {
+            int blk = -1, count = 0, p0 = -1;
+            std::vector<int> slots;
+        };
+        std::map<int, Arrivals> arrived;  // fused launches: per supernode
         for (int q = 0; q < l.count; ++q) {
             ck.item = q;
             ++ck.items;
             const Item& it = A.h_items[l.first + q];
-            const int s = it.s, w = F.width(s), m = F.rows(s), f = S.sn_first[s];
-            const long long us = A.h_uoff[s], ue = A.h_uoff[s + 1];
-            const int j0 = it.a * kSolveBlock, jb = std::min(kSolveBlock, w - j0);
+            if (l.wide && l.kind != K_FWD_GATHER) {
+                Arrivals& ar = arrived[it.s];
+                if (ar.count > 0 && (ar.blk != it.a || (l.kind == K_BWD_UPDATE && ar.p0 != it.d))) {
+                    ++ck.bounds;
+                    ck.report("fused solve items of one supernode disagree on the block or first slot", "s", it.s);
+                }
+                ar.blk = it.a;
+                ar.p0 = it.d;
+                ++ar.count;
+                ar.slots.push_back(it.c);
+            }
             switch (l.kind) {
                 case K_FWD_GATHER:
-                    for (long long i = us; i < ue; ++i) ck.wr(V.U, i, 0.0, us, ue);
-                    for (int t = S.child_ptr[s]; t < S.child_ptr[s + 1]; ++t) {
-                        const int c = S.child_list[t];
-                        const int cc = F.rows(c) - F.width(c);
-                        const int* rel = S.rel.data() + S.rel_off[c];
-                        const long long uc = A.h_uoff[c];
-                        for (int i = 0; i < cc; ++i) {
-                            const C v = ck.rd(V.U, uc + i, uc, uc + cc);
-                            if (rel[i] < w) ck.wr(V.y, f + rel[i], ck.rd(V.y, f + rel[i], f, f + w) + v, f, f + w);
-                            else ck.wr(V.U, us + rel[i] - w, ck.rd(V.U, us + rel[i] - w, us, ue) + v, us, ue);
-                        }
-                    }
+                    gather(it.s);
+                    if (l.wide) fdiag(it.s, 0);  // the same CTA, after its gather
                     break;
-                case K_FWD_DIAG: {
-                    std::vector<C> ys(jb);
-                    for (int i = 0; i < jb; ++i) ys[i] = ck.rd(V.y, f + j0 + i, f, f + w);
-                    for (int j = 0; j < jb; ++j)
-                        for (int i = j + 1; i < jb; ++i) ys[i] -= Lv(s, j0 + i, j0 + j) * ys[j];
-                    for (int i = 0; i < jb; ++i) ck.wr(V.y, f + j0 + i, ys[i], f, f + w);
-                    break;
-                }
-                case K_FWD_UPDATE: {
-                    std::vector<C> ys(jb);
-                    for (int j = 0; j < jb; ++j) ys[j] = ck.rd(V.y, f + j0 + j, f, f + w);
-                    const int r0 = it.b, r1 = std::min(it.b + kSolveRows, m);
-                    std::vector<C> acc(std::max(r1 - r0, 0), 0.0);  // each row's sum in column order
-                    for (int j = 0; j < jb; ++j)
-                        for (int r = r0; r < r1; ++r) acc[r - r0] += Lv(s, r, j0 + j) * ys[j];
-                    for (int r = r0; r < r1; ++r) {
-                        if (r < w) ck.wr(V.y, f + r, ck.rd(V.y, f + r, f, f + w) - acc[r - r0], f, f + w);
-                        else ck.wr(V.U, us + r - w, ck.rd(V.U, us + r - w, us, ue) - acc[r - r0], us, ue);
-                    }
-                    break;
-                }
-                case K_BWD_UPDATE: {
-                    const int row0 = it.b, slot = it.c, nrows = std::min(kSolveRows, m - row0);
-                    const int* st = S.structs.data() + S.sn_struct_off[s];
-                    std::vector<C> xs(nrows);
-                    for (int t = 0; t < nrows; ++t) {
-                        const int r = row0 + t;
-                        xs[t] = ck.rd(V.y, r < w ? f + r : st[r], 0, n);
-                    }
-                    const long long pb = static_cast<long long>(slot) * kSolveBlock * 8;
-                    for (int j = 0; j < jb; ++j) {
-                        C acc = 0.0;
-                        for (int t = 0; t < nrows; ++t) acc += Lv(s, row0 + t, j0 + j) * xs[t];
-                        ck.wr(V.part, pb + j * 8, acc, pb, pb + kSolveBlock * 8);
-                    }
-                    break;
-                }
-                case K_BWD_DIAG: {
-                    const int p0 = it.b, np = it.c;
-                    std::vector<C> z(jb);
-                    for (int j = 0; j < jb; ++j) {
-                        C sum = 0.0;
-                        for (int qq = 0; qq < np; ++qq) {
-                            const long long pb = static_cast<long long>(p0 + qq) * kSolveBlock * 8;
-                            sum += ck.rd(V.part, pb + j * 8, pb, pb + kSolveBlock * 8);
-                        }
-                        z[j] = ck.rd(V.y, f + j0 + j, f, f + w) / Lv(s, j0 + j, j0 + j) - sum;
-                    }
-                    for (int j = jb - 1; j >= 0; --j)
-                        for (int t = 0; t < j; ++t) z[t] -= Lv(s, j0 + j, j0 + t) * z[j];
-                    for (int j = 0; j < jb; ++j) ck.wr(V.y, f + j0 + j, z[j], f, f + w);
-                    break;
-                }
+                case K_FWD_DIAG: fdiag(it.s, it.a); break;
+                case K_FWD_UPDATE: fupd(it); break;
+                case K_BWD_UPDATE: bupd(it); break;
+                case K_BWD_DIAG: bdiag(it.s, it.a, it.b, it.c); break;
                 default:
                     ++ck.bounds;
                     ck.report("unexpected kind in a solve plan", "plan", l.kind);
+            }
+        }
+        if (arrived.empty()) continue;
+        // The last CTA of each supernode: after every other CTA of the launch
+        // (a phase of its own for the race checks).
+        ++ck.launch;
+        ck.kind = "solve (fused, last CTA)";
+        for (const auto& kv : arrived) {
+            const int s = kv.first;
+            const Arrivals& ar = kv.second;
+            ck.item = s;
+            const bool bwd = l.kind == K_BWD_UPDATE;
+            if (ar.count != chunks(s, ar.blk, bwd)) {
+                ++ck.bounds;
+                ck.report("fused solve: the kernel's expected arrivals differ from the plan's items", "s", s);
+                continue;
+            }
+            if (bwd) {
+                std::vector<int> sl = ar.slots;
+                std::sort(sl.begin(), sl.end());
+                for (int k = 0; k < static_cast<int>(sl.size()); ++k)
+                    if (sl[k] != ar.p0 + k) {
+                        ++ck.bounds;
+                        ck.report("fused backward slots are not p0 .. p0 + np - 1", "s", s);
+                        break;
+                    }
+                bdiag(s, ar.blk, ar.p0, ar.count);
+            } else if (ar.blk + 1 < nblocks(s)) {
+                fdiag(s, ar.blk + 1);
             }
         }
     }
@@ -682,13 +745,18 @@ int check_matrix(int n, const std::vector<int>& rp, const std::vector<int>& ci, 
                 d[S.ref_of_post[S.sn_first[s] + j]] = F.L.v[S.sn_loff[s] + j + static_cast<long long>(j) * F.rows(s)];
         const long long f_launches = ck.launches, f_items = ck.items;
         SolveMem V(n, A->upool, A->max_parts);
-        for (int i = 0; i < n; ++i) V.y.v[i] = bz[S.orig_of_new[i]];
-        run_solve_plan(*A, F, V, A->plan_fwd);
-        run_solve_plan(*A, F, V, A->plan_bwd);
-        std::vector<C> x(n);
-        for (int o = 0; o < n; ++o) x[o] = V.y.v[S.new_of_orig[o]];
+        std::vector<C> x(n), x_split(n);
+        for (int form = 0; form < 2; ++form) {  // the fused plans, then the split ones
+            for (int i = 0; i < n; ++i) V.y.v[i] = bz[S.orig_of_new[i]];
+            run_solve_plan(*A, F, V, form ? A->plan_fwd_split : A->plan_fwd);
+            run_solve_plan(*A, F, V, form ? A->plan_bwd_split : A->plan_bwd);
+            for (int o = 0; o < n; ++o) (form ? x_split : x)[o] = V.y.v[S.new_of_orig[o]];
+        }
         const double de = rel_err(d, d_or), xe = rel_err(x, x_or);
-        const bool ok = !ck.bounds && !ck.ww && !ck.rw && !ck.stale && de <= 1e-12 && xe <= 1e-10;
+        // The fused and split solve plans do the same arithmetic in the same order.
+        const bool same = x == x_split;
+        const bool ok = !ck.bounds && !ck.ww && !ck.rw && !ck.stale && de <= 1e-12 && xe <= 1e-10 && same;
+        if (!same) std::printf("fused and split solve plans differ\n");
         int caps[3] = {0, 0, 0};  // trailing-update launches applying 1, 2 and 4 panels
         for (const Launch& l : *plans[p])
             if (l.kind == K_UPDATE_WIDE || l.kind == K_UPDATE_TC) ++caps[l.kcap == kTcPanel ? 0 : l.kcap == 2 * kTcPanel ? 1 : 2];

@@ -287,6 +287,43 @@ def test_cocg_refinement_converges(cuda):
     assert ok and (res[:, 0, 0] <= 1e-13).all(), (iters, res)
 
 
+@pytest.mark.parametrize("precision", [ab.PREC_FP64, ab.PREC_FP32])
+def test_fused_solve_plans_equal_split_ones_bit_for_bit(precision, cuda):
+    """The solves' fused plans (each triangle solved by the last CTA of the
+    launch before it, handed over by an arrival counter) against the split
+    plans (a launch per triangle): the same arithmetic in the same order, so
+    the same bits, with 9 right-hand sides (two passes of the counters), a
+    batch of 3, and twice in a row on one handle."""
+    import os
+    w = ab.Workload.cylinder(16)
+    an = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx))
+    asm = ab.Assembly(ab.workload_arrays(w))
+    vals, rhs = asm.refill(2 * np.pi * np.array([50.0, 1e4, 1e6]))
+    g = torch.Generator(device="cuda").manual_seed(3)
+    b = torch.randn(3, 9, an.n, 2, device="cuda", dtype=torch.float64, generator=g)
+    b = torch.view_as_complex(b.contiguous())
+    b[:, 0] = rhs
+    saved = os.environ.get("APHI_SOLVE_SPLIT")
+    xs = []
+    try:
+        for split in ("0", "1"):
+            os.environ["APHI_SOLVE_SPLIT"] = split
+            f = ab.Factor(an, precision=precision, batch=3)
+            assert f.factorize(vals)
+            for _ in range(2):
+                xs.append(f.solve(b).cpu().numpy())
+            f.close()
+    finally:
+        if saved is None:
+            os.environ.pop("APHI_SOLVE_SPLIT", None)
+        else:
+            os.environ["APHI_SOLVE_SPLIT"] = saved
+    assert np.isfinite(xs[0]).all()
+    for x in xs[1:]:
+        np.testing.assert_array_equal(x, xs[0])
+    assert an.plan_stats(2).get("fwd_diag") is None and an.plan_stats(3).get("bwd_diag") is None
+
+
 def test_factor_profile_counts_every_planned_launch(cuda):
     """aphi_factor_profile: one factorization with timing on records exactly
     the launches its plan holds, per kind, with positive durations. The

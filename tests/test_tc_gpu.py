@@ -117,6 +117,42 @@ def test_tc_factor_as_accurate_as_simt(cells, cuda):
     assert ok and (res[:, 0, 0] <= 1e-13).all(), (iters, res)
 
 
+@pytest.mark.parametrize("group,stages", [(2, 3), (2, 4), (4, 4)])
+def test_presplit_operands_give_the_in_tile_split_bit_for_bit(group, stages, cuda):
+    """The two-piece tile on operands split once per panel group (k_tc_split,
+    bulk copies, separate producer and MMA-issuer threads) computes exactly
+    what the tile that splits its own operands computes: the same planes, the
+    same MMAs in the same order, the same drains. Factors of a 16^3 sweep
+    batch, solved, equal bit for bit, for each accumulator group and buffer
+    count; and again on a second factorization with the same handle."""
+    w = ab.Workload.cylinder(16)
+    an = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx))
+    assert an.plan_stats(1).get("tc_split", (0, 0))[0] > 0
+    asm = ab.Assembly(ab.workload_arrays(w))
+    vals, rhs = asm.refill(2 * np.pi * np.geomspace(50.0, 1.0e6, 3))
+    keys = ("APHI_TC_PRESPLIT", "APHI_TC_PRESTAGES", "APHI_TC_GROUP")
+    saved = {k: os.environ.get(k) for k in keys}
+    xs = []
+    try:
+        for pre in ("0", "1"):
+            os.environ.update(APHI_TC_PRESPLIT=pre, APHI_TC_PRESTAGES=str(stages), APHI_TC_GROUP=str(group))
+            f = ab.Factor(an, precision=ab.PREC_FP32, batch=3)
+            f.set_tc_split(2)
+            for _ in range(2):
+                assert f.factorize(vals)
+                xs.append(f.solve(rhs).cpu().numpy())
+            f.close()
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    assert np.isfinite(xs[0]).all()
+    for x in xs[1:]:
+        np.testing.assert_array_equal(x, xs[0])
+
+
 def test_bounded_wait_gives_up_and_the_context_survives(cuda):
     """A device wait that nothing ends -- an mbarrier whose one arrival never
     comes -- waited on with the tensor-core tile's own bounded wait: the
