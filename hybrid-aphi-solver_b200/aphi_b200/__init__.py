@@ -92,7 +92,7 @@ class AssemblyDesc(C.Structure):
 
 class AnalysisOptions(C.Structure):
     _fields_ = [("relax_small", I), ("relax_fill", D), ("relax_max_width", I), ("small_front", I),
-                ("group4_rows", I), ("group2_rows", I)]
+                ("group4_rows", I), ("group2_rows", I), ("tc_group4_rows", I), ("tc_group2_rows", I)]
 
 
 class FactorStats(C.Structure):

@@ -8,7 +8,12 @@ one CTA (`small_front` rows and fewer), and how far supernodes are relaxed
 (`relax_fill`, `relax_max_width`: fewer, wider supernodes at the price of
 padded zeros). The permutation is never touched: it is the caller's (the
 reference's AMD), and every candidate factors the same matrices to the same
-result up to rounding.
+result up to rounding. The panel-group thresholds tuned here are the FP64
+plan's; the tensor-core (FP32) plan keeps its own (`tc_group4_rows`,
+`tc_group2_rows`), because its grouping sets the FP32 factor's rounding and
+so how many refinement steps the stiffer frequencies of a sweep need: a
+grouping a few per cent faster to factor cost a whole frequency's FP64
+refactorization on the 32^3 sweep.
 
 `tune` builds the analysis for each candidate, times whole factorizations of
 the caller's frequencies on the device (CUDA events on the stream the

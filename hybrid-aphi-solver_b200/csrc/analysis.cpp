@@ -50,8 +50,12 @@ void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing,
     // options, which the autotuner (aphi_b200.autotune) picks per mesh. Only full groups are grouped: the
     // narrow tiles then end exactly at the group's last column, and a front's
     // incomplete last group is updated panel by panel.
-    const int group4 = A.opt.group4_rows > 0 ? A.opt.group4_rows : kGroup4Rows;
-    const int group2 = A.opt.group2_rows > 0 ? A.opt.group2_rows : 0;
+    // The tensor-core plan has thresholds of its own (its grouping sets the
+    // FP32 factor's rounding, which the refinement depends on).
+    const bool tc = trailing == K_UPDATE_TC;
+    const int g4opt = tc ? A.opt.tc_group4_rows : A.opt.group4_rows, g2opt = tc ? A.opt.tc_group2_rows : A.opt.group2_rows;
+    const int group4 = g4opt > 0 ? g4opt : kGroup4Rows;
+    const int group2 = g2opt > 0 ? g2opt : 0;
     for (int L = 0; L < S.num_levels; ++L) {
         const int* lb = S.level_list.data() + S.level_ptr[L];
         const int* le = S.level_list.data() + S.level_ptr[L + 1];

@@ -17,6 +17,8 @@ void aphi_analysis_default_options(aphi_analysis_options* o) {
     o->small_front = 96;
     o->group4_rows = kGroup4Rows;
     o->group2_rows = 0;
+    o->tc_group4_rows = kGroup4Rows;
+    o->tc_group2_rows = 0;
 }
 
 int aphi_analysis_create(int n, const int* row_ptr, const int* col_idx, const int* perm, const int* parent,

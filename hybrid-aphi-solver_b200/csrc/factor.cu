@@ -1012,6 +1012,12 @@ int solve_refined(aphi_factor* f, int nrhs, const double* values, const double* 
     return status;
 }
 
+// COCG steps without a stall_ratio drop of the best relative residual before
+// a system is declared stalled. COCG's residual is not monotone: near
+// rho(I - M^-1 A) ~ 0.9 it can stay above half its best for three steps and
+// still converge a few steps later.
+constexpr int kCocgPatience = 5;
+
 // ---------------------------------------------------------------- Krylov refinement
 // Preconditioned COCG (conjugate orthogonal CG: CG with the unconjugated
 // bilinear form x^T y, valid for complex symmetric A and M) in FP64 on the
@@ -1226,7 +1232,7 @@ int solve_krylov(aphi_factor* f, int nrhs, const double* values, const double* b
             if (rr < opt.stall_ratio * best[k]) {
                 best[k] = rr;
                 since[k] = 0;
-            } else if (++since[k] >= 3 || !(rr == rr)) {
+            } else if (++since[k] >= kCocgPatience || !(rr == rr)) {
                 act[k] = 0;
                 status = APHI_ERR_IR_STALL;
                 continue;

@@ -232,6 +232,13 @@ typedef struct {
     int small_front;       /* fronts up to this many rows use the one-CTA kernel */
     int group4_rows;       /* fronts this tall apply their trailing updates 4 panels at a time (<= 0: 8192) */
     int group2_rows;       /* shorter fronts this tall, 2 panels at a time; shorter still, one (<= 0: all 2) */
+    /* The same two thresholds for the tensor-core (FP32) factorization plan,
+     * kept apart from the FP64 plan's: the grouping changes the FP32
+     * factor's rounding, and with it how many refinement steps the stiffer
+     * systems of a sweep need, or whether they converge at all, so the FP64
+     * plan's grouping can be tuned for speed alone. (<= 0: 8192 / all 2.) */
+    int tc_group4_rows;
+    int tc_group2_rows;
 } aphi_analysis_options;
 
 typedef struct aphi_analysis aphi_analysis;
@@ -353,9 +360,10 @@ int aphi_residuals_noalloc(const aphi_analysis* an, int batch, int nrhs, const d
  * for complex symmetric A), which keeps converging where plain refinement
  * stalls because cond(A) * eps(FP32) approaches 1. A system is done when
  * its backward error <= tol AND its relative residual ||b - A x|| / ||b|| <=
- * rtol; one whose relative residual has not dropped by stall_ratio in 3
- * steps, or that reaches max_iters, is frozen and IR_STALL returned -- the
- * caller's cue to refactorize it in FP64. iters/berr: per batch x rhs. */
+ * rtol; one whose relative residual has not dropped by stall_ratio in 5
+ * COCG steps (its residual is not monotone; plain refinement: in 1 step), or
+ * that reaches max_iters, is frozen and IR_STALL returned -- the caller's cue
+ * to refactorize it in FP64. iters/berr: per batch x rhs. */
 typedef struct {
     int max_iters;
     double tol;               /* target backward error */

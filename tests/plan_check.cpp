@@ -613,6 +613,8 @@ aphi_analysis_options default_options() {
     o.small_front = 96;
     o.group4_rows = kGroup4Rows;
     o.group2_rows = 0;
+    o.tc_group4_rows = kGroup4Rows;
+    o.tc_group2_rows = 0;
     return o;
 }
 
