@@ -295,7 +295,8 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
                 break;
             case K_TC_SPLIT:
                 if constexpr (sizeof(R) == 4)
-                    k_tc_split<<<grid, kTcThreads, 0, st>>>(S, l.first, L, ls, f->tcws, f->tcws_stride, l.kcap);
+                    k_tc_split<<<dim3(grid.x, grid.y, (l.kcap + 8 * kTcK - 1) / (8 * kTcK)), kTcThreads, 0, st>>>(
+                        S, l.first, L, ls, f->tcws, f->tcws_stride, l.kcap);
                 else
                     throw Error(APHI_ERR_INVALID, "operand split planned for an FP64 factor");
                 break;

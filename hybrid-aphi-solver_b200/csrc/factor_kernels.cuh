@@ -656,10 +656,13 @@ __global__ void __launch_bounds__(kTcThreads) k_update_tc(Sched S, long long ite
 // (workspace offset d) holds the A blocks (128 rows) and the B blocks (64
 // rows) in the layout tc_tile_presplit reads (pre_a_off, pre_b_off), each
 // plane in the canonical K-major core-matrix layout; rows past the front and
-// columns past K are zeros. One thread per row.
+// columns past K are zeros. One thread per row; blockIdx.z picks 8 of the
+// stages, so the rows' loads of those 64 columns are all in flight at once.
 __global__ void __launch_bounds__(kTcThreads) k_tc_split(Sched S, long long item0, const cx<float>* Lb,
                                                          long long lstride, unsigned char* ws, long long ws_stride,
                                                          int kcap) {
+    constexpr int kStagesPerCta = 8;  // blockIdx.z: this CTA's stages c0 .. c0 + 7 (64 columns)
+    __shared__ cx<float> piv[kStagesPerCta * kTcK];
     const Item it = S.items[item0 + blockIdx.x];
     const int s = it.s, p0 = it.a, r0 = it.b;
     const int w = S.first[s + 1] - S.first[s];
@@ -667,13 +670,30 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_split(Sched S, long long item
     const int K = min(kcap, w - p0), pe = p0 + K;
     const int R = (m - pe + kTcM - 1) / kTcM * kTcM;
     const int nst = (K + kTcK - 1) / kTcK;
+    const int c0 = blockIdx.z * kStagesPerCta;
+    if (c0 >= nst) return;  // the whole CTA: no barrier follows for it
     unsigned char* region = ws + ws_stride * blockIdx.y + static_cast<long long>(it.d) * 256;
     const cx<float>* P = Lb + lstride * blockIdx.y + S.loff[s];
+    if (threadIdx.x < kStagesPerCta * kTcK) {
+        const int k = c0 * kTcK + threadIdx.x;
+        piv[threadIdx.x] = k < K ? P[(p0 + k) + static_cast<long long>(p0 + k) * m] : cx<float>{0.f, 0.f};
+    }
     const int r = r0 + threadIdx.x;  // row within the trailing part
     const int row = pe + r;
     const bool in = row < m;
+    // The CTA's 64 columns of this row, every load in flight before use.
+    cx<float> v[kStagesPerCta * kTcK];
+#pragma unroll
+    for (int u = 0; u < kStagesPerCta * kTcK; ++u) {
+        const int k = c0 * kTcK + u;
+        v[u] = in && k < K ? P[row + static_cast<long long>(p0 + k) * m] : cx<float>{0.f, 0.f};
+    }
+    __syncthreads();
     const uint32_t oa = plane_off(r & 127, 0), ob = plane_off(r & 63, 0);
-    for (int c = 0; c < nst; ++c) {
+#pragma unroll
+    for (int cc = 0; cc < kStagesPerCta; ++cc) {
+        const int c = c0 + cc;
+        if (c >= nst) break;
         unsigned char* A = region + pre_a_off(R, nst, r, c);
         unsigned char* B = region + pre_b_off(R, nst, r, c);
 #pragma unroll
@@ -681,17 +701,12 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_split(Sched S, long long item
             float ar[4], ai[4], br[4], bi[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const int k = kTcK * c + 4 * h + q;
-                ar[q] = ai[q] = br[q] = bi[q] = 0.f;
-                if (in && k < K) {
-                    const int col = p0 + k;
-                    const cx<float> v = P[row + static_cast<long long>(col) * m];
-                    const cx<float> d = P[col + static_cast<long long>(col) * m];
-                    ar[q] = v.re * d.re - v.im * d.im;
-                    ai[q] = v.re * d.im + v.im * d.re;
-                    br[q] = v.re;
-                    bi[q] = v.im;
-                }
+                const cx<float> x = v[cc * kTcK + 4 * h + q];
+                const cx<float> d = piv[cc * kTcK + 4 * h + q];
+                ar[q] = x.re * d.re - x.im * d.im;
+                ai[q] = x.re * d.im + x.im * d.re;
+                br[q] = x.re;
+                bi[q] = x.im;
             }
             // A: re hi, re lo, im hi, im lo; B per piece: -Bi, Br, Bi
             split_store4<2>(A, kTcPlaneA, oa + h * 128, ar);

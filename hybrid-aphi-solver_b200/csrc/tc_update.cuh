@@ -496,9 +496,13 @@ __device__ bool tc_tile_presplit(unsigned char* smem, const unsigned char* regio
     constexpr int P = Stages;
     constexpr int kStage = TcBytes<2>::stage;
     constexpr int kProducer = 0, kIssuer = 32;
-    // A group's drain waits for each of its stages' commits in turn; each
-    // buffer then holds at most one commit that no thread has waited for yet,
-    // so a parity wait cannot match a phase one round early.
+    // A group's drain waits on its last stage's commit only (s - 1, buffer
+    // (s - 1) % P). That parity wait is exact as long as the buffer's previous
+    // commit (stage s - 1 - P) has already arrived: with Group <= Stages that
+    // stage is no later than the one the previous drain waited for, and a
+    // commit arrives only once every earlier MMA of the issuing thread has
+    // completed, in issue order. (Waiting on each stage of the group in turn
+    // instead measured 1.7x slower on the 32^3 factorization.)
     static_assert(Group <= Stages, "an accumulator group must not span more stages than there are buffers");
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
@@ -550,12 +554,11 @@ __device__ bool tc_tile_presplit(unsigned char* smem, const unsigned char* regio
         const int b = s % P;
         const bool group_start = s % Group == 0;
         if (group_start && s > 0) {
-            // The previous group's main products are complete once its stages'
-            // commits have arrived (waited for in order, the last being s - 1's):
-            // into the running sums before stage s restarts the main accumulator.
-            bool mine = true;
-            for (int p = s - Group; p < s && mine; ++p)
-                mine = mbar_wait_live(smem_u32(empty + p % P), (p / P) & 1, state);
+            // The previous group's main products are complete once stage s - 1's
+            // commit has arrived: into the running sums before stage s
+            // restarts the main accumulator.
+            const int p = s - 1;
+            bool mine = mbar_wait_live(smem_u32(empty + p % P), (p / P) & 1, state);
             mine = __all_sync(0xffffffffu, mine);  // the TMEM loads are warp-wide
             asm volatile("tcgen05.fence::after_thread_sync;");
             if (mine) tc_drain(tmem, sr, si);
