@@ -7,7 +7,10 @@ It builds the workload, the reference's AMD ordering and the supernodal
 analysis on the host, assembles `batch` log-spaced frequencies on the device,
 factorizes them `--reps` times and prints one JSON line: per kind the launches
 and milliseconds of the last factorization, the useful Schur-update flops of
-the plan, and the whole factorization's time.
+the plan, and the whole factorization's time. With `--solves N` it then times
+N solves of the batch's right-hand sides (CUDA events, after one untimed
+solve), one more with per-kind timing, and the solves' algorithmic factor
+traffic (2 nnz(L) values per entry) per millisecond.
 """
 from __future__ import annotations
 
@@ -31,6 +34,7 @@ def main() -> None:
     ap.add_argument("--simt", action="store_true", help="FP32 on the SIMT kernels instead of tcgen05")
     ap.add_argument("--tc-split", type=int, default=3, choices=[2, 3],
                     help="TF32 pieces per operand in the tensor-core update")
+    ap.add_argument("--solves", type=int, default=0, help="also time this many solves of the batch")
     a = ap.parse_args()
     import torch
     if a.simt:
@@ -38,7 +42,7 @@ def main() -> None:
     w = ab.Workload.cylinder(a.cells)
     an = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx))
     asm = ab.Assembly(ab.workload_arrays(w))
-    vals, _ = asm.refill(2 * np.pi * np.geomspace(a.f_lo, a.f_hi, a.batch))
+    vals, rhs = asm.refill(2 * np.pi * np.geomspace(a.f_lo, a.f_hi, a.batch))
     f = ab.Factor(an, precision=a.precision, batch=a.batch)
     if a.precision == 32:
         f.set_tc_split(a.tc_split)
@@ -61,6 +65,24 @@ def main() -> None:
            "kinds": {k: {"launches": n, "ms": t, "useful_flops": plan.get(k, (0, 0, 0.0))[2] * a.batch,
                          "tflops": (plan.get(k, (0, 0, 0.0))[2] * a.batch / (t / 1000.0) / 1e12) if t else None}
                      for k, (n, t) in kinds.items()}}
+    if a.solves > 0:
+        f.profile(False)
+        f.solve(rhs)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.solves):
+            f.solve(rhs)
+        e1.record()
+        torch.cuda.synchronize()
+        sms = e0.elapsed_time(e1) / a.solves
+        f.profile(True, ["fwd_gather", "fwd_diag", "fwd_update", "bwd_update", "bwd_diag"])
+        f.solve(rhs)
+        torch.cuda.synchronize()
+        value_bytes = 16 if a.precision == 64 else 8
+        traffic = 2.0 * an.info["nnz_l"] * value_bytes * a.batch
+        out["solve"] = {"ms": sms, "factor_gb_per_s": traffic / sms / 1e6,
+                        "kinds": {k: {"launches": n, "ms": t} for k, (n, t) in f.profile_read().items()}}
+        f.profile(False)
     print(json.dumps(out))
 
 

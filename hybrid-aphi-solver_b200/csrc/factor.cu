@@ -473,11 +473,18 @@ void solve_numeric(aphi_factor* f, int nrhs, const double* b, double* x, cudaStr
     const dim3 g(ceil_div(std::max(n, 1), 256), f->batch * nrhs);
     k_permute_in<R><<<g, 256, 0, st>>>(n, nrhs, A->d.orig_of_new, f->dscale, b, y);
     APHI_CHECK_LAUNCH();
+    // The fused plans (half the launches, each triangle in the launch before
+    // it) win while one entry is solved; with more, every CTA's reservation of
+    // a triangle's shared memory costs occupancy and the split plans are
+    // faster (32^3, FP32: 15.4 against 15.9 ms for one entry, 30.4 against
+    // 25.4 ms for six).
+    const int rows = entries ? nentries : f->batch;
+    const bool split = f->solve_form == 1 || (f->solve_form < 0 && rows > 1);
     for (int k0 = 0; k0 < nrhs; k0 += 8) {
         const SolveArgs sa{n,       nrhs, k0, std::min(8, nrhs - k0), A->upool, A->max_parts, entries,
                            entries ? nentries : 0, f->counters, A->S.ns};
-        run_plan<R>(f, f->solve_split ? A->plan_fwd_split : A->plan_fwd, st, &sa, y, U, part);
-        run_plan<R>(f, f->solve_split ? A->plan_bwd_split : A->plan_bwd, st, &sa, y, U, part);
+        run_plan<R>(f, split ? A->plan_fwd_split : A->plan_fwd, st, &sa, y, U, part);
+        run_plan<R>(f, split ? A->plan_bwd_split : A->plan_bwd, st, &sa, y, U, part);
     }
     k_permute_out<R><<<g, 256, 0, st>>>(n, nrhs, A->d.new_of_orig, f->dscale, y, x);
     APHI_CHECK_LAUNCH();
@@ -529,7 +536,7 @@ aphi_factor* factor_create(aphi_analysis* an, int precision, int batch) {
         f->counters = dalloc<int>(static_cast<size_t>(std::max(S.ns, 1)) * batch);
         APHI_CUDA(cudaMemset(f->counters, 0, sizeof(int) * std::max(S.ns, 1) * batch));
         const char* split_solve = std::getenv("APHI_SOLVE_SPLIT");
-        f->solve_split = split_solve && split_solve[0] == '1';
+        f->solve_form = split_solve && split_solve[0] == '1' ? 1 : (split_solve && split_solve[0] == '0' ? 0 : -1);
         f->host_stats.assign(batch, aphi_factor_stats{});
     } catch (...) {
         delete f;

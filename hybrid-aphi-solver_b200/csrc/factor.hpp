@@ -46,7 +46,8 @@ struct aphi_factor {
     int* err = nullptr;         // device error word (bounded waits)
     int* kmax = nullptr;        // capacity: the column where each entry's factorization stopped
     int* counters = nullptr;    // fused solve plans: arrival counters, ns per batch entry (zero between launches)
-    bool solve_split = false;   // APHI_SOLVE_SPLIT=1: the solve plans with a launch per triangle
+    int solve_form = -1;        // solve plans: -1 by batch (fused for one entry, split for more), 0 fused, 1 split
+                                // (APHI_SOLVE_SPLIT=0 / 1)
     // Per-kind launch timing (aphi_factor_profile).
     bool profile = false;
     unsigned prof_mask = ~0u;  // kinds (bit k: kind k) timed while profiling
