@@ -1201,6 +1201,7 @@ int solve_krylov(aphi_factor* f, int nrhs, const double* values, const double* b
     k_amax<<<dim3(ceil_div(std::max<long long>(A->S.nnz_a, 1), 256), B), 256, 0, st>>>(values, A->S.nnz_a, amax);
     APHI_CHECK_LAUNCH();
     std::vector<int> act(q, 1), it(q, 0), since(q, 0), ent;
+    std::vector<int> restarted(q, 0), restart_now(q, 0);
     std::vector<double> h(4 * static_cast<size_t>(q)), best(q, INFINITY);
     APHI_CUDA(cudaMemcpyAsync(active, act.data(), sizeof(int) * q, cudaMemcpyHostToDevice, st));
 
@@ -1241,9 +1242,19 @@ int solve_krylov(aphi_factor* f, int nrhs, const double* values, const double* b
                 best[k] = rr;
                 since[k] = 0;
             } else if (++since[k] >= kCocgPatience || !(rr == rr)) {
-                act[k] = 0;
-                status = APHI_ERR_IR_STALL;
-                continue;
+                if (rr == rr && !restarted[k]) {
+                    // Once per system: restart the recurrence from the current
+                    // iterate (p = z, rho = r^T z) before calling it stalled.
+                    // COCG's unconjugated form can stagnate near a breakdown
+                    // of its recurrence that a fresh start avoids.
+                    restarted[k] = restart_now[k] = 1;
+                    since[k] = 0;
+                    best[k] = rr;
+                } else {
+                    act[k] = 0;
+                    status = APHI_ERR_IR_STALL;
+                    continue;
+                }
             }
             if (it[k] >= opt.max_iters) {
                 act[k] = 0;
@@ -1274,6 +1285,11 @@ int solve_krylov(aphi_factor* f, int nrhs, const double* values, const double* b
             started = true;
         } else {
             dot(r, z, 2);
+            for (int k = 0; k < q; ++k)
+                if (restart_now[k]) {  // beta = 0: p = z
+                    APHI_CUDA(cudaMemsetAsync(beta + 2 * k, 0, 2 * sizeof(double), st));
+                    restart_now[k] = 0;
+                }
             k_xpby_sys<<<gv, 256, 0, st>>>(n, active, beta, z, p);
             APHI_CHECK_LAUNCH();
         }

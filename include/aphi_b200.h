@@ -361,8 +361,9 @@ int aphi_residuals_noalloc(const aphi_analysis* an, int batch, int nrhs, const d
  * stalls because cond(A) * eps(FP32) approaches 1. A system is done when
  * its backward error <= tol AND its relative residual ||b - A x|| / ||b|| <=
  * rtol; one whose relative residual has not dropped by stall_ratio in 5
- * COCG steps (its residual is not monotone; plain refinement: in 1 step), or
- * that reaches max_iters, is frozen and IR_STALL returned -- the caller's cue
+ * COCG steps (its residual is not monotone; plain refinement: in 1 step) --
+ * COCG first restarts its recurrence once from the current iterate -- or
+ * that reaches max_iters, is frozen and IR_STALL returned: the caller's cue
  * to refactorize it in FP64. iters/berr: per batch x rhs. */
 typedef struct {
     int max_iters;
