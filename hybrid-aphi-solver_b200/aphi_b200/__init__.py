@@ -918,8 +918,8 @@ class SweepSolver:
 
     overlap=True: entries predicted to need FP64 are factorized and solved on
     a side stream, from a second host thread, while the FP32 entries are
-    being refined (results are the same either way; only the schedule
-    changes).
+    being factorized and refined (results are the same either way; only the
+    schedule changes).
 
     fp64_refine=True refines every FP64-factorized entry (fallbacks included)
     by COCG preconditioned with its own FP64 factor, to the same rtol / tol:
@@ -1088,15 +1088,16 @@ class SweepSolver:
                 todo.append(k)
                 reports[k]["predicted_fp64"] = self.precision == "mixed"
         # Entries known in advance to need FP64 are factorized on a side stream
-        # from a second host thread while the FP32 entries are refined: the
-        # refinement's solves are small, latency-bound launches that leave
-        # most of the device to the FP64 factorization. The two factorizations
-        # share the analysis's workspace and take turns on it; the solves do
-        # not touch it.
+        # from a second host thread while the FP32 entries are factorized and
+        # refined: the FP32 factorization's small in-panel and split launches
+        # and the refinement's latency-bound solves leave much of the device to
+        # the FP64 factorization. Each precision has its own contribution-block
+        # workspace in the analysis, so the two factorizations run at the same
+        # time; the solves do not touch the workspaces.
         side = None
-        side_todo = []
         if self.overlap and todo and fp32_idx:
-            side_todo, todo = todo, []
+            side = self._start_fp64(todo, vals, rhs, stream)
+            todo = []
         for idx in self._chunks(fp32_idx, self.fp32_batch):
             f = self._factor(PREC_FP32, len(idx))
             whole = len(idx) == self.batch
@@ -1105,9 +1106,6 @@ class SweepSolver:
             b = rhs if whole else rhs.index_select(0, sel)
             f.factorize(v, 10, 0.0, stream=stream)
             self.factorized[PREC_FP32] += len(idx)
-            if side_todo and side is None:
-                # after the FP32 factorization has released the workspace
-                side = self._start_fp64(side_todo, vals, rhs, stream)
             xs, iters, berr, _ = f.solve_refined(v, b, tol=self.tol, rtol=self.rtol, max_iters=self.max_iters,
                                                  stream=stream)
             res = residuals(self.analysis, v, xs, b, stream=stream)

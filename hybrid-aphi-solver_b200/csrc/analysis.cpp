@@ -416,7 +416,8 @@ void analysis_info(const aphi_analysis* a, double* info) {
 }  // namespace aphi_b200
 
 aphi_analysis::~aphi_analysis() {
-    if (ws) cudaFree(ws);
+    for (void* w : ws)
+        if (w) cudaFree(w);
     void* ptrs[] = {d.first, d.rows, d.loff, d.cboff, d.soff, d.structs, d.reloff, d.rel, d.child_ptr,
                     d.child_list, d.uoff, d.a_dest, d.row_ptr, d.col_idx, d.new_of_orig, d.orig_of_new,
                     d.ref_of_post, d.fptr, d.fcol, d.fmap, d.items};

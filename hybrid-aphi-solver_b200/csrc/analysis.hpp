@@ -102,9 +102,13 @@ struct aphi_analysis {
     bool on_device = false;
     int device = -1;       // the CUDA device holding the device copy (set with it)
     bool fronts = false;   // built from independent dense fronts (no matrix pattern)
-    void* ws = nullptr;    // contribution-block workspace shared by this analysis's factors
-    size_t ws_bytes = 0;
-    std::mutex ws_mu;      // held while a factorization (or aphi_fronts_read) uses ws
+    // Contribution-block workspaces shared by this analysis's factors, one per
+    // precision ([0] FP64, [1] FP32), so that an FP64 and an FP32
+    // factorization can run at the same time on different streams; each is
+    // held by its lock while a factorization (or aphi_fronts_read) uses it.
+    void* ws[2] = {nullptr, nullptr};
+    size_t ws_bytes[2] = {0, 0};
+    std::mutex ws_mu[2];
     long long num_items = 0;
     long long upool = 0;   // update-vector pool entries (per rhs)
     int max_parts = 1;

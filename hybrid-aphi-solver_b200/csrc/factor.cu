@@ -552,9 +552,10 @@ void fronts_read(const aphi_factor* f, int k, double* panels_out, double* cb_out
     if (!A->fronts) throw Error(APHI_ERR_INVALID, "fronts_read: not a fronts analysis");
     if (k < 0 || k >= f->batch) throw Error(APHI_ERR_BAD_SHAPE, "fronts_read: batch index out of range");
     if (!f->factored) throw Error(APHI_ERR_INVALID, "fronts_read: nothing factorized yet");
-    // The contribution blocks live in the analysis's shared workspace: they
-    // are those of its latest factorization.
-    std::lock_guard<std::mutex> ws_lock(f->an->ws_mu);
+    // The contribution blocks live in the analysis's shared workspace of this
+    // precision: they are those of its latest factorization.
+    const int wi = f->precision == 64 ? 0 : 1;
+    std::lock_guard<std::mutex> ws_lock(f->an->ws_mu[wi]);
     const long long ls = A->S.stored, cs = A->S.cb_pool;
     auto widen = [&](const void* src, long long len, double* dst) {
         if (!dst || len == 0) return;
@@ -565,7 +566,7 @@ void fronts_read(const aphi_factor* f, int k, double* panels_out, double* cb_out
         APHI_CHECK_LAUNCH();
     };
     widen(static_cast<const char*>(f->L) + static_cast<size_t>(ls) * k * f->elem, ls, panels_out);
-    widen(static_cast<const char*>(A->ws) + static_cast<size_t>(cs) * k * f->elem, cs, cb_out);
+    widen(static_cast<const char*>(A->ws[wi]) + static_cast<size_t>(cs) * k * f->elem, cs, cb_out);
     APHI_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -614,26 +615,28 @@ int factorize(aphi_factor* f, const double* values, int equil_iters, double pivo
         APHI_CHECK_LAUNCH();
     }
     // The contribution-block pool is only live during a factorization, so it
-    // is a workspace owned by the analysis and shared by every factor made
-    // from it. A factorization holds the analysis's lock from here until its
-    // stream has finished with the pool (the synchronize below), so
-    // factorizations of one analysis from several host threads, on any
-    // streams, take turns.
-    std::unique_lock<std::mutex> ws_lock(f->an->ws_mu);
+    // is a workspace owned by the analysis and shared by every factor of the
+    // same precision made from it (one pool per precision). A factorization
+    // holds that pool's lock from here until its stream has finished with the
+    // pool (the synchronize below), so factorizations of one precision from
+    // several host threads, on any streams, take turns, while an FP64 and an
+    // FP32 factorization can run at the same time.
+    const int wi = f->precision == 64 ? 0 : 1;
+    std::unique_lock<std::mutex> ws_lock(f->an->ws_mu[wi]);
     {
         aphi_analysis* an = f->an;
         const size_t need = static_cast<size_t>(std::max<long long>(S.cb_pool, 1)) * B * f->elem;
-        if (an->ws_bytes < need) {
-            if (an->ws) {
+        if (an->ws_bytes[wi] < need) {
+            if (an->ws[wi]) {
                 APHI_CUDA(cudaDeviceSynchronize());
-                cudaFree(an->ws);
-                an->ws = nullptr;
-                an->ws_bytes = 0;
+                cudaFree(an->ws[wi]);
+                an->ws[wi] = nullptr;
+                an->ws_bytes[wi] = 0;
             }
-            APHI_CUDA(cudaMalloc(&an->ws, need));
-            an->ws_bytes = need;
+            APHI_CUDA(cudaMalloc(&an->ws[wi], need));
+            an->ws_bytes[wi] = need;
         }
-        f->CB = an->ws;
+        f->CB = an->ws[wi];
     }
     if (f->precision == 64)
         factorize_numeric<double>(f, values, panels, st);
