@@ -563,7 +563,8 @@ class Analysis:
         self.row_ptr, self.col_idx = rp, ci
 
     PLAN_KINDS = ["extend_add", "small_front", "diag_block", "panel_rows", "update_wide", "fwd_gather", "fwd_diag",
-                  "fwd_update", "bwd_update", "bwd_diag", "update_panel", "update_tc", "tc_split"]
+                  "fwd_update", "bwd_update", "bwd_diag", "update_panel", "update_tc", "tc_split",
+                  "dmma_scale"]
 
     def plan_stats(self, plan: int, flops: bool = False) -> dict:
         """{kind: (launches, items)} of launch plan `plan` (0 factorization,

@@ -38,6 +38,9 @@ void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing,
     // trailing-update kernel as 128 x 64 tiles of K = 32, its columns capped
     // at the panel's end; the tensor-core plan keeps the 64 x 64 SIMT tiles.
     const bool panel_wide = trailing == K_UPDATE_WIDE;
+    // Trailing updates whose operands are prepared once per front and panel
+    // group (K_TC_SPLIT / K_DMMA_SCALE launches) rather than inside every tile.
+    const bool staged = trailing == K_UPDATE_TC || trailing == K_UPDATE_WIDE;
     // Panels are grouped for the trailing update: after each panel but a
     // group's last only the group's remaining columns are updated; after its
     // last, the rest of the front with all of the group's panels, so every
@@ -144,32 +147,36 @@ void build_factor_plan(aphi_analysis& A, std::vector<Item>& items, int trailing,
                     for (int j = pe; j < jend; j += kTcN)
                         for (int i = pe; i < m; i += kTcM)
                             if (i + kTcM > j) items.push_back({s, p0, i, j});
-                    if (trailing == K_UPDATE_TC && static_cast<long long>(items.size()) > before) {
+                    if (staged && static_cast<long long>(items.size()) > before) {
                         // The front's trailing operands (rows [pe, m), the group's K
-                        // columns) split once into TF32 planes: a region of the
-                        // launch's workspace, 10 planes x 8-column stages x R rows
-                        // (R = m - pe rounded up to 128), 32 bytes per row and stage.
+                        // columns) prepared once for all of its tiles, in a region of
+                        // the launch's workspace (R = m - pe rounded up to 128):
+                        //  tensor-core plan: split into TF32 planes, 10 planes x
+                        //    8-column stages x R rows, 32 bytes per row and stage;
+                        //  FP64 plan: W = L D, R x K complex128, column-major.
                         const int K = std::min(cap_group * kTcPanel, w - p0);
                         const long long R = (m - pe + kTcM - 1) / kTcM * kTcM;
-                        const long long units = ((K + kTcK - 1) / kTcK) * kTcPlanes * R / 8;
+                        const long long units = trailing == K_UPDATE_TC ? ((K + kTcK - 1) / kTcK) * kTcPlanes * R / 8
+                                                                        : R * K / 16;
                         for (long long t = before; t < static_cast<long long>(items.size()); ++t)
                             items[t].d = static_cast<int>(region);
                         split_fronts.push_back({s, p0, pe, static_cast<int>(region)});
                         region += units;
                         if (region > 0x7fffffffLL)
-                            throw Error(APHI_ERR_BAD_SHAPE, "pre-split workspace of one launch exceeds 512 GiB");
+                            throw Error(APHI_ERR_BAD_SHAPE, "the prepared operands of one launch exceed 512 GiB");
                     }
                 }
-                if (trailing == K_UPDATE_TC && count_since(f0) > 0) {
-                    // The split of every front of the launch runs just before it.
+                if (staged && count_since(f0) > 0) {
+                    // The operand launch of every front of the launch runs just before it.
                     std::vector<Item> upd(items.begin() + f0, items.end());
                     items.resize(f0);
                     for (const auto& sf : split_fronts) {
                         const int m = S.sn_rows[sf.s];
                         for (int r0 = 0; r0 < m - sf.pe; r0 += kTcM) items.push_back({sf.s, sf.p0, r0, 0, sf.d});
                     }
-                    push(K_TC_SPLIT, f0, cap_group * kTcPanel);
-                    A.tc_ws_units = std::max(A.tc_ws_units, region);
+                    push(trailing == K_UPDATE_TC ? K_TC_SPLIT : K_DMMA_SCALE, f0, cap_group * kTcPanel);
+                    long long& units_max = trailing == K_UPDATE_TC ? A.tc_ws_units : A.dmma_ws_units;
+                    units_max = std::max(units_max, region);
                     f0 = static_cast<long long>(items.size());
                     items.insert(items.end(), upd.begin(), upd.end());
                 }

@@ -30,6 +30,7 @@ enum Kind : int {
     K_UPDATE_PANEL = 10,  // (s, k0, i0, j0): update tile restricted to the current 128-column panel
     K_UPDATE_TC = 11,     // (s, p0, i0, j0, d): tensor-core trailing update by a whole panel
     K_TC_SPLIT = 12,      // (s, p0, r0, d): a front's trailing operands split into TF32 planes, 128 rows
+    K_DMMA_SCALE = 13,    // (s, p0, r0, d): a front's trailing rows scaled by the group's pivots (W = L D), 128 rows
 };
 
 struct Launch {
@@ -43,7 +44,8 @@ struct Launch {
 
 struct Item {
     int s, a, b, c;
-    int d = 0;  // K_UPDATE_TC / K_TC_SPLIT: the front's plane region, in 256-byte units of an entry's workspace
+    int d = 0;  // staged trailing updates and their operand launches: the front's region, in 256-byte units
+                // of an entry's workspace (K_UPDATE_TC / K_TC_SPLIT; K_UPDATE_WIDE / K_DMMA_SCALE)
 };
 
 constexpr int kStep = 32;        // pivot block width of the blocked factorization
@@ -114,7 +116,8 @@ struct aphi_analysis {
     int max_parts = 1;
     long long stat_first = 0;  // items of the statistics pass (s, col0)
     int stat_count = 0;     // partial-sum slots of the largest backward update launch
-    long long tc_ws_units = 0;  // split-operand workspace of the tensor-core plan, per entry (256-byte units)
+    long long tc_ws_units = 0;    // split-operand workspace of the tensor-core plan, per entry (256-byte units)
+    long long dmma_ws_units = 0;  // scaled-operand (W = L D) workspace of the FP64 plan, per entry (256-byte units)
     long long device_bytes = 0;
     ~aphi_analysis();
 };

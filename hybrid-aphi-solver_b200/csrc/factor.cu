@@ -261,9 +261,13 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
     const bool presplit = sizeof(R) == 4 && f->tc_split == 2 && f->presplit && f->tcws;
     const size_t tri_smem = kTriSmem * sizeof(cx<R>);               // forward triangles
     const size_t bwd_smem = (kTriSmem + kRedSmem) * sizeof(cx<R>);  // backward triangles
+    // FP64 trailing updates on pre-scaled operands (W = L D per panel group).
+    const bool prescaled = sizeof(R) == 8 && f->dws;
     for (const Launch& l : plan) {
-        // Without pre-split operands the tile splits them itself: no split launch.
+        // Without pre-split (pre-scaled) operands the tile splits (scales) them
+        // itself: no operand launch.
         if (l.kind == K_TC_SPLIT && !presplit) continue;
+        if (l.kind == K_DMMA_SCALE && !prescaled) continue;
         dim3 grid(l.count, sa && sa->ny > 0 ? sa->ny : f->batch);
         const bool timed = prof && ((f->prof_mask >> l.kind) & 1u);
         if (timed) {
@@ -286,12 +290,23 @@ void run_plan(const aphi_factor* f, const std::vector<Launch>& plan, cudaStream_
                     k_update_panel<R><<<grid, 256, 2 * kStep * kTile * sizeof(cx<R>), st>>>(S, l.first, L, CB, ls, cs);
                     break;
                 }
-                if constexpr (sizeof(R) == 8)
-                    k_update_wide_dmma<<<grid, 256, kDmmaSmem, st>>>(S, l.first, L, CB, ls, cs, l.kcap,
-                                                                    l.kind == K_UPDATE_PANEL ? 1 : 0);
-                else
+                if constexpr (sizeof(R) == 8) {
+                    if (l.kind == K_UPDATE_WIDE && prescaled)
+                        k_update_wide_dmma<true><<<grid, 256, kDmmaSmem, st>>>(S, l.first, L, CB, ls, cs, l.kcap, 0,
+                                                                              f->dws, f->dws_stride);
+                    else
+                        k_update_wide_dmma<false><<<grid, 256, kDmmaSmem, st>>>(
+                            S, l.first, L, CB, ls, cs, l.kcap, l.kind == K_UPDATE_PANEL ? 1 : 0, nullptr, 0);
+                } else
                     k_update_wide<R><<<grid, 256, wide_smem<R>(), st>>>(S, l.first, L, CB, ls, cs, l.kcap,
                                                                       l.kind == K_UPDATE_PANEL ? 1 : 0);
+                break;
+            case K_DMMA_SCALE:
+                if constexpr (sizeof(R) == 8)
+                    k_dmma_scale<<<dim3(grid.x, grid.y, (l.kcap + 63) / 64), 128, 0, st>>>(S, l.first, L, ls, f->dws,
+                                                                                         f->dws_stride, l.kcap);
+                else
+                    throw Error(APHI_ERR_INVALID, "operand scaling planned for an FP32 factor");
                 break;
             case K_TC_SPLIT:
                 if constexpr (sizeof(R) == 4)
@@ -379,8 +394,12 @@ void set_smem_limits(int small_front) {
     APHI_CUDA(cudaFuncSetAttribute(k_update_panel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    2 * kStep * kTile * static_cast<int>(sizeof(cx<R>))));
     APHI_CUDA(cudaFuncSetAttribute(k_update_wide<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, wide_smem<R>()));
-    if constexpr (sizeof(R) == 8)
-        APHI_CUDA(cudaFuncSetAttribute(k_update_wide_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, kDmmaSmem));
+    if constexpr (sizeof(R) == 8) {
+        APHI_CUDA(cudaFuncSetAttribute(k_update_wide_dmma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kDmmaSmem));
+        APHI_CUDA(cudaFuncSetAttribute(k_update_wide_dmma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kDmmaSmem));
+    }
     if constexpr (sizeof(R) == 4)
         APHI_CUDA(cudaFuncSetAttribute(k_update_tc<3, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        TcSmem<3, 2>::bytes));
@@ -523,6 +542,11 @@ aphi_factor* factor_create(aphi_analysis* an, int precision, int batch) {
         if (precision == 32 && an->tc_ws_units > 0) {
             f->tcws_stride = an->tc_ws_units * 256;
             APHI_CUDA(cudaMalloc(&f->tcws, static_cast<size_t>(f->tcws_stride) * batch));
+        }
+        const char* psc = std::getenv("APHI_DMMA_PRESCALE");
+        if (precision == 64 && an->dmma_ws_units > 0 && !(psc && psc[0] == '0')) {
+            f->dws_stride = an->dmma_ws_units * 256;
+            APHI_CUDA(cudaMalloc(&f->dws, static_cast<size_t>(f->dws_stride) * batch));
         }
         const Symbolic& S = an->S;
         APHI_CUDA(cudaMalloc(&f->L, static_cast<size_t>(std::max<long long>(S.stored, 1)) * batch * f->elem));
@@ -1398,7 +1422,7 @@ void factor_export(const aphi_factor* f, int k, int* col_ptr, int* row_index, do
 aphi_factor::~aphi_factor() {
     for (cudaEvent_t e : prof_events) cudaEventDestroy(e);
     void* ptrs[] = {L, dscale, rowmax, stats, dref, y, U, part, ir, red, norms, kr, err, kmax, hvals, hvec, tcws,
-                    counters};
+                    counters, dws};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }

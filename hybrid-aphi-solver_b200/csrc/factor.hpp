@@ -41,6 +41,8 @@ struct aphi_factor {
     int tc_group = 2;           // split 2: stages per fresh main accumulator (2 or 4; APHI_TC_GROUP)
     bool presplit = true;       // split 2: operands split once per panel group (k_tc_split; APHI_TC_PRESPLIT=0: in the tile)
     int pre_stages = 3;         // plane buffers of the pre-split tile (APHI_TC_PRESTAGES=4: four; always four with tc_group 4)
+    unsigned char* dws = nullptr;  // FP64: the trailing updates' scaled operands W = L D, dws_stride bytes per entry
+    long long dws_stride = 0;      // (APHI_DMMA_PRESCALE=0: scaled inside every tile instead)
     unsigned char* tcws = nullptr;  // the pre-split operand planes, tcws_stride bytes per entry (capacity entries)
     long long tcws_stride = 0;
     int* err = nullptr;         // device error word (bounded waits)

@@ -492,9 +492,60 @@ __device__ __forceinline__ void red_sub(double* p, double v) {
     asm volatile("red.global.add.f64 [%0], %1;" ::"l"(p), "d"(-v) : "memory");
 }
 
+// K_DMMA_SCALE item (s, p0, r0, d): rows pe + r0 .. pe + r0 + 127 of front
+// s's trailing part (pe = p0 + K) times the group's pivots, W[r, k] =
+// L[pe + r, p0 + k] D[k] (the product the tile forms for its A operand, in
+// the same order), into region d: column-major, leading dimension R (the
+// trailing rows rounded up to 128); rows past the front are zeros. One thread
+// per row; blockIdx.z picks 64 of the K columns, whose loads are all in
+// flight at once.
+__global__ void __launch_bounds__(128) k_dmma_scale(Sched S, long long item0, const cx<double>* Lb,
+                                                    long long lstride, unsigned char* ws, long long ws_stride,
+                                                    int kcap) {
+    constexpr int kCols = 64;
+    __shared__ cx<double> piv[kCols];
+    const Item it = S.items[item0 + blockIdx.x];
+    const int s = it.s, p0 = it.a, r0 = it.b;
+    const int w = S.first[s + 1] - S.first[s];
+    const int m = S.rows[s];
+    const int K = min(kcap, w - p0), pe = p0 + K;
+    const long long R = (m - pe + kTcM - 1) / kTcM * kTcM;
+    const int k0 = blockIdx.z * kCols;
+    if (k0 >= K) return;  // the whole CTA: no barrier follows for it
+    cx<double>* W = reinterpret_cast<cx<double>*>(ws + ws_stride * blockIdx.y + static_cast<long long>(it.d) * 256);
+    const cx<double>* P = Lb + lstride * blockIdx.y + S.loff[s];
+    if (threadIdx.x < kCols) {
+        const int k = k0 + threadIdx.x;
+        piv[threadIdx.x] = k < K ? P[(p0 + k) + static_cast<long long>(p0 + k) * m] : cx<double>{0, 0};
+    }
+    const int r = r0 + threadIdx.x;  // row within the trailing part
+    const int row = pe + r;
+    const bool in = row < m;
+    __syncthreads();
+#pragma unroll 2
+    for (int c = 0; c < kCols; c += 32) {
+        cx<double> v[32];
+#pragma unroll
+        for (int u = 0; u < 32; ++u) {
+            const int k = k0 + c + u;
+            v[u] = in && k < K ? P[row + static_cast<long long>(p0 + k) * m] : cx<double>{0, 0};
+        }
+#pragma unroll
+        for (int u = 0; u < 32; ++u) {
+            const int k = k0 + c + u;
+            if (k < K) W[r + k * R] = v[u] * piv[c + u];
+        }
+    }
+}
+
+// Pre: the A operand comes scaled (W = L D, written by the launch's
+// k_dmma_scale into workspace region it.d), so the tile only moves it; without
+// it the A fragments are scaled by the pivots as they are read.
+template <bool Pre>
 __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long item0, cx<double>* Lb,
                                                           cx<double>* CBb, long long lstride, long long cbstride,
-                                                          int kcap, int panel) {
+                                                          int kcap, int panel, const unsigned char* ws,
+                                                          long long ws_stride) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<double>* Ds = reinterpret_cast<cx<double>*>(smem_raw);  // [kWidePair] pivots of the group's panels
     cx<double>* Ring = Ds + kWidePair;                           // [stage][A: KC x ldA | B: KC x ldB]
@@ -510,6 +561,13 @@ __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long ite
     cx<double>* CBs = CB + (cs > 0 ? S.cboff[s] : 0);
     const cx<double>* P = Ls + static_cast<long long>(p0) * m;
     const cx<double>* dg = Ls + p0 + static_cast<long long>(p0) * m;
+    // The A operand: W's rows i0 - pe .. (leading dimension R), or the panel's.
+    const int pe = p0 + K;
+    const long long ldw = Pre ? static_cast<long long>(m - pe + kTcM - 1) / kTcM * kTcM : m;
+    const cx<double>* PA =
+        Pre ? reinterpret_cast<const cx<double>*>(ws + ws_stride * blockIdx.y + static_cast<long long>(it.d) * 256) +
+                  (i0 - pe)
+            : P + i0;
     const int tid = threadIdx.x;
     const uint32_t ring = smem_u32(Ring);
     // Chunk c: panel columns 16c.. of rows i0.. (A, 128 rows) and j0.. (B, 64).
@@ -521,7 +579,7 @@ __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long ite
         for (int q = 0; q < kDmmaKC * kWideM / 256; ++q) {
             const int e = tid + 256 * q, k = e / kWideM, r = e % kWideM;
             const bool in = kbase + k < K && i0 + r < m;
-            cp_async16(sa + (k * kDmmaLdA + r) * 16, in ? P + static_cast<long long>(kbase + k) * m + i0 + r : P,
+            cp_async16(sa + (k * kDmmaLdA + r) * 16, in ? PA + static_cast<long long>(kbase + k) * ldw + r : P,
                        in ? 16u : 0u);
         }
 #pragma unroll
@@ -545,7 +603,8 @@ __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long ite
     cp_async_commit();
     if (nc > 1) fetch(1);
     cp_async_commit();
-    for (int t = tid; t < kWidePair; t += 256) Ds[t] = t < K ? dg[static_cast<long long>(t) * (m + 1)] : cx<double>{0, 0};
+    if constexpr (!Pre)
+        for (int t = tid; t < kWidePair; t += 256) Ds[t] = t < K ? dg[static_cast<long long>(t) * (m + 1)] : cx<double>{0, 0};
     for (int c = 0; c < nc; ++c) {
         cp_async_wait<1>();  // this thread's copies of chunk c have landed
         __syncthreads();     // everyone's have; everyone is done with chunk c - 1
@@ -555,10 +614,15 @@ __global__ void __launch_bounds__(256) k_update_wide_dmma(Sched S, long long ite
         const cx<double>* B = A + kDmmaKC * kDmmaLdA;
 #pragma unroll
         for (int ks = 0; ks < kDmmaKC; ks += 4) {
-            const cx<double> d = Ds[c * kDmmaKC + ks + t4];
             cx<double> af[4], bf[4];
+            if constexpr (Pre) {
 #pragma unroll
-            for (int a = 0; a < 4; ++a) af[a] = A[(ks + t4) * kDmmaLdA + 32 * wm + 8 * a + g] * d;
+                for (int a = 0; a < 4; ++a) af[a] = A[(ks + t4) * kDmmaLdA + 32 * wm + 8 * a + g];
+            } else {
+                const cx<double> d = Ds[c * kDmmaKC + ks + t4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) af[a] = A[(ks + t4) * kDmmaLdA + 32 * wm + 8 * a + g] * d;
+            }
 #pragma unroll
             for (int b = 0; b < 4; ++b) bf[b] = B[(ks + t4) * kDmmaLdB + 32 * wn + 8 * b + g];
             // One real product over all 16 blocks before the next, so that

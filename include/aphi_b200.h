@@ -443,11 +443,12 @@ int aphi_fronts_read(const aphi_factor* f, int k, double* panels_dev, double* cb
  * 5-9 solve kernels (gather, forward diagonal, forward update, backward
  * update, backward diagonal), 10 panel-restricted update tile, 11
  * tensor-core update tile, 12 the operand split into TF32 planes that the
- * two-piece tensor-core tile reads. useful[k] (may be NULL): the real flops of the
+ * two-piece tensor-core tile reads, 13 the FP64 trailing update's operand
+ * scaled by its pivots (W = L D) once per panel group. useful[k] (may be NULL): the real flops of the
  * update kinds' Schur-complement work, counting only lower-triangle entries
  * (8 per complex multiply-add); executed[k] (may be NULL): the flops their
  * tiles perform, padding included. */
-#define APHI_PLAN_KINDS 13
+#define APHI_PLAN_KINDS 14
 int aphi_analysis_plan_stats(const aphi_analysis* a, int plan, int64_t* launches, int64_t* items, double* useful,
                              double* executed);
 

@@ -267,30 +267,34 @@ void update_tile(Fronts& F, int s, int c, int K, int i0, int j0, int tm, int tn,
     }
 }
 
-// The pre-split workspace. A K_TC_SPLIT item writes 128 rows of every stage's
-// ten planes of its front's region: the region must lie inside the
-// per-entry workspace, the regions of different fronts in one launch must not
-// overlap, and one front's items must agree on it. The K_UPDATE_TC launch that
-// follows reads, per tile, A rows i0 - pe .. +127 and B rows j0 - pe .. +63 of
-// its front's region: the launch just before it must be a split launch that
-// wrote those rows of that region, for the same panel group.
-long long g_tc_ws_units = 0;
+// The prepared-operand workspaces. A K_TC_SPLIT item writes 128 rows of
+// every stage's ten planes of its front's region (tensor-core plan); a
+// K_DMMA_SCALE item writes 128 rows of W = L D over the group's K columns
+// (FP64 plan). The region must lie inside the per-entry workspace, the regions
+// of different fronts in one launch must not overlap, and one front's items
+// must agree on it. The trailing-update launch that follows reads, per tile,
+// rows i0 - pe .. +127 (and, for the split planes, B rows j0 - pe .. +63) of
+// its front's region: the launch just before it must be the operand launch
+// that wrote those rows of that region, for the same panel group and K.
+long long g_tc_ws_units = 0, g_dmma_ws_units = 0;
 struct SplitFront {
     long long d, units;
-    int p0;
+    int p0, K;
     std::vector<char> rows;  // 128-row blocks written
 };
 std::map<int, SplitFront> g_split;
-int g_split_launch = -1;  // ck.launch of the last split launch
+int g_split_launch = -1;  // ck.launch of the last operand launch
 
-void tc_split_region(Fronts& F, const Launch& l, const Item& it, int w) {
+void operand_region(Fronts& F, const Launch& l, const Item& it, int w) {
     const int m = F.rows(it.s);
     const int K = std::min(l.kcap, w - it.a), pe = it.a + K;
     const long long R = (m - pe + kTcM - 1) / kTcM * kTcM;
-    const long long units = ((K + kTcK - 1) / kTcK) * kTcPlanes * R / 8;
-    if (it.d < 0 || it.d + units > g_tc_ws_units || it.b < 0 || it.b >= R || it.b % kTcM) {
+    const bool tc = l.kind == K_TC_SPLIT;
+    const long long units = tc ? ((K + kTcK - 1) / kTcK) * kTcPlanes * R / 8 : R * K / 16;
+    const long long cap = tc ? g_tc_ws_units : g_dmma_ws_units;
+    if (it.d < 0 || it.d + units > cap || it.b < 0 || it.b >= R || it.b % kTcM) {
         ++F.ck.bounds;
-        F.ck.report("tc split region outside the workspace", "d", it.d);
+        F.ck.report("operand region outside the workspace", "d", it.d);
         return;
     }
     auto found = g_split.find(it.s);
@@ -298,53 +302,57 @@ void tc_split_region(Fronts& F, const Launch& l, const Item& it, int w) {
         for (const auto& kv : g_split)
             if (it.d < kv.second.d + kv.second.units && kv.second.d < it.d + units) {
                 ++F.ck.ww;
-                F.ck.report("tc split regions of two fronts overlap", "d", it.d);
+                F.ck.report("operand regions of two fronts overlap", "d", it.d);
             }
-        found = g_split.emplace(it.s, SplitFront{it.d, units, it.a, std::vector<char>(R / kTcM, 0)}).first;
+        found = g_split.emplace(it.s, SplitFront{it.d, units, it.a, K, std::vector<char>(R / kTcM, 0)}).first;
     } else if (found->second.d != it.d || found->second.p0 != it.a) {
         ++F.ck.bounds;
-        F.ck.report("tc split items of one front disagree on the region", "d", it.d);
+        F.ck.report("operand items of one front disagree on the region", "d", it.d);
         return;
     }
     char& blk = found->second.rows[it.b / kTcM];
     if (blk) {
         ++F.ck.ww;
-        F.ck.report("tc split row block written twice", "row", it.b);
+        F.ck.report("operand row block written twice", "row", it.b);
     }
     blk = 1;
 }
 
-// A K_UPDATE_TC tile of a plan with split launches reads only planes that the
-// split launch just before it wrote.
-void tc_tile_region(Fronts& F, const Launch& l, const Item& it, int w) {
+// A trailing-update tile of a plan with operand launches reads only rows that
+// the operand launch just before it wrote (B rows too for the split planes).
+void tile_region(Fronts& F, const Launch& l, const Item& it, int w) {
     const int K = std::min(l.kcap, w - it.a), pe = it.a + K;
     const auto found = g_split.find(it.s);
     const bool fresh = g_split_launch == F.ck.launch - 1;
-    bool ok = fresh && found != g_split.end() && found->second.d == it.d && found->second.p0 == it.a;
+    bool ok = fresh && found != g_split.end() && found->second.d == it.d && found->second.p0 == it.a &&
+              found->second.K == K;
     if (ok) {
         const std::vector<char>& rows = found->second.rows;
         const int ia = (it.b - pe) / kTcM, jb = (it.c - pe) / kTcM;
-        ok = it.b >= pe && it.c >= pe && ia < static_cast<int>(rows.size()) && jb < static_cast<int>(rows.size()) &&
-             rows[ia] && rows[jb];
+        ok = it.b >= pe && it.c >= pe && ia < static_cast<int>(rows.size()) && rows[ia] &&
+             (l.kind != K_UPDATE_TC || (jb < static_cast<int>(rows.size()) && rows[jb]));
     }
     if (!ok) {
         ++F.ck.rw;
-        F.ck.report("tc tile reads planes its split launch did not write", "row", it.b);
+        F.ck.report("trailing tile reads operands its operand launch did not write", "row", it.b);
     }
 }
 
 void run_factor_plan(Fronts& F, const std::vector<Launch>& plan, const std::vector<Item>& items) {
     static const char* names[] = {"extend_add", "small", "diag", "trsm", "update_wide", "", "", "", "", "",
-                                  "update_panel", "update_tc", "tc_split"};
+                                  "update_panel", "update_tc", "tc_split", "dmma_scale"};
     Checker& ck = F.ck;
-    const bool presplit = std::any_of(plan.begin(), plan.end(), [](const Launch& l) { return l.kind == K_TC_SPLIT; });
+    auto has = [&](int kind) {
+        return std::any_of(plan.begin(), plan.end(), [&](const Launch& l) { return l.kind == kind; });
+    };
+    const bool presplit = has(K_TC_SPLIT), prescaled = has(K_DMMA_SCALE);
     g_split.clear();
     g_split_launch = -1;
     for (const Launch& l : plan) {
         ++ck.launch;
         ++ck.launches;
-        ck.kind = l.kind >= 0 && l.kind < 13 ? names[l.kind] : "?";
-        if (l.kind == K_TC_SPLIT) {
+        ck.kind = l.kind >= 0 && l.kind < 14 ? names[l.kind] : "?";
+        if (l.kind == K_TC_SPLIT || l.kind == K_DMMA_SCALE) {
             g_split.clear();
             g_split_launch = ck.launch;
         }
@@ -370,15 +378,17 @@ void run_factor_plan(Fronts& F, const std::vector<Launch>& plan, const std::vect
                 case K_UPDATE_WIDE:
                 case K_UPDATE_TC: {
                     const int K = std::min(l.kcap, w - it.a);
-                    if (l.kind == K_UPDATE_TC && presplit) tc_tile_region(F, l, it, w);
+                    if ((l.kind == K_UPDATE_TC && presplit) || (l.kind == K_UPDATE_WIDE && prescaled))
+                        tile_region(F, l, it, w);
                     update_tile(F, it.s, it.a, K, it.b, it.c, kTcM, kTcN, F.rows(it.s));
                     break;
                 }
                 case K_TC_SPLIT:
-                    // A copy of the panel's operands into the split-plane workspace:
-                    // the arithmetic is the tiles' (update_tile). Its region must lie
+                case K_DMMA_SCALE:
+                    // The panel group's operands prepared in the workspace: the
+                    // arithmetic is the tiles' (update_tile). The region must lie
                     // inside the analysis's per-entry workspace.
-                    tc_split_region(F, l, it, w);
+                    operand_region(F, l, it, w);
                     break;
                 default:
                     ++ck.bounds;
@@ -597,7 +607,7 @@ bool plant_mistake(aphi_analysis& A, const std::string& what) {
             }
     } else if (what == "kcap") {
         for (Launch& l : A.plan_factor)
-            if (l.kcap > kTcPanel) {
+            if (l.kind == K_UPDATE_WIDE && l.kcap > kTcPanel) {
                 l.kcap = kTcPanel;
                 return true;
             }
@@ -728,6 +738,7 @@ int check_matrix(int n, const std::vector<int>& rp, const std::vector<int>& ci, 
     }
     int bad = 0;
     g_tc_ws_units = A->tc_ws_units;
+    g_dmma_ws_units = A->dmma_ws_units;
     const std::vector<Launch>* plans[2] = {&A->plan_factor, &A->plan_factor_tc};
     const char* pname[2] = {"dmma", "tc"};
     for (int p = 0; p < 2; ++p) {
@@ -809,6 +820,8 @@ int check_fronts(unsigned seed, int count, int max_rows) {
                 ck.wr(F.L, S.sn_loff[s] + i + static_cast<long long>(j) * m, v, 0, S.stored);
             }
     }
+    g_tc_ws_units = A->tc_ws_units;
+    g_dmma_ws_units = A->dmma_ws_units;
     run_factor_plan(F, A->plan_factor, A->h_items);
     double err = 0;
     for (int s = 0; s < S.ns; ++s) {
