@@ -324,6 +324,44 @@ def test_fused_solve_plans_equal_split_ones_bit_for_bit(precision, cuda):
     assert an.plan_stats(2).get("fwd_diag") is None and an.plan_stats(3).get("bwd_diag") is None
 
 
+def test_prescaled_fp64_operand_matches_the_in_tile_scaling(cuda):
+    """The FP64 trailing update on W = L D written once per panel group
+    (k_dmma_scale) against the tile scaling its own A fragments
+    (APHI_DMMA_PRESCALE=0): the same products, rounded in another kernel, so
+    both solve to a relative residual <= 1e-12 and their solutions agree to
+    1e-9 (cond(A) eps: the systems' conditioning grows with frequency); the
+    scale launches run only in the first."""
+    import os
+    w = ab.Workload.cylinder(16)
+    an = ab.Analysis(w.row_ptr, w.col_idx, ab.amd_ordering(w.row_ptr, w.col_idx))
+    assert an.plan_stats(0).get("dmma_scale", (0, 0))[0] > 0
+    asm = ab.Assembly(ab.workload_arrays(w))
+    vals, rhs = asm.refill(2 * np.pi * np.array([50.0, 1e4]))
+    saved = os.environ.get("APHI_DMMA_PRESCALE")
+    xs, launches = [], []
+    try:
+        for pre in ("1", "0"):
+            os.environ["APHI_DMMA_PRESCALE"] = pre
+            f = ab.Factor(an, precision=ab.PREC_FP64, batch=2)
+            f.profile(True)
+            assert f.factorize(vals)
+            launches.append(f.profile_read().get("dmma_scale", (0, 0.0))[0])
+            f.profile(False)
+            x = f.solve(rhs)
+            res = ab.residuals(an, vals, x, rhs)
+            assert (res[:, 0, 0] <= 1e-12).all(), res
+            xs.append(x.cpu().numpy())
+            f.close()
+    finally:
+        if saved is None:
+            os.environ.pop("APHI_DMMA_PRESCALE", None)
+        else:
+            os.environ["APHI_DMMA_PRESCALE"] = saved
+    assert launches[0] > 0 and launches[1] == 0
+    for k in range(2):
+        assert np.linalg.norm(xs[0][k] - xs[1][k]) <= 1e-9 * np.linalg.norm(xs[1][k])
+
+
 def test_factor_profile_counts_every_planned_launch(cuda):
     """aphi_factor_profile: one factorization with timing on records exactly
     the launches its plan holds, per kind, with positive durations. The
