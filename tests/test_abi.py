@@ -81,6 +81,14 @@ def test_plan_stats_account_for_the_same_update_work():
     # the trailing and in-panel updates carry (almost) all of the factorization's flops
     total = simt["update_wide"][2] + simt["update_panel"][2]
     assert 0.9 * an.info["flops"] <= total <= 1.5 * an.info["flops"]
+    # every trailing-update launch is preceded by its operand launch (W = L D in
+    # the FP64 plan, the TF32 planes in the tensor-core plan), with one item per
+    # 128 trailing rows of each front and no flops of its own
+    assert simt["dmma_scale"][0] == simt["update_wide"][0]
+    assert tc["tc_split"][0] == tc["update_tc"][0]
+    assert simt["dmma_scale"][1] == tc["tc_split"][1]
+    assert simt["dmma_scale"][2] == 0 and tc["tc_split"][2] == 0
+    assert "tc_split" not in simt and "dmma_scale" not in tc
 
 
 def _small_pattern():
