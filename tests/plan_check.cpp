@@ -575,7 +575,8 @@ double rel_err(const std::vector<C>& a, const std::vector<C>& b) {
 // checks catch it: two live CBs placed on one another ("overlap"), a tile
 // updated by two items of one launch ("dup"), a child's extend-add map
 // entry repeated ("rel"), a 2-panel group's trailing update cut to its last
-// panel ("kcap").
+// panel ("kcap"), a trailing tile pointed at another part of the prepared-
+// operand workspace than its operand launch wrote ("region").
 bool plant_mistake(aphi_analysis& A, const std::string& what) {
     Symbolic& S = A.S;
     auto cb_rows = [&](int s) { return S.sn_rows[s] - (S.sn_first[s + 1] - S.sn_first[s]); };
@@ -611,6 +612,15 @@ bool plant_mistake(aphi_analysis& A, const std::string& what) {
                 l.kcap = kTcPanel;
                 return true;
             }
+    } else if (what == "region") {
+        bool staged = false;  // the launch before was an operand launch
+        for (const Launch& l : A.plan_factor) {
+            if (l.kind == K_UPDATE_WIDE && staged) {
+                A.h_items[l.first].d += 16;
+                return true;
+            }
+            staged = l.kind == K_DMMA_SCALE;
+        }
     }
     return false;
 }

@@ -83,6 +83,7 @@ def test_edge_patterns_replay_clean(plan_check, build, shape, n, seed, order):
     ("dup", r"ww [1-9]"),                             # one tile updated by two items of a launch
     ("rel", r"bounds [1-9]"),                         # a child's map repeats a row
     ("kcap", r"d_err [1-9]\.\d+e-0[1-6]"),            # a 2-panel group applied as one panel
+    ("region", r"rw [1-9]"),                          # a tile reading operands nobody wrote for it
 ])
 def test_planted_mistakes_are_caught(plan_check, mistake, caught):
     r = plan_check("plan_check", "cylinder", 8, mistake)
