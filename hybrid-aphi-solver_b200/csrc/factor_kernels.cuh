@@ -180,9 +180,14 @@ __global__ void __launch_bounds__(256) k_small_front(Sched S, long long item0, c
 }
 
 // ---------------------------------------------------------------- blocked fronts
-// Step k0 of a large front: factor the kb x kb diagonal block in place.
+// Step k0 of a large front: factor the kb x kb diagonal block in place. The
+// block is staged with every thread's loads in flight. At step k warp v
+// updates columns k + 1 + v, k + 5 + v, ... and lane l the entry l rows below
+// each column's diagonal (the lower triangle only, no index division); each
+// entry gets the same arithmetic, in the same order of k, as before.
 template <class R>
 __global__ void __launch_bounds__(128) k_diag_block(Sched S, long long item0, cx<R>* Lb, long long lstride) {
+    static_assert(kStep == 32 && kStep * kStep % 128 == 0, "one lane per row, eight entries per thread");
     __shared__ cx<R> F[kStep * kStep];
     const Item it = S.items[item0 + blockIdx.x];
     const int s = it.s, k0 = it.a;
@@ -191,25 +196,32 @@ __global__ void __launch_bounds__(128) k_diag_block(Sched S, long long item0, cx
     const int m = S.rows[s];
     const int kb = min(kStep, w - k0);
     cx<R>* D = L + S.loff[s] + k0 + static_cast<long long>(k0) * m;
-    for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
-        const int i = e % kb, j = e / kb;
-        F[i + j * kStep] = D[i + static_cast<long long>(j) * m];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    {
+        cx<R> v[kStep * kStep / 128];
+#pragma unroll
+        for (int u = 0; u < kStep * kStep / 128; ++u) {
+            const int e = tid + 128 * u, i = e % kStep, j = e / kStep;
+            v[u] = i < kb && j < kb ? D[i + static_cast<long long>(j) * m] : cx<R>{0, 0};
+        }
+#pragma unroll
+        for (int u = 0; u < kStep * kStep / 128; ++u) F[tid + 128 * u] = v[u];
     }
     __syncthreads();
     for (int k = 0; k < kb; ++k) {
         const cx<R> inv = crecip(F[k + k * kStep]);
-        const int rem = kb - k - 1;
-        for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
-            const int i = k + 1 + e % rem, j = k + 1 + e / rem;
-            if (i >= j) F[i + j * kStep] = fms(F[i + j * kStep], F[i + k * kStep], F[j + k * kStep] * inv);
+        for (int j = k + 1 + warp; j < kb; j += 4) {
+            const int i = j + lane;
+            if (i < kb) F[i + j * kStep] = fms(F[i + j * kStep], F[i + k * kStep], F[j + k * kStep] * inv);
         }
         __syncthreads();
-        for (int i = k + 1 + threadIdx.x; i < kb; i += blockDim.x) F[i + k * kStep] = F[i + k * kStep] * inv;
+        for (int i = k + 1 + tid; i < kb; i += blockDim.x) F[i + k * kStep] = F[i + k * kStep] * inv;
         __syncthreads();
     }
-    for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
-        const int i = e % kb, j = e / kb;
-        if (i >= j) D[i + static_cast<long long>(j) * m] = F[i + j * kStep];
+#pragma unroll
+    for (int u = 0; u < kStep * kStep / 128; ++u) {
+        const int e = tid + 128 * u, i = e % kStep, j = e / kStep;
+        if (i < kb && j < kb && i >= j) D[i + static_cast<long long>(j) * m] = F[e];
     }
 }
 
